@@ -1,0 +1,112 @@
+"""ctypes wrapper of the CPU oracle (oracle/ql_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, never by the ql_dns_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+
+
+class OracleParams(ctypes.Structure):
+    _fields_ = [
+        ("model", ctypes.c_int), ("integrator", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("NZ", ctypes.c_int),
+        ("L", ctypes.c_double * 3),
+        ("q", ctypes.c_double), ("omega", ctypes.c_double),
+        ("nu", ctypes.c_double), ("eta", ctypes.c_double), ("B0z", ctypes.c_double),
+        ("viscosity_order", ctypes.c_int),
+        ("dt", ctypes.c_double),
+        ("remap", ctypes.c_int), ("quasilinear", ctypes.c_int),
+        ("nthreads", ctypes.c_int),
+    ]
+
+
+def build(native: bool = False) -> None:
+    target = ["native"] if native else []
+    subprocess.run(["make", "-s", "-C", HERE] + target, check=True)
+
+
+_LIBS = {}
+
+
+def lib(kind: str = "strict"):
+    """kind: 'strict' (parity), 'fast' (portable timing build) or 'native'."""
+    if kind in _LIBS:
+        return _LIBS[kind]
+    if kind == "native":
+        path = os.path.join(BUILD, "native", "liboracle_fast.so")
+    else:
+        path = os.path.join(BUILD, f"liboracle_{kind}.so")
+    if not os.path.exists(path):
+        build(native=(kind == "native"))
+    L = ctypes.CDLL(path)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.oracle_run.argtypes = [ctypes.POINTER(OracleParams), dp, dp, dp, dp,
+                             ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
+    L.oracle_rhs.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_double, ctypes.c_double,
+                             dp, dp, dp, dp, dp, dp]
+    L.oracle_diagnostics.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_double, dp, dp, dp, dp]
+    L.oracle_fft.argtypes = [ctypes.c_int, ctypes.c_int, dp]
+    _LIBS[kind] = L
+    return L
+
+
+def _params(p, nthreads: int = 0) -> OracleParams:
+    return OracleParams(p.model, p.integrator, p.nx, p.ny, p.NZ, (ctypes.c_double * 3)(*p.L),
+                        p.q, p.omega, p.nu, p.eta, p.B0z, p.viscosity_order, p.dt,
+                        p.remap, p.quasilinear, nthreads)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def fft(x: np.ndarray, forward: bool, kind: str = "strict") -> np.ndarray:
+    a = np.ascontiguousarray(x, dtype=np.complex128).copy()
+    lib(kind).oracle_fft(a.size, 1 if forward else -1, _dp(a))
+    return a
+
+
+def rhs(p, t, dt_lin, lin, mf, kx0=None, kind: str = "strict"):
+    """One Model::rhs evaluation -> (Flin, Fmf, linOp[nxy,4,nz])."""
+    lin = np.ascontiguousarray(lin, dtype=np.complex128)
+    mf = np.ascontiguousarray(mf, dtype=np.complex128)
+    Fl = np.zeros_like(lin)
+    Fm = np.zeros_like(mf)
+    L = np.zeros(lin.shape, dtype=np.float64)
+    k = None if kx0 is None else _dp(np.ascontiguousarray(kx0, dtype=np.float64))
+    pp = _params(p)
+    lib(kind).oracle_rhs(ctypes.byref(pp), t, dt_lin, _dp(lin), _dp(mf), k, _dp(Fl), _dp(Fm), _dp(L))
+    return Fl, Fm, L
+
+
+def diagnostics(p, t, lin, mf, kx0=None, kind: str = "strict") -> np.ndarray:
+    lin = np.ascontiguousarray(lin, dtype=np.complex128)
+    mf = np.ascontiguousarray(mf, dtype=np.complex128)
+    out = np.zeros(14)
+    k = None if kx0 is None else _dp(np.ascontiguousarray(kx0, dtype=np.float64))
+    pp = _params(p)
+    lib(kind).oracle_diagnostics(ctypes.byref(pp), t, _dp(lin), _dp(mf), k, _dp(out))
+    return out
+
+
+def run(p, t0, lin, mf, kx0, nsteps, diag_every=0, kind: str = "strict", nthreads: int = 0):
+    """main.cpp loop for nsteps -> (t, lin, mf, kx0, diag[nrec, 15])."""
+    lin = np.ascontiguousarray(lin, dtype=np.complex128).copy()
+    mf = np.ascontiguousarray(mf, dtype=np.complex128).copy()
+    kx0 = np.ascontiguousarray(kx0, dtype=np.float64).copy()
+    t = np.array([t0], dtype=np.float64)
+    maxd = (nsteps + 2) if diag_every > 0 else 1
+    diag = np.zeros((maxd, 15))
+    pp = _params(p, nthreads)
+    n = lib(kind).oracle_run(ctypes.byref(pp), _dp(t), _dp(lin), _dp(mf), _dp(kx0), nsteps,
+                             diag_every, _dp(diag), maxd)
+    return float(t[0]), lin, mf, kx0, diag[:n]
