@@ -1,0 +1,122 @@
+/*
+ * qlgpu.h -- C ABI of the B200 (sm_100a) quasi-linear shearing-box time step.
+ *
+ * A drop-in for the time step of Cxb1993/ql_dns: the Model / Integrator /
+ * solution C++ API of the reference (QL_DNS/Models/Model.h:24-112,
+ * QL_DNS/Integrators/Integrator.h:20-28, QL_DNS/solution.h:23-49) maps onto
+ * these entry points.  Plain pointers and sizes only; every function returns
+ * a status code (QLGPU_OK = 0) where the reference calls ABORT / MPI_Abort
+ * (QL_DNS/General_Definitions.h:68-72).
+ *
+ * Data layout (host and device alike, interleaved re/im doubles):
+ *   lin[nxy][4][nz]   fluctuations (u, zeta, b, eta) = (u_x, w_x, b_x, j_x),
+ *                     kz in dealiased order 0..(nz-1)/2, -(nz-1)/2..-1
+ *                     (QL_DNS/solution.cpp:17-25; solution::pLin(i, V))
+ *   mf[nmf][nz]       mean fields (Bx, By[, Ux, Uy]) (solution.cpp:27-31;
+ *                     solution::pMF(i))
+ *   kx0[nxy]          unsheared kx of every mode (Kdata::kx imaginary part,
+ *                     QL_DNS/Auxiliary/Kdata.cpp:30-46), shifted by remaps
+ * nz = 1 + 2*floor(NZ/3), nxy = (nx-1)*(ny/2) (QL_DNS/Models/Model.h:34-36).
+ *
+ * Threading: one host thread per handle at a time.  Each handle owns its
+ * device memory and one CUDA stream; host buffers are read or written only
+ * during the call.
+ */
+#ifndef QLGPU_H_
+#define QLGPU_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QLGPU_OK 0
+#define QLGPU_ERR_ARG 1         /* invalid parameter or size */
+#define QLGPU_ERR_UNSUPPORTED 2 /* valid for the reference but not built here */
+#define QLGPU_ERR_CUDA 3        /* CUDA runtime error (message via qlgpu_last_error) */
+#define QLGPU_ERR_STATUS 4      /* device status word set: non-finite / unstable solution */
+#define QLGPU_ERR_NODEVICE 5    /* no CUDA device / extension unusable */
+
+#define QLGPU_MODEL_MHD_BQLIN 0    /* QL_DNS/Models/MHD_BQlin.cpp */
+#define QLGPU_MODEL_MHD_FULLQLIN 1 /* QL_DNS/Models/MHD_FullQlin.cpp */
+#define QLGPU_INTEG_RK3CN_ELIN 0   /* QL_DNS/Integrators/RK3CN_Elin.cpp (what main.cpp:95 uses) */
+#define QLGPU_INTEG_RK3CN 1        /* QL_DNS/Integrators/RK3CN.cpp */
+
+/* Parameters: the Inputs fields the step reads
+ * (QL_DNS/Auxiliary/Input_parameters.cpp:68-138). */
+typedef struct qlgpu_params {
+    int model;           /* QLGPU_MODEL_* (equations_to_use_) */
+    int integrator;      /* QLGPU_INTEG_* */
+    int nx, ny, NZ;      /* nx_, ny_, nz_ (NZ: power of two, 16..256) */
+    double L[3];         /* lx_, ly_, lz_ */
+    double q, omega;     /* q_, omega_ (MHD_BQlin uses 2q/3, MHD_BQlin.cpp:19) */
+    double nu, eta, B0z; /* nu_, eta_, B0z_ */
+    int viscosity_order; /* viscosity_order_ (MHD_FullQlin) */
+    double dt;           /* dt_ (> 0; variable CFL dt is not supported) */
+    int remap;           /* Remap? */
+    int quasilinear;     /* QuasiLinear? */
+} qlgpu_params;
+
+typedef struct qlgpu_handle qlgpu_t;
+
+/* Model + Integrator construction: replaces `new MHD_BQlin(SP, mpi, fft)` /
+ * `new MHD_FullQlin(...)` (QL_DNS/main.cpp:58-61) and `new RK3CN_Elin(t, SP,
+ * model)` (main.cpp:95).  device < 0 picks the current device.  The state
+ * starts at zero with t = 0 and kx0 from the wavenumber tables. */
+int qlgpu_create(const qlgpu_params* p, int device, qlgpu_t** out);
+int qlgpu_destroy(qlgpu_t* h);
+
+/* Model::Dimxy(), num_Lin(), NZ() (dealiased), num_MFs() (Model.h:53-58). */
+int qlgpu_dims(const qlgpu_t* h, int* nxy, int* nlin, int* nz, int* nmf);
+
+/* solution contents <-> host buffers (solution::pLin / pMF, Kdata::kx).
+ * set_state also resets the integrator as its constructor does
+ * (RK3CN.cpp:57: linear operators taken at t) and the diagnostic clock.
+ * kx0 may be NULL (set: wavenumber tables; get: not returned). */
+int qlgpu_set_state(qlgpu_t* h, double t, const double* lin, const double* mf, const double* kx0);
+int qlgpu_get_state(qlgpu_t* h, double* t, double* lin, double* mf, double* kx0);
+
+/* Same, with device pointers (already resident in this device's memory). */
+int qlgpu_set_state_device(qlgpu_t* h, double t, const void* lin, const void* mf, const void* kx0);
+int qlgpu_get_state_device(qlgpu_t* h, double* t, void* lin, void* mf, void* kx0);
+
+/* The main-loop body of QL_DNS/main.cpp:108-133 repeated nsteps times:
+ * Integrator::Step, t += dt, ShearingBox_Remap(q t) if remap, and
+ * Calc_Energy_AM_Diss whenever the time-variable accumulator reaches
+ * diag_every*dt (main.cpp:127-130; diag_every <= 0: never).  Each diagnostic
+ * record is 15 doubles: t, energy[MU, MB, u, b], AM[MU, MB, u, b],
+ * diss[MU, MB, u, b], etaK_times_kmax[2] (MHD_BQlin.cpp:449-477).  Records go
+ * to diag_out (max_diag of them; extra records set QLGPU_ERR_STATUS); *ndiag
+ * receives the count.  diag_out may be NULL when diag_every <= 0. */
+int qlgpu_step(qlgpu_t* h, int nsteps, int diag_every, double* diag_out, int max_diag, int* ndiag);
+
+/* Calc_Energy_AM_Diss at the current time without stepping (15 doubles as
+ * above): the initial record of main.cpp:98-103. */
+int qlgpu_diagnostics(qlgpu_t* h, double* out15);
+
+/* Model::rhs(t, dt_lin, SolIn, SolOut, linOp) (Model.h:46-47) on host
+ * buffers: rhs of the fluctuations and mean fields and the linear operator
+ * at t + dt_lin.  Uses the handle's kx0; does not touch its state.
+ * linop (nxy*4*nz doubles) may be NULL. */
+int qlgpu_rhs(qlgpu_t* h, double t, double dt_lin, const double* lin_in, const double* mf_in, double* lin_rhs,
+              double* mf_rhs, double* linop);
+
+/* Device status word (solution::Check_Solution, QL_DNS/solution.cpp:169-203):
+ * bit 1 non-finite mean field, bit 2 |mean field| > 1e20, bit 4 diagnostic
+ * records dropped.  Reading does not clear it; set_state clears it. */
+int qlgpu_status(qlgpu_t* h, int* status);
+
+/* Current simulation time and the CUDA stream (cudaStream_t) of the handle. */
+int qlgpu_time(qlgpu_t* h, double* t);
+int qlgpu_stream(qlgpu_t* h, void** stream);
+
+/* Message of the last error on this handle (or of the last failed create
+ * when h is NULL).  Returns the message length. */
+int qlgpu_last_error(const qlgpu_t* h, char* buf, int buflen);
+
+/* Library version string. */
+const char* qlgpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QLGPU_H_ */

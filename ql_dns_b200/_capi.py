@@ -1,0 +1,95 @@
+"""ctypes binding of the C ABI declared in include/qlgpu.h (libqlgpu.so).
+
+The library is loaded from the package's ``_lib`` directory.  There is no CPU
+fallback: if the library or a CUDA device is missing every call fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libqlgpu.so")
+
+QLGPU_OK = 0
+ERRORS = {1: "QLGPU_ERR_ARG", 2: "QLGPU_ERR_UNSUPPORTED", 3: "QLGPU_ERR_CUDA", 4: "QLGPU_ERR_STATUS",
+          5: "QLGPU_ERR_NODEVICE"}
+
+# Every symbol include/qlgpu.h declares.
+EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "qlgpu_get_state",
+           "qlgpu_set_state_device", "qlgpu_get_state_device", "qlgpu_step", "qlgpu_diagnostics",
+           "qlgpu_rhs", "qlgpu_status", "qlgpu_time", "qlgpu_stream", "qlgpu_last_error", "qlgpu_version"]
+
+
+class qlgpu_params(ctypes.Structure):
+    _fields_ = [
+        ("model", ctypes.c_int), ("integrator", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("NZ", ctypes.c_int),
+        ("L", ctypes.c_double * 3),
+        ("q", ctypes.c_double), ("omega", ctypes.c_double),
+        ("nu", ctypes.c_double), ("eta", ctypes.c_double), ("B0z", ctypes.c_double),
+        ("viscosity_order", ctypes.c_int),
+        ("dt", ctypes.c_double),
+        ("remap", ctypes.c_int), ("quasilinear", ctypes.c_int),
+    ]
+
+
+class QLGPUError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libqlgpu.so (raises if it is missing; there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise QLGPUError(5, f"{path} not built (python -m ql_dns_b200.build)")
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.qlgpu_create.argtypes = [ctypes.POINTER(qlgpu_params), ctypes.c_int, ctypes.POINTER(vp)]
+    L.qlgpu_destroy.argtypes = [vp]
+    L.qlgpu_dims.argtypes = [vp, ip, ip, ip, ip]
+    L.qlgpu_set_state.argtypes = [vp, ctypes.c_double, dp, dp, dp]
+    L.qlgpu_get_state.argtypes = [vp, dp, dp, dp, dp]
+    L.qlgpu_set_state_device.argtypes = [vp, ctypes.c_double, vp, vp, vp]
+    L.qlgpu_get_state_device.argtypes = [vp, dp, vp, vp, vp]
+    L.qlgpu_step.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ip]
+    L.qlgpu_diagnostics.argtypes = [vp, dp]
+    L.qlgpu_rhs.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp, dp]
+    L.qlgpu_status.argtypes = [vp, ip]
+    L.qlgpu_time.argtypes = [vp, dp]
+    L.qlgpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.qlgpu_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    L.qlgpu_version.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        if name not in ("qlgpu_version",):
+            getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def to_c(p) -> qlgpu_params:
+    return qlgpu_params(p.model, p.integrator, p.nx, p.ny, p.NZ, (ctypes.c_double * 3)(*p.L), p.q, p.omega,
+                        p.nu, p.eta, p.B0z, p.viscosity_order, p.dt, p.remap, p.quasilinear)
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def check(rc: int, h=None):
+    if rc != QLGPU_OK:
+        L = load()
+        buf = ctypes.create_string_buffer(512)
+        L.qlgpu_last_error(h, buf, 512)
+        raise QLGPUError(rc, buf.value.decode(errors="replace"))

@@ -1,0 +1,589 @@
+// qlgpu.cu -- host side of the C ABI in include/qlgpu.h: handle lifetime,
+// wavenumber tables, device buffers, stage launches and the main-loop
+// bookkeeping of QL_DNS/main.cpp:108-133.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/qlgpu.h"
+#include "qlgpu_kernel.cuh"
+
+using namespace qlgpu;
+
+namespace {
+
+const double kPI = 3.14159265358979323846;  // General_Definitions.h PI
+
+thread_local std::string g_create_error;
+
+// RK3 coefficients (RK3CN_Elin.cpp:19-20, RK3CN.cpp:19-20)
+const double a0_ = 8.0 / 15.0, a1_ = 5.0 / 12.0, a2_ = 3.0 / 4.0, b1_ = -17.0 / 60.0, b2_ = -5.0 / 12.0;
+const double p1_ = 8.0 / 15.0, p2_ = 2.0 / 3.0;
+
+typedef void (*stage_launch_fn)(const StageArgs&, const DevParams&, int grid, int block, size_t smem, cudaStream_t);
+typedef void (*diag_launch_fn)(const cplx*, const cplx*, const double*, const double*, const int*, const int*,
+                               const DevParams&, double, double*, cudaStream_t);
+typedef size_t (*smem_fn)(int warps);
+typedef const void* (*kptr_fn)();
+
+template <int NZ, int MODEL, int INTEG>
+void launch_stage(const StageArgs& A, const DevParams& P, int grid, int block, size_t smem, cudaStream_t st) {
+    stage_kernel<NZ, MODEL, INTEG><<<grid, block, smem, st>>>(A, P);
+}
+template <int NZ, int MODEL, int INTEG>
+const void* stage_ptr() {
+    return reinterpret_cast<const void*>(&stage_kernel<NZ, MODEL, INTEG>);
+}
+template <int NZ, int MODEL>
+size_t stage_smem(int warps) {
+    return Smem<Geom<NZ>, MODEL>::bytes(warps);
+}
+template <int NZ>
+void launch_diag(const cplx* lin, const cplx* mf, const double* kx0, const double* ky, const int* kxi, const int* kyi,
+                 const DevParams& P, double t, double* out, cudaStream_t st) {
+    diag_kernel<NZ><<<1, 128, 0, st>>>(lin, mf, kx0, ky, kxi, kyi, P, t, out);
+}
+
+struct Variant {
+    stage_launch_fn launch;
+    kptr_fn kernel;
+    smem_fn smem;
+    diag_launch_fn diag;
+    int T;   // threads per mode
+    int PL;  // partial vector length
+};
+
+template <int NZ, int MODEL, int INTEG>
+Variant make_variant() {
+    Variant v;
+    v.launch = &launch_stage<NZ, MODEL, INTEG>;
+    v.kernel = &stage_ptr<NZ, MODEL, INTEG>;
+    v.smem = &stage_smem<NZ, MODEL>;
+    v.diag = &launch_diag<NZ>;
+    v.T = Geom<NZ>::T;
+    v.PL = Smem<Geom<NZ>, MODEL>::PL;
+    return v;
+}
+
+bool pick_variant(int NZ, int model, int integ, Variant* out) {
+#define QLGPU_CASE(NZV)                                                                         \
+    if (NZ == NZV) {                                                                            \
+        if (model == MODEL_BQLIN && integ == INTEG_EXP) *out = make_variant<NZV, MODEL_BQLIN, INTEG_EXP>(); \
+        else if (model == MODEL_BQLIN && integ == INTEG_CN) *out = make_variant<NZV, MODEL_BQLIN, INTEG_CN>(); \
+        else return false;                                                                      \
+        return true;                                                                            \
+    }
+    QLGPU_CASE(16)
+    QLGPU_CASE(32)
+    QLGPU_CASE(64)
+    QLGPU_CASE(128)
+    QLGPU_CASE(256)
+#undef QLGPU_CASE
+    return false;
+}
+
+}  // namespace
+
+struct qlgpu_handle {
+    qlgpu_params p;
+    DevParams dp;
+    Variant var;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int nxy = 0, nz = 0, NZ = 0, nmf = 0;
+    cplx* d_lin[2] = {nullptr, nullptr};
+    int cur = 0;
+    cplx* d_F1 = nullptr;
+    cplx* d_F2 = nullptr;
+    cplx* d_mf = nullptr;
+    cplx* d_Fmf1 = nullptr;
+    cplx* d_Fmf2 = nullptr;
+    double* d_kx0 = nullptr;
+    double* d_ky = nullptr;
+    int* d_kxi = nullptr;
+    int* d_kyi = nullptr;
+    cplx* d_tw = nullptr;
+    double* d_partials = nullptr;
+    double* d_gpartials = nullptr;
+    DevClock* d_clk = nullptr;
+    double* d_diag = nullptr;
+    int diag_cap = 0;
+    double* d_out15 = nullptr;
+    double* d_linop = nullptr;
+    int grid = 0, warps = 4, block = 128;
+    size_t smem = 0;
+    std::vector<double> kx_tab, ky_tab;
+    std::vector<int> kxi_tab, kyi_tab;
+    std::string err;
+};
+
+namespace {
+
+int fail(qlgpu_t* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define QLGPU_CK(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return fail(h, QLGPU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Kdata tables (QL_DNS/Auxiliary/Kdata.cpp:24-46)
+void ktables(const qlgpu_params& p, std::vector<double>& kx, std::vector<double>& ky, std::vector<int>& kxi,
+             std::vector<int>& kyi) {
+    const double kxL = 2 * kPI / p.L[0], kyL = 2 * kPI / p.L[1];
+    const int ny = ((p.ny / 2) * 2) / 2, nx = p.nx / 2;
+    const int nxy = (p.nx - 1) * (p.ny / 2);
+    kx.assign(nxy, 0.0);
+    ky.assign(nxy, 0.0);
+    kxi.assign(nxy, 0);
+    kyi.assign(nxy, 0);
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            kx[j + ny * i] = i * kxL;
+            ky[j + ny * i] = j * kyL;
+            kxi[j + ny * i] = i;
+            kyi[j + ny * i] = j;
+        }
+    for (int i = nx + 1; i < 2 * nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            kx[j + ny * (i - 1)] = (-2 * nx + i) * kxL;
+            ky[j + ny * (i - 1)] = j * kyL;
+            kxi[j + ny * (i - 1)] = -2 * nx + i;
+            kyi[j + ny * (i - 1)] = j;
+        }
+}
+
+int reset_clock(qlgpu_t* h, double t) {
+    DevClock c;
+    std::memset(&c, 0, sizeof(c));
+    c.t = t;
+    c.timevar = 0.0;
+    c.old_init = 1;
+    QLGPU_CK(cudaMemcpyAsync(h->d_clk, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream));
+    return QLGPU_OK;
+}
+
+StageArgs base_args(qlgpu_t* h) {
+    StageArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.mf = h->d_mf;
+    A.kx0 = h->d_kx0;
+    A.ky = h->d_ky;
+    A.kxi = h->d_kxi;
+    A.kyi = h->d_kyi;
+    A.tw = h->d_tw;
+    A.partials = h->d_partials;
+    A.gpartials = h->d_gpartials;
+    A.clk = h->d_clk;
+    A.diag_ring = h->d_diag;
+    A.diag_cap = h->diag_cap;
+    return A;
+}
+
+// One RK3 step = three stage launches (RK3CN_Elin::Step / RK3CN::Step).
+void enqueue_step(qlgpu_t* h) {
+    const double dt = h->p.dt;
+    const bool cn = h->p.integrator == INTEG_CN;
+    const double lcf = cn ? dt / 2 : dt;
+    struct {
+        double t_off, dt_lin, linC, n1, n2;
+        int has_prev;
+    } st[3] = {
+        {0.0, dt * p1_, lcf * (a0_), a0_ * dt, 0.0, 0},
+        {dt * p1_, dt * (p2_ - p1_), lcf * (a1_ + b1_), a1_ * dt, b1_ * dt, 1},
+        {dt * p2_, dt * (1.0 - p2_), lcf * (a2_ + b2_), a2_ * dt, b2_ * dt, 1},
+    };
+    cplx* Fbuf[3] = {h->d_F1, h->d_F2, nullptr};
+    const cplx* Fprev[3] = {nullptr, h->d_F1, h->d_F2};
+    cplx* Fmf[3] = {h->d_Fmf1, h->d_Fmf2, h->d_Fmf1};
+    const cplx* Fmfp[3] = {nullptr, h->d_Fmf1, h->d_Fmf2};
+    for (int s = 0; s < 3; ++s) {
+        StageArgs A = base_args(h);
+        A.lin_in = h->d_lin[h->cur];
+        A.lin_out = h->d_lin[h->cur ^ 1];
+        A.Fprev = Fprev[s];
+        A.Fout = Fbuf[s];
+        A.Fmf_prev = Fmfp[s];
+        A.Fmf_out = (s < 2) ? Fmf[s] : nullptr;
+        A.sc.t_off = st[s].t_off;
+        A.sc.dt_lin = st[s].dt_lin;
+        A.sc.linC = st[s].linC;
+        A.sc.n1 = st[s].n1;
+        A.sc.n2 = st[s].n2;
+        A.sc.has_prev = st[s].has_prev;
+        A.sc.last = (s == 2);
+        h->var.launch(A, h->dp, h->grid, h->block, h->smem, h->stream);
+        h->cur ^= 1;
+    }
+}
+
+int ensure_diag(qlgpu_t* h, int cap) {
+    if (cap <= h->diag_cap) return QLGPU_OK;
+    if (h->d_diag) cudaFree(h->d_diag);
+    h->d_diag = nullptr;
+    QLGPU_CK(cudaMalloc(&h->d_diag, sizeof(double) * 15 * (size_t)cap));
+    h->diag_cap = cap;
+    return QLGPU_OK;
+}
+
+int check_launch(qlgpu_t* h) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, QLGPU_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return QLGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* qlgpu_version(void) { return "qlgpu 0.1 (sm_100a, FP64)"; }
+
+int qlgpu_last_error(const qlgpu_t* h, char* buf, int buflen) {
+    const std::string& s = h ? h->err : g_create_error;
+    if (buf && buflen > 0) {
+        std::snprintf(buf, (size_t)buflen, "%s", s.c_str());
+    }
+    return (int)s.size();
+}
+
+int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
+    qlgpu_t* h = nullptr;
+    if (!pp || !out) return fail(nullptr, QLGPU_ERR_ARG, "null argument");
+    *out = nullptr;
+    const qlgpu_params& p = *pp;
+    if (p.model != QLGPU_MODEL_MHD_BQLIN && p.model != QLGPU_MODEL_MHD_FULLQLIN)
+        return fail(nullptr, QLGPU_ERR_ARG, "unknown model (no matching model found, main.cpp:71-74)");
+    if (p.integrator != QLGPU_INTEG_RK3CN_ELIN && p.integrator != QLGPU_INTEG_RK3CN)
+        return fail(nullptr, QLGPU_ERR_ARG, "unknown integrator");
+    if (p.nx < 2 || (p.nx % 2) || p.ny < 2 || (p.ny % 2))
+        return fail(nullptr, QLGPU_ERR_ARG, "nx and ny must be even and >= 2");
+    if (!(p.dt > 0))
+        return fail(nullptr, QLGPU_ERR_UNSUPPORTED, "dt must be > 0 (variable CFL time step not supported)");
+    if (!(p.L[0] > 0 && p.L[1] > 0 && p.L[2] > 0)) return fail(nullptr, QLGPU_ERR_ARG, "box lengths must be > 0");
+    if (p.model == QLGPU_MODEL_MHD_BQLIN && p.nu == 0.0)
+        return fail(nullptr, QLGPU_ERR_ARG, "MHD_BQlin divides by nu (MHD_BQlin.cpp:251); nu must be nonzero");
+    Variant var;
+    if (!pick_variant(p.NZ, p.model, p.integrator, &var))
+        return fail(nullptr, QLGPU_ERR_UNSUPPORTED,
+                    "unsupported (NZ, model): NZ must be a power of two in [16, 256]; model built: MHD_BQlin");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(nullptr, QLGPU_ERR_NODEVICE, "no CUDA device");
+    h = new (std::nothrow) qlgpu_handle();
+    if (!h) return fail(nullptr, QLGPU_ERR_ARG, "out of host memory");
+    h->p = p;
+    h->var = var;
+    if (device < 0) cudaGetDevice(&device);
+    h->device = device;
+    int rc;
+    auto bail = [&](int code) {
+        g_create_error = h->err;
+        qlgpu_destroy(h);
+        return code;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) {
+        h->err = "cudaSetDevice failed";
+        return bail(QLGPU_ERR_NODEVICE);
+    }
+    h->NZ = p.NZ;
+    h->nz = 1 + 2 * int(p.NZ / 3.0);
+    h->nxy = (p.nx - 1) * (p.ny / 2);
+    h->nmf = p.model == QLGPU_MODEL_MHD_BQLIN ? 2 : 4;
+    // Device parameters
+    DevParams& d = h->dp;
+    std::memset(&d, 0, sizeof(d));
+    d.nxy = h->nxy;
+    d.nz = h->nz;
+    d.NZ = h->NZ;
+    d.nmf = h->nmf;
+    d.q = p.q;
+    d.Omega = p.model == QLGPU_MODEL_MHD_BQLIN ? 2.0 / 3.0 * p.q : p.omega;
+    d.nu = p.nu;
+    d.eta = p.eta;
+    d.etanu = p.model == QLGPU_MODEL_MHD_BQLIN ? p.eta / p.nu : p.eta;
+    d.B0z = p.B0z;
+    d.visc_half = p.viscosity_order / 2;
+    d.ql = p.quasilinear ? 1 : 0;
+    d.remap = p.remap ? 1 : 0;
+    d.kzL = 2 * kPI / p.L[2];
+    d.fac = 1.0 / p.NZ;
+    const int Nx = p.nx, Ny = (p.ny / 2) * 2;
+    d.rs_fac = 1.0 / (Ny * Nx) / (Ny * Nx);
+    long totalN2 = (long)Nx * Ny * p.NZ;
+    totalN2 = totalN2 * totalN2;
+    d.divfac = p.L[2] / (double)totalN2;
+    d.divMF = p.L[2] / ((double)p.NZ * p.NZ);
+    const double kxLfac = 2 * kPI / p.L[0];
+    const int nxm1 = Nx - 1;
+    d.remap_thresh = nxm1 / 2.0 * kxLfac;
+    d.remap_shift = nxm1 * kxLfac;
+    d.dt = p.dt;
+    d.tv_interval = 0.0;
+    d.kzmax = 2 * kPI / p.L[2] * (p.NZ / 3);
+
+    ktables(p, h->kx_tab, h->ky_tab, h->kxi_tab, h->kyi_tab);
+    // Launch geometry: as many CTAs as fit, at most one mode per group
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        h->err = "cudaGetDeviceProperties failed";
+        return bail(QLGPU_ERR_CUDA);
+    }
+    h->warps = 4;
+    h->block = 32 * h->warps;
+    h->smem = var.smem(h->warps);
+    if (cudaFuncSetAttribute(var.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem) != cudaSuccess) {
+        h->err = "shared memory request too large";
+        return bail(QLGPU_ERR_CUDA);
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, var.kernel(), h->block, h->smem);
+    if (per_sm < 1) per_sm = 1;
+    const int groups_per_cta = h->warps * (32 / var.T);
+    int need = (h->nxy + groups_per_cta - 1) / groups_per_cta;
+    int cap = prop.multiProcessorCount * per_sm;
+    h->grid = need < cap ? need : cap;
+    if (h->grid > 64 * RED_GROUP) h->grid = 64 * RED_GROUP;
+    if (h->grid < 1) h->grid = 1;
+    const int ngroups = (h->grid + RED_GROUP - 1) / RED_GROUP;
+
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        h->err = "stream create failed";
+        return bail(QLGPU_ERR_CUDA);
+    }
+    const size_t nlin = (size_t)h->nxy * 4 * h->nz, nmfe = (size_t)h->nmf * h->nz;
+#define QLGPU_ALLOC(ptr, bytes)                                        \
+    if (cudaMalloc(&(ptr), (bytes)) != cudaSuccess) {                  \
+        h->err = "cudaMalloc failed for " #ptr;                        \
+        return bail(QLGPU_ERR_CUDA);                                   \
+    }                                                                  \
+    cudaMemsetAsync((ptr), 0, (bytes), h->stream);
+    QLGPU_ALLOC(h->d_lin[0], nlin * sizeof(cplx));
+    QLGPU_ALLOC(h->d_lin[1], nlin * sizeof(cplx));
+    QLGPU_ALLOC(h->d_F1, nlin * sizeof(cplx));
+    QLGPU_ALLOC(h->d_F2, nlin * sizeof(cplx));
+    QLGPU_ALLOC(h->d_mf, nmfe * sizeof(cplx));
+    QLGPU_ALLOC(h->d_Fmf1, nmfe * sizeof(cplx));
+    QLGPU_ALLOC(h->d_Fmf2, nmfe * sizeof(cplx));
+    QLGPU_ALLOC(h->d_kx0, h->nxy * sizeof(double));
+    QLGPU_ALLOC(h->d_ky, h->nxy * sizeof(double));
+    QLGPU_ALLOC(h->d_kxi, h->nxy * sizeof(int));
+    QLGPU_ALLOC(h->d_kyi, h->nxy * sizeof(int));
+    QLGPU_ALLOC(h->d_tw, h->NZ * sizeof(cplx));
+    QLGPU_ALLOC(h->d_partials, (size_t)h->grid * var.PL * sizeof(double));
+    QLGPU_ALLOC(h->d_gpartials, (size_t)ngroups * var.PL * sizeof(double));
+    QLGPU_ALLOC(h->d_clk, sizeof(DevClock));
+    QLGPU_ALLOC(h->d_out15, 15 * sizeof(double));
+#undef QLGPU_ALLOC
+    // Twiddles tw[n2*T + t] = exp(+2 pi i n2 t/NZ)
+    std::vector<cplx> tw(h->NZ);
+    const int T = var.T, P = h->NZ / T;
+    for (int n2 = 0; n2 < P; ++n2)
+        for (int t = 0; t < T; ++t) {
+            const int m = (n2 * t) % h->NZ;
+            const double ang = 2.0 * kPI * (double)m / (double)h->NZ;
+            tw[n2 * T + t].x = std::cos(ang);
+            tw[n2 * T + t].y = std::sin(ang);
+        }
+    cudaMemcpyAsync(h->d_tw, tw.data(), tw.size() * sizeof(cplx), cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_kx0, h->kx_tab.data(), h->nxy * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_ky, h->ky_tab.data(), h->nxy * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_kxi, h->kxi_tab.data(), h->nxy * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_kyi, h->kyi_tab.data(), h->nxy * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    rc = reset_clock(h, 0.0);
+    if (rc) return bail(rc);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        h->err = "initialisation failed";
+        return bail(QLGPU_ERR_CUDA);
+    }
+    *out = h;
+    return QLGPU_OK;
+}
+
+int qlgpu_destroy(qlgpu_t* h) {
+    if (!h) return QLGPU_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    void* bufs[] = {h->d_lin[0], h->d_lin[1], h->d_F1, h->d_F2, h->d_mf, h->d_Fmf1, h->d_Fmf2,
+                    h->d_kx0, h->d_ky, h->d_kxi, h->d_kyi, h->d_tw, h->d_partials, h->d_gpartials,
+                    h->d_clk, h->d_diag, h->d_out15, h->d_linop};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return QLGPU_OK;
+}
+
+int qlgpu_dims(const qlgpu_t* h, int* nxy, int* nlin, int* nz, int* nmf) {
+    if (!h) return QLGPU_ERR_ARG;
+    if (nxy) *nxy = h->nxy;
+    if (nlin) *nlin = 4;
+    if (nz) *nz = h->nz;
+    if (nmf) *nmf = h->nmf;
+    return QLGPU_OK;
+}
+
+static int set_state_impl(qlgpu_t* h, double t, const void* lin, const void* mf, const void* kx0, cudaMemcpyKind k) {
+    if (!h || !lin || !mf) return fail(h, QLGPU_ERR_ARG, "null state pointer");
+    QLGPU_CK(cudaSetDevice(h->device));
+    const size_t nlin = (size_t)h->nxy * 4 * h->nz, nmfe = (size_t)h->nmf * h->nz;
+    h->cur = 0;
+    QLGPU_CK(cudaMemcpyAsync(h->d_lin[0], lin, nlin * sizeof(cplx), k, h->stream));
+    QLGPU_CK(cudaMemcpyAsync(h->d_mf, mf, nmfe * sizeof(cplx), k, h->stream));
+    if (kx0) QLGPU_CK(cudaMemcpyAsync(h->d_kx0, kx0, h->nxy * sizeof(double), k, h->stream));
+    else
+        QLGPU_CK(cudaMemcpyAsync(h->d_kx0, h->kx_tab.data(), h->nxy * sizeof(double), cudaMemcpyHostToDevice,
+                                 h->stream));
+    int rc = reset_clock(h, t);
+    if (rc) return rc;
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    return QLGPU_OK;
+}
+
+static int get_state_impl(qlgpu_t* h, double* t, void* lin, void* mf, void* kx0, cudaMemcpyKind k) {
+    if (!h) return QLGPU_ERR_ARG;
+    QLGPU_CK(cudaSetDevice(h->device));
+    const size_t nlin = (size_t)h->nxy * 4 * h->nz, nmfe = (size_t)h->nmf * h->nz;
+    if (lin) QLGPU_CK(cudaMemcpyAsync(lin, h->d_lin[h->cur], nlin * sizeof(cplx), k, h->stream));
+    if (mf) QLGPU_CK(cudaMemcpyAsync(mf, h->d_mf, nmfe * sizeof(cplx), k, h->stream));
+    if (kx0) QLGPU_CK(cudaMemcpyAsync(kx0, h->d_kx0, h->nxy * sizeof(double), k, h->stream));
+    double tt = 0;
+    QLGPU_CK(cudaMemcpyAsync(&tt, &h->d_clk->t, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    if (t) *t = tt;
+    return QLGPU_OK;
+}
+
+int qlgpu_set_state(qlgpu_t* h, double t, const double* lin, const double* mf, const double* kx0) {
+    return set_state_impl(h, t, lin, mf, kx0, cudaMemcpyHostToDevice);
+}
+int qlgpu_get_state(qlgpu_t* h, double* t, double* lin, double* mf, double* kx0) {
+    return get_state_impl(h, t, lin, mf, kx0, cudaMemcpyDeviceToHost);
+}
+int qlgpu_set_state_device(qlgpu_t* h, double t, const void* lin, const void* mf, const void* kx0) {
+    return set_state_impl(h, t, lin, mf, kx0, cudaMemcpyDeviceToDevice);
+}
+int qlgpu_get_state_device(qlgpu_t* h, double* t, void* lin, void* mf, void* kx0) {
+    return get_state_impl(h, t, lin, mf, kx0, cudaMemcpyDeviceToDevice);
+}
+
+int qlgpu_step(qlgpu_t* h, int nsteps, int diag_every, double* diag_out, int max_diag, int* ndiag) {
+    if (!h) return QLGPU_ERR_ARG;
+    if (nsteps < 0) return fail(h, QLGPU_ERR_ARG, "nsteps < 0");
+    if (diag_every > 0 && (!diag_out || max_diag < 0)) return fail(h, QLGPU_ERR_ARG, "diag_out required");
+    QLGPU_CK(cudaSetDevice(h->device));
+    const double interval = diag_every > 0 ? diag_every * h->p.dt : 0.0;
+    if (interval != h->dp.tv_interval) h->dp.tv_interval = interval;
+    if (diag_every > 0) {
+        int rc = ensure_diag(h, max_diag > 0 ? max_diag : 1);
+        if (rc) return rc;
+        // restart the record counter for this call
+        int zero = 0;
+        QLGPU_CK(cudaMemcpyAsync(&h->d_clk->ndiag, &zero, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    }
+    for (int n = 0; n < nsteps; ++n) {
+        enqueue_step(h);
+        if ((n & 63) == 63) {
+            int rc = check_launch(h);
+            if (rc) return rc;
+        }
+    }
+    int rc = check_launch(h);
+    if (rc) return rc;
+    DevClock c;
+    QLGPU_CK(cudaMemcpyAsync(&c, h->d_clk, sizeof(DevClock), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    int nrec = 0;
+    if (diag_every > 0) {
+        nrec = c.ndiag < max_diag ? c.ndiag : max_diag;
+        if (nrec > 0)
+            QLGPU_CK(cudaMemcpy(diag_out, h->d_diag, sizeof(double) * 15 * (size_t)nrec, cudaMemcpyDeviceToHost));
+    }
+    if (ndiag) *ndiag = nrec;
+    if (c.status & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE | QLGPU_STATUS_DIAG_FULL)) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "device status 0x%x: %s", c.status,
+                      (c.status & QLGPU_STATUS_NONFINITE)  ? "solution contains NaN or Inf (solution.cpp:194)"
+                      : (c.status & QLGPU_STATUS_UNSTABLE) ? "solution is very large, probably unstable (solution.cpp:184)"
+                                                           : "diagnostic records dropped (max_diag too small)");
+        return fail(h, QLGPU_ERR_STATUS, buf);
+    }
+    return QLGPU_OK;
+}
+
+int qlgpu_diagnostics(qlgpu_t* h, double* out15) {
+    if (!h || !out15) return QLGPU_ERR_ARG;
+    QLGPU_CK(cudaSetDevice(h->device));
+    double t = 0;
+    QLGPU_CK(cudaMemcpyAsync(&t, &h->d_clk->t, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    h->var.diag(h->d_lin[h->cur], h->d_mf, h->d_kx0, h->d_ky, h->d_kxi, h->d_kyi, h->dp, t, h->d_out15, h->stream);
+    int rc = check_launch(h);
+    if (rc) return rc;
+    QLGPU_CK(cudaMemcpyAsync(out15, h->d_out15, 15 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_rhs(qlgpu_t* h, double t, double dt_lin, const double* lin_in, const double* mf_in, double* lin_rhs,
+              double* mf_rhs, double* linop) {
+    if (!h || !lin_in || !mf_in || !lin_rhs || !mf_rhs) return fail(h, QLGPU_ERR_ARG, "null argument");
+    QLGPU_CK(cudaSetDevice(h->device));
+    const size_t nlin = (size_t)h->nxy * 4 * h->nz, nmfe = (size_t)h->nmf * h->nz;
+    if (linop && !h->d_linop) QLGPU_CK(cudaMalloc(&h->d_linop, nlin * sizeof(double)));
+    // Scratch: F1 holds the input copy, F2 the rhs, Fmf2 the input MF copy, Fmf1 the MF rhs.
+    // The model reads the mean field from A.mf, so the handle's mean field is saved and restored.
+    QLGPU_CK(cudaMemcpyAsync(h->d_F1, lin_in, nlin * sizeof(cplx), cudaMemcpyHostToDevice, h->stream));
+    QLGPU_CK(cudaMemcpyAsync(h->d_Fmf2, h->d_mf, nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, h->stream));
+    QLGPU_CK(cudaMemcpyAsync(h->d_mf, mf_in, nmfe * sizeof(cplx), cudaMemcpyHostToDevice, h->stream));
+    StageArgs A = base_args(h);
+    A.lin_in = h->d_F1;
+    A.lin_out = h->d_F2;
+    A.Fmf_out = h->d_Fmf1;
+    A.rhs_only = 1;
+    A.linop_out = linop ? h->d_linop : nullptr;
+    A.sc.t_off = t;
+    A.sc.abs_time = 1;
+    A.sc.dt_lin = dt_lin;
+    h->var.launch(A, h->dp, h->grid, h->block, h->smem, h->stream);
+    int rc = check_launch(h);
+    if (rc) return rc;
+    QLGPU_CK(cudaMemcpyAsync(lin_rhs, h->d_F2, nlin * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaMemcpyAsync(mf_rhs, h->d_Fmf1, nmfe * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream));
+    if (linop) QLGPU_CK(cudaMemcpyAsync(linop, h->d_linop, nlin * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaMemcpyAsync(h->d_mf, h->d_Fmf2, nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_status(qlgpu_t* h, int* status) {
+    if (!h || !status) return QLGPU_ERR_ARG;
+    QLGPU_CK(cudaSetDevice(h->device));
+    QLGPU_CK(cudaMemcpyAsync(status, &h->d_clk->status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_time(qlgpu_t* h, double* t) {
+    if (!h || !t) return QLGPU_ERR_ARG;
+    QLGPU_CK(cudaSetDevice(h->device));
+    QLGPU_CK(cudaMemcpyAsync(t, &h->d_clk->t, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_stream(qlgpu_t* h, void** stream) {
+    if (!h || !stream) return QLGPU_ERR_ARG;
+    *stream = (void*)h->stream;
+    return QLGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,391 @@
+// qlgpu_kernel.cuh -- the stage kernel (sm_100a): mean-field profiles, the
+// per-mode loop, the remap / diagnostics epilogue, the fixed-order two-level
+// reduction over CTAs and the mean-field update done by the last CTA.
+#pragma once
+#include "qlgpu_stage.cuh"
+
+namespace qlgpu {
+
+constexpr int RED_GROUP = 16;  // CTAs per first-level reduction group
+
+// Mean-field real-space profiles for the stage (MHD_BQlin.cpp:122-127:
+// By, dz By, dz^2 By; MHD_FullQlin.cpp:180-198: Bx, By, Ux, Uy and dz of each),
+// real part kept (the mean fields are real in z).
+template <class G, int MODEL>
+__device__ __forceinline__ void mean_profiles(const DevParams& P, const cplx* mf, double* mfr, cplx* xch, const cplx* tw,
+                                              int gidx, int ngroups, int t, unsigned gmask) {
+    constexpr int NMFR = Smem<G, MODEL>::NMFR;
+    for (int arr = gidx; arr < NMFR; arr += ngroups) {
+        int src, deriv;
+        if (MODEL == MODEL_BQLIN) {
+            src = 1;
+            deriv = arr;  // 0: By, 1: dz By, 2: dz^2 By
+        } else {
+            src = arr / 2;  // Bx, By, Ux, Uy
+            deriv = arr % 2;
+        }
+        cplx x[G::P];
+#pragma unroll
+        for (int k2 = 0; k2 < G::P; ++k2) {
+            const int k = t + G::T * k2;
+            const int s = stored_index<G>(k);
+            cplx v = mk(0.0, 0.0);
+            if (s >= 0) {
+                v = cscale(ldc_cg(mf + src * P.nz + s), P.fac);
+                const double c = kzval(kz_int<G>(k), P.kzL);
+                if (deriv == 1) v = imul(v, c);
+                if (deriv == 2) v = cscale(v, kz2val(c));
+            }
+            x[k2] = v;
+        }
+        inv_fft<G>(x, xch, tw, t, gmask);
+#pragma unroll
+        for (int j = 0; j < G::P; ++j) mfr[arr * G::NZ + zpos<G>(t, j)] = x[j].x;
+    }
+}
+
+// Diagnostic contributions of one mode at time t (MHD_BQlin.cpp:365-407):
+// acc[0..5] += mult*{energy_u, energy_b, AM_u, AM_b}, mult*nu*diss_u, mult*eta*diss_b
+template <class G>
+__device__ __forceinline__ void mode_diag(const DevParams& P, const cplx* u, int mode_kxi, int kyi, double kx0,
+                                          double ky, double t, int tt, double* acc) {
+    const double a = kx_at(kx0, P.q, t, ky);
+    const double ab = __dmul_rn(a, ky);
+    const double mult = (ky == 0.0) ? 1.0 : 2.0;
+    (void)mode_kxi;
+#pragma unroll
+    for (int k2 = 0; k2 < G::P; ++k2) {
+        const int k = tt + G::T * k2;
+        const int s = stored_index<G>(k);
+        if (s < 0) continue;
+        const double c = kzval(kz_int<G>(k), P.kzL);
+        const bool z0 = (kyi == 0 && s == 0);
+        const double lap2 = lap2val(ky, kz2val(c), z0);
+        const double il2 = ilap2val(lap2, z0);
+        const double lapF = __dadd_rn(-__dmul_rn(a, a), lap2);
+        const double l2 = __dmul_rn(lapF, il2);
+        cplx f[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) f[v] = ldc_cg(u + v * P.nz + s);
+        const double n0 = f[0].x * f[0].x + f[0].y * f[0].y, n1 = f[1].x * f[1].x + f[1].y * f[1].y;
+        const double n2 = f[2].x * f[2].x + f[2].y * f[2].y, n3 = f[3].x * f[3].x + f[3].y * f[3].y;
+        const double eu = l2 * n0 - il2 * n1, eb = l2 * n2 - il2 * n3;
+        acc[0] += mult * eu;
+        acc[1] += mult * eb;
+        // uy = (ab u + i c zeta) ilap2 (MHD_BQlin.cpp:388-392)
+        cplx uy = cscale(cadd(cscale(f[0], ab), imul(f[1], c)), il2);
+        cplx by = cscale(cadd(cscale(f[2], ab), imul(f[3], c)), il2);
+        acc[2] += mult * (f[0].x * uy.x + f[0].y * uy.y);
+        acc[3] += mult * (f[2].x * by.x + f[2].y * by.y);
+        acc[4] += mult * P.nu * (-lapF * eu);
+        acc[5] += mult * P.eta * (-lapF * eb);
+    }
+}
+
+template <int NZ, int MODEL, int INTEG>
+__global__ void stage_kernel(StageArgs A, DevParams P) {
+    using G = Geom<NZ>;
+    using SM = Smem<G, MODEL>;
+    constexpr int SW = SM::SW;
+    constexpr int NEMF = SM::NEMF;
+    constexpr int PL = SM::PL;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warps = blockDim.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int slot = lane / G::T, t = lane % G::T;
+    const unsigned gmask = (G::T == 32 ? 0xffffffffu : (((1u << G::T) - 1u) << (slot * G::T)));
+    cplx* tw_s = reinterpret_cast<cplx*>(smem_raw);
+    double* mfr = reinterpret_cast<double*>(tw_s + G::NZ);
+    double* spec = mfr + SM::NMFR * G::NZ;
+    cplx* xch_all = reinterpret_cast<cplx*>(spec + 2 * NEMF * (G::H + 1));
+    cplx* priv_all = xch_all + (size_t)warps * SW * G::XSIZE;
+    cplx* xch = xch_all + (size_t)(warp * SW + slot) * G::XSIZE;
+    cplx* priv = priv_all + (size_t)warp * SM::NPRIV * G::P * 32;
+    const int gidx = warp * SW + slot;    // group index in the CTA
+    const int ngc = warps * SW;           // groups per CTA
+    const StageConst& S = A.sc;
+
+    for (int i = tid; i < G::NZ; i += blockDim.x) tw_s[i] = A.tw[i];
+    const double tclock = __ldcg(&A.clk->t);
+    CnOld cn;
+    cn.t_old = __ldcg(&A.clk->t_old);
+    cn.dtlin_old = __ldcg(&A.clk->dtlin_old);
+    cn.old_init = __ldcg(&A.clk->old_init);
+    __syncthreads();
+    mean_profiles<G, MODEL>(P, A.mf, mfr, xch, tw_s, gidx, ngc, t, gmask);
+    __syncthreads();
+
+    // Last-stage bookkeeping identical in every CTA (main.cpp:111-130)
+    const double t_new = __dadd_rn(tclock, P.dt);
+    const bool last = S.last && !A.rhs_only;
+    bool diag_due = false;
+    if (last && P.tv_interval > 0.0) {
+        const double tv = __dadd_rn(__ldcg(&A.clk->timevar), P.dt);
+        diag_due = __dsub_rn(tv, P.tv_interval) > -1e-8;
+    }
+    const double qt = __dmul_rn(P.q, t_new);
+
+    double emfx[G::P], emfy[G::P];
+#pragma unroll
+    for (int j = 0; j < G::P; ++j) { emfx[j] = 0.0; emfy[j] = 0.0; }
+    double dacc[6] = {0, 0, 0, 0, 0, 0};
+
+    const int gid = blockIdx.x * ngc + gidx;
+    const int NG = gridDim.x * ngc;
+    for (int mode = gid; mode < P.nxy; mode += NG) {
+        if (MODEL == MODEL_BQLIN)
+            bqlin_mode<G, INTEG>(A, P, mode, t, gmask, xch, priv, lane, tw_s, mfr, emfx, emfy, tclock, cn);
+        if (last) {
+            // ShearingBox_Remap(q t) after t += dt (main.cpp:122-123, MHD_BQlin.cpp:319-329)
+            double kx0 = A.kx0[mode];
+            const double ky = __ldg(A.ky + mode);
+            bool zeroed = false;
+            if (P.remap) {
+                const double kxt = __dadd_rn(kx0, __dmul_rn(qt, ky));
+                if (kxt > P.remap_thresh) {
+                    zeroed = true;
+                    kx0 = __dsub_rn(kx0, P.remap_shift);
+                    cplx* uo = A.lin_out + (size_t)mode * 4 * P.nz;
+#pragma unroll
+                    for (int k2 = 0; k2 < G::P; ++k2) {
+                        const int s = stored_index<G>(t + G::T * k2);
+                        if (s < 0) continue;
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) stc(uo + v * P.nz + s, mk(0.0, 0.0));
+                    }
+                    __syncwarp(gmask);
+                    if (t == 0) A.kx0[mode] = kx0;
+                }
+            }
+            if (diag_due && !zeroed)
+                mode_diag<G>(P, A.lin_out + (size_t)mode * 4 * P.nz, __ldg(A.kxi + mode), __ldg(A.kyi + mode), kx0,
+                             ky, t_new, t, dacc);
+        }
+    }
+
+    // ---- CTA reduction of the stress profiles and diagnostics (fixed order)
+    __syncthreads();
+    double* red = reinterpret_cast<double*>(priv_all);  // [ngc][NEMF][NZ] then [blockDim][6]
+#pragma unroll
+    for (int j = 0; j < G::P; ++j) {
+        const int z = zpos<G>(t, j);
+        red[(gidx * NEMF + 0) * G::NZ + z] = emfx[j];
+        red[(gidx * NEMF + 1) * G::NZ + z] = emfy[j];
+    }
+    double* dred = red + (size_t)ngc * NEMF * G::NZ;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) dred[tid * 6 + c] = dacc[c];
+    __syncthreads();
+    double* part = A.partials + (size_t)blockIdx.x * PL;
+    for (int idx = tid; idx < NEMF * G::NZ; idx += blockDim.x) {
+        double s = 0.0;
+        for (int g = 0; g < ngc; ++g) s += red[g * NEMF * G::NZ + idx];
+        part[idx] = s;
+    }
+    if (tid < 6) {
+        double s = 0.0;
+        for (int r = 0; r < (int)blockDim.x; ++r) s += dred[r * 6 + tid];
+        part[NEMF * G::NZ + tid] = s;
+    }
+
+    // ---- two-level last-arriver reduction
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    const int ngroups = (gridDim.x + RED_GROUP - 1) / RED_GROUP;
+    const int grp = blockIdx.x / RED_GROUP;
+    const int c0 = grp * RED_GROUP;
+    const int cn_in = min(RED_GROUP, (int)gridDim.x - c0);
+    if (tid == 0) {
+        unsigned tk = atomicAdd(&A.clk->cnt_group[grp], 1u);
+        s_last = (tk == (unsigned)(cn_in - 1));
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double* gpart = A.gpartials + (size_t)grp * PL;
+    for (int idx = tid; idx < PL; idx += blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < cn_in; ++c) s += __ldcg(A.partials + (size_t)(c0 + c) * PL + idx);
+        gpart[idx] = s;
+    }
+    if (tid == 0) A.clk->cnt_group[grp] = 0u;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+        unsigned tk = atomicAdd(&A.clk->cnt_top, 1u);
+        s_last = (tk == (unsigned)(ngroups - 1));
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double* tot = red;  // reuse: [PL]
+    for (int idx = tid; idx < PL; idx += blockDim.x) {
+        double s = 0.0;
+        for (int g = 0; g < ngroups; ++g) s += __ldcg(A.gpartials + (size_t)g * PL + idx);
+        tot[idx] = s;
+    }
+    if (tid == 0) A.clk->cnt_top = 0u;
+    __syncthreads();
+
+    // ---- mean-field stage (top CTA only)
+    // Stress spectra: fwd of the real profiles, half spectrum k = 0..H
+    // (MHD_BQlin.cpp:228-240 after the sum over modes; linear, so one transform)
+    for (int e = gidx; e < NEMF; e += ngc) {
+        cplx x[G::P];
+#pragma unroll
+        for (int j = 0; j < G::P; ++j) x[j] = mk(tot[e * G::NZ + zpos<G>(t, j)], 0.0);
+        fwd_fft<G>(x, xch, tw_s, t, gmask);
+#pragma unroll
+        for (int k2 = 0; k2 < G::P; ++k2) {
+            const int k = t + G::T * k2;
+            if (k <= G::H) {
+                cplx v = cscale(x[k2], P.rs_fac);
+                if (MODEL == MODEL_BQLIN || e < 2) v = imul(v, kzval(k, P.kzL));  // times kz (z derivative)
+                spec[(e * (G::H + 1) + k) * 2 + 0] = v.x;
+                spec[(e * (G::H + 1) + k) * 2 + 1] = v.y;
+            }
+        }
+    }
+    __syncthreads();
+    const int nzd = P.nz;
+    for (int s = tid; s < nzd; s += blockDim.x) {
+        // unpack: full[s] = half[s] (s <= H) or conj(half[nz - s]) (MHD_BQlin.cpp:264-267)
+        cplx drive[NEMF];
+#pragma unroll
+        for (int e = 0; e < NEMF; ++e) {
+            const int hs = s <= G::H ? s : nzd - s;
+            cplx v = mk(spec[(e * (G::H + 1) + hs) * 2], spec[(e * (G::H + 1) + hs) * 2 + 1]);
+            drive[e] = s <= G::H ? v : conjc(v);
+        }
+        const int kzi = s <= G::H ? s : s - nzd;
+        const double c = kzval(kzi, P.kzL);
+        const double kz2 = kz2val(c);
+        cplx m[4], F[4];
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) m[mm] = (mm < P.nmf) ? ldc_cg(A.mf + mm * nzd + s) : mk(0.0, 0.0);
+        if (MODEL == MODEL_BQLIN) {
+            // dBy = -q Bx + EMF_y, dBx = EMF_x (MHD_BQlin.cpp:274-280)
+            F[0] = P.ql ? drive[0] : mk(0.0, 0.0);
+            F[1] = P.ql ? cadd(cscale(m[0], -P.q), drive[1]) : mk(0.0, 0.0);
+        }
+        for (int mm = 0; mm < P.nmf; ++mm) {
+            if (A.rhs_only) {
+                stc(A.Fmf_out + mm * nzd + s, F[mm]);
+                continue;
+            }
+            const double Lm = P.ql ? __dmul_rn((MODEL == MODEL_FULLQLIN && mm >= 2) ? P.nu : P.eta, kz2) : 0.0;
+            cplx fp = S.has_prev ? ldc_cg(A.Fmf_prev + mm * nzd + s) : mk(0.0, 0.0);
+            cplx nv = rk_update<INTEG>(S, Lm, Lm, F[mm], fp, m[mm], S.has_prev);
+            if (A.Fmf_out) stc(A.Fmf_out + mm * nzd + s, F[mm]);
+            stc(A.mf + mm * nzd + s, nv);
+            const double mag = nv.x * nv.x + nv.y * nv.y;
+            if (!(mag == mag) || isinf(mag)) atomicOr(&A.clk->status, QLGPU_STATUS_NONFINITE);
+            else if (mag > 1e40) atomicOr(&A.clk->status, QLGPU_STATUS_UNSTABLE);
+        }
+    }
+    __syncthreads();
+    if (A.rhs_only) return;
+    if (tid == 0) {
+        DevClock* C = A.clk;
+        // CN bookkeeping: this stage's operator time becomes "old" (RK3CN.cpp:119-122)
+        C->t_old = S.abs_time ? S.t_off : __dadd_rn(tclock, S.t_off);
+        C->dtlin_old = S.dt_lin;
+        C->old_init = 0;
+        if (last) {
+            C->t = t_new;
+            C->timevar = __dadd_rn(C->timevar, P.dt);
+            C->since += 1;
+            if (diag_due) {
+                // Calc_Energy_AM_Diss (MHD_BQlin.cpp:408-477)
+                double eMB = 0, aMB = 0, dMB = 0, eMU = 0, aMU = 0, dMU = 0;
+                for (int s = 0; s < nzd; ++s) {
+                    const int kzi = s <= G::H ? s : s - nzd;
+                    const double kz2 = kz2val(kzval(kzi, P.kzL));
+                    cplx b0 = ldc_cg(A.mf + s), b1 = ldc_cg(A.mf + nzd + s);
+                    eMB += (b0.x * b0.x + b0.y * b0.y) + (b1.x * b1.x + b1.y * b1.y);
+                    aMB += b0.x * b1.x + b0.y * b1.y;
+                    dMB += -kz2 * (b0.x * b0.x + b0.y * b0.y) - kz2 * (b1.x * b1.x + b1.y * b1.y);
+                    if (P.nmf == 4) {
+                        cplx u0 = ldc_cg(A.mf + 2 * nzd + s), u1 = ldc_cg(A.mf + 3 * nzd + s);
+                        eMU += (u0.x * u0.x + u0.y * u0.y) + (u1.x * u1.x + u1.y * u1.y);
+                        aMU += u0.x * u1.x + u0.y * u1.y;
+                        dMU += -kz2 * (u0.x * u0.x + u0.y * u0.y) - kz2 * (u1.x * u1.x + u1.y * u1.y);
+                    }
+                }
+                eMB *= P.divMF; eMU *= P.divMF; aMB *= P.divMF; aMU *= P.divMF;
+                dMB *= P.divMF * P.eta; dMU *= P.divMF * P.nu;
+                const double* ds = tot + NEMF * G::NZ;
+                const double eu = ds[0] * P.divfac, eb = ds[1] * P.divfac;
+                const double au = ds[2] * P.divfac, abv = ds[3] * P.divfac;
+                const double du = ds[4] * P.divfac, db = ds[5] * P.divfac;
+                const int r = C->ndiag;
+                if (r < A.diag_cap) {
+                    double* o = A.diag_ring + (size_t)r * 15;
+                    o[0] = t_new;
+                    o[1] = eMU / 2; o[2] = eMB / 2; o[3] = eu / 2; o[4] = eb / 2;
+                    o[5] = aMU; o[6] = aMB; o[7] = au; o[8] = abv;
+                    o[9] = dMU; o[10] = dMB; o[11] = du; o[12] = db;
+                    o[13] = pow(P.nu * P.nu * P.nu / (dMU + du), 0.25) * P.kzmax;
+                    o[14] = pow(P.eta * P.eta * P.eta / (dMB + db), 0.25) * P.kzmax;
+                } else {
+                    C->status |= QLGPU_STATUS_DIAG_FULL;
+                }
+                C->ndiag = r + 1;
+                C->timevar = __dsub_rn(C->timevar, P.tv_interval);
+                C->since = 0;
+            }
+        }
+    }
+}
+
+// Diagnostics of the current state without stepping (the initial record,
+// main.cpp:98-103).  One CTA, fixed-order reduction.
+template <int NZ>
+__global__ void diag_kernel(const cplx* lin, const cplx* mf, const double* kx0, const double* ky, const int* kxi,
+                            const int* kyi, DevParams P, double t, double* out) {
+    using G = Geom<NZ>;
+    __shared__ double red[1024 * 6 / 8];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const int groups = blockDim.x / G::T;
+    const int g = threadIdx.x / G::T, tt = threadIdx.x % G::T;
+    for (int mode = g; mode < P.nxy; mode += groups)
+        mode_diag<G>(P, lin + (size_t)mode * 4 * P.nz, kxi[mode], kyi[mode], kx0[mode], ky[mode], t, tt, acc);
+    // reduce: blockDim <= 128 keeps red within 768 doubles
+    for (int c = 0; c < 6; ++c) red[threadIdx.x * 6 + c] = acc[c];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ds[6] = {0, 0, 0, 0, 0, 0};
+        for (int r = 0; r < (int)blockDim.x; ++r)
+            for (int c = 0; c < 6; ++c) ds[c] += red[r * 6 + c];
+        const int nzd = P.nz;
+        double eMB = 0, aMB = 0, dMB = 0, eMU = 0, aMU = 0, dMU = 0;
+        for (int s = 0; s < nzd; ++s) {
+            const int kzi = s <= G::H ? s : s - nzd;
+            const double kz2 = kz2val(kzval(kzi, P.kzL));
+            cplx b0 = mf[s], b1 = mf[nzd + s];
+            eMB += (b0.x * b0.x + b0.y * b0.y) + (b1.x * b1.x + b1.y * b1.y);
+            aMB += b0.x * b1.x + b0.y * b1.y;
+            dMB += -kz2 * (b0.x * b0.x + b0.y * b0.y) - kz2 * (b1.x * b1.x + b1.y * b1.y);
+            if (P.nmf == 4) {
+                cplx u0 = mf[2 * nzd + s], u1 = mf[3 * nzd + s];
+                eMU += (u0.x * u0.x + u0.y * u0.y) + (u1.x * u1.x + u1.y * u1.y);
+                aMU += u0.x * u1.x + u0.y * u1.y;
+                dMU += -kz2 * (u0.x * u0.x + u0.y * u0.y) - kz2 * (u1.x * u1.x + u1.y * u1.y);
+            }
+        }
+        eMB *= P.divMF; eMU *= P.divMF; aMB *= P.divMF; aMU *= P.divMF;
+        dMB *= P.divMF * P.eta; dMU *= P.divMF * P.nu;
+        const double eu = ds[0] * P.divfac, eb = ds[1] * P.divfac;
+        const double au = ds[2] * P.divfac, abv = ds[3] * P.divfac;
+        const double du = ds[4] * P.divfac, db = ds[5] * P.divfac;
+        out[0] = t;
+        out[1] = eMU / 2; out[2] = eMB / 2; out[3] = eu / 2; out[4] = eb / 2;
+        out[5] = aMU; out[6] = aMB; out[7] = au; out[8] = abv;
+        out[9] = dMU; out[10] = dMB; out[11] = du; out[12] = db;
+        out[13] = pow(P.nu * P.nu * P.nu / (dMU + du), 0.25) * P.kzmax;
+        out[14] = pow(P.eta * P.eta * P.eta / (dMB + db), 0.25) * P.kzmax;
+    }
+}
+
+}  // namespace qlgpu

@@ -1,0 +1,89 @@
+// qlgpu_types.h -- device-side parameter and argument blocks shared by the
+// host code (qlgpu.cu) and the stage kernels (qlgpu_stage.cuh).
+#pragma once
+
+namespace qlgpu {
+
+struct cplx;
+
+enum { MODEL_BQLIN = 0, MODEL_FULLQLIN = 1 };
+enum { INTEG_EXP = 0, INTEG_CN = 1 };
+
+// Run constants, fixed for a handle.
+struct DevParams {
+    int nxy, nz, NZ, nmf;
+    double q;       // shear
+    double Omega;   // rotation: 2q/3 for MHD_BQlin (MHD_BQlin.cpp:19), input omega for FullQlin
+    double nu, eta, etanu;  // etanu = eta/nu (MHD_BQlin.cpp:251)
+    double B0z;
+    int visc_half;  // viscosity_order/2 (integer division, MHD_FullQlin.cpp:372)
+    int ql;         // QuasiLinear?
+    int remap;      // Remap?
+    double kzL;     // 2 pi / Lz
+    double fac;     // 1/NZ (fftwPlans.cpp:30)
+    double rs_fac;  // 1/(Ny Nx)^2 (MHD_BQlin.cpp:56)
+    double divfac;  // Lz/(Nx Ny NZ)^2 (MHD_BQlin.cpp:420)
+    double divMF;   // Lz/NZ^2 (MHD_BQlin.cpp:434)
+    double remap_thresh;  // (Nx-1)/2.0 * kxLfac (MHD_BQlin.cpp:322)
+    double remap_shift;   // (Nx-1) * kxLfac     (MHD_BQlin.cpp:324)
+    double dt;
+    double tv_interval;   // diagnostic interval (<= 0: none)
+    double kzmax;         // 2 pi/Lz * (NZ/3) for etaK (MHD_BQlin.cpp:476)
+};
+
+// Mutable per-handle clock and reduction state, in device memory.
+struct DevClock {
+    double t;          // current time (t += dt after each step, main.cpp:116)
+    double timevar;    // SP.timevar_t accumulator (main.cpp:117,127-130)
+    double t_old;      // CN: time at which the previous stage's operator was evaluated
+    double dtlin_old;  // CN: dt_lin of the previous stage
+    int old_init;      // CN: 1 -> the old operator is linearOPs_Init(t0) (RK3CN.cpp:57)
+    int ndiag;         // diagnostic records written
+    int since;         // steps since the last diagnostic record
+    int status;        // error bits (QLGPU_STATUS_*)
+    unsigned cnt_top;
+    unsigned pad;
+    unsigned cnt_group[64];
+};
+
+// Coefficients of one stage (RK3CN_Elin.cpp:89-91,122-125,155-158;
+// RK3CN.cpp:92-94,...).
+struct StageConst {
+    double t_off;     // stage time = t + t_off (dt*{0, p1, p2})
+    double dt_lin;    // operators evaluated at t_s + dt_lin
+    double linC;      // dt*(a+b) (exp) or dt/2*(a+b) (CN)
+    double n1, n2;    // a*dt, b*dt
+    int has_prev;     // stage uses F of the previous stage
+    int last;         // last stage of the step: advance time, remap, diagnostics
+    int abs_time;     // Model::rhs mode: stage time is t_off itself
+    int pad;
+};
+
+struct StageArgs {
+    const cplx* lin_in;
+    cplx* lin_out;
+    const cplx* Fprev;
+    cplx* Fout;
+    cplx* mf;               // mean fields, updated in place by the top CTA
+    const cplx* Fmf_prev;
+    cplx* Fmf_out;
+    double* kx0;            // unsheared kx per mode (Kdata::kx), updated by remap
+    const double* ky;
+    const int* kxi;
+    const int* kyi;
+    const cplx* tw;  // twiddles exp(2 pi i n2 t/NZ), [P][T]
+    double* partials;       // [grid][PL]
+    double* gpartials;      // [ngroups][PL]
+    DevClock* clk;
+    double* diag_ring;      // [diag_cap][15]
+    int diag_cap;
+    int rhs_only;           // Model::rhs: write F (and linop) only, no update
+    double* linop_out;      // rhs_only: [nxy][4][nz]
+    StageConst sc;
+};
+
+}  // namespace qlgpu
+
+#define QLGPU_STATUS_NONFINITE 1   // solution::Check_Solution NaN/Inf (solution.cpp:194)
+#define QLGPU_STATUS_UNSTABLE 2    // |mean field| > 1e20 (solution.cpp:184)
+#define QLGPU_STATUS_DIAG_FULL 4   // diagnostic ring overflowed (records dropped)
