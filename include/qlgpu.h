@@ -89,6 +89,12 @@ int qlgpu_get_state_device(qlgpu_t* h, double* t, void* lin, void* mf, void* kx0
  * receives the count.  diag_out may be NULL when diag_every <= 0. */
 int qlgpu_step(qlgpu_t* h, int nsteps, int diag_every, double* diag_out, int max_diag, int* ndiag);
 
+/* One step (as qlgpu_step with diag_every = 0) with a CUDA event pair around
+ * each of its three stage launches on the handle's stream; stage_ms[3]
+ * receives the device time of each stage kernel.  Profiling aid standing in
+ * for the reference's clock() accumulators (QL_DNS/Auxiliary/TimeVariables.h:51-54). */
+int qlgpu_step_timed(qlgpu_t* h, float* stage_ms);
+
 /* Calc_Energy_AM_Diss at the current time without stepping (15 doubles as
  * above): the initial record of main.cpp:98-103. */
 int qlgpu_diagnostics(qlgpu_t* h, double* out15);
@@ -104,6 +110,12 @@ int qlgpu_rhs(qlgpu_t* h, double t, double dt_lin, const double* lin_in, const d
  * bit 1 non-finite mean field, bit 2 |mean field| > 1e20, bit 4 diagnostic
  * records dropped.  Reading does not clear it; set_state clears it. */
 int qlgpu_status(qlgpu_t* h, int* status);
+
+/* Profiling aid: with QLGPU_TRACE=1 in the environment at qlgpu_create, each
+ * stage kernel records %globaltimer stamps (ns) of its phases; out96 receives
+ * 3 stages x 32 slots of the most recent step (slot meanings are listed in
+ * ql_dns_b200/csrc/qlgpu_kernel.cuh).  Returns QLGPU_ERR_UNSUPPORTED when off. */
+int qlgpu_trace(qlgpu_t* h, unsigned long long* out96);
 
 /* Current simulation time and the CUDA stream (cudaStream_t) of the handle. */
 int qlgpu_time(qlgpu_t* h, double* t);

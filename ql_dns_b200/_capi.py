@@ -19,8 +19,9 @@ ERRORS = {1: "QLGPU_ERR_ARG", 2: "QLGPU_ERR_UNSUPPORTED", 3: "QLGPU_ERR_CUDA", 4
 
 # Every symbol include/qlgpu.h declares.
 EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "qlgpu_get_state",
-           "qlgpu_set_state_device", "qlgpu_get_state_device", "qlgpu_step", "qlgpu_diagnostics",
-           "qlgpu_rhs", "qlgpu_status", "qlgpu_time", "qlgpu_stream", "qlgpu_last_error", "qlgpu_version"]
+           "qlgpu_set_state_device", "qlgpu_get_state_device", "qlgpu_step", "qlgpu_step_timed", "qlgpu_diagnostics",
+           "qlgpu_rhs", "qlgpu_status", "qlgpu_time", "qlgpu_trace", "qlgpu_stream", "qlgpu_last_error",
+           "qlgpu_version"]
 
 
 class qlgpu_params(ctypes.Structure):
@@ -64,10 +65,12 @@ def load(path: str = LIB_PATH):
     L.qlgpu_set_state_device.argtypes = [vp, ctypes.c_double, vp, vp, vp]
     L.qlgpu_get_state_device.argtypes = [vp, dp, vp, vp, vp]
     L.qlgpu_step.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ip]
+    L.qlgpu_step_timed.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     L.qlgpu_diagnostics.argtypes = [vp, dp]
     L.qlgpu_rhs.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp, dp]
     L.qlgpu_status.argtypes = [vp, ip]
     L.qlgpu_time.argtypes = [vp, dp]
+    L.qlgpu_trace.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
     L.qlgpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.qlgpu_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.qlgpu_version.restype = ctypes.c_char_p

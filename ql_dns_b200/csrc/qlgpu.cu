@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -29,19 +30,28 @@ typedef void (*stage_launch_fn)(const StageArgs&, const DevParams&, int grid, in
 typedef void (*diag_launch_fn)(const cplx*, const cplx*, const double*, const double*, const int*, const int*,
                                const DevParams&, double, double*, cudaStream_t);
 typedef size_t (*smem_fn)(int warps);
+typedef int (*tmem_fn)(int warps);
 typedef const void* (*kptr_fn)();
 
-template <int NZ, int MODEL, int INTEG>
+template <int NZ, int MODEL, int INTEG, bool TM>
 void launch_stage(const StageArgs& A, const DevParams& P, int grid, int block, size_t smem, cudaStream_t st) {
-    stage_kernel<NZ, MODEL, INTEG><<<grid, block, smem, st>>>(A, P);
+    stage_kernel<NZ, MODEL, INTEG, TM><<<grid, block, smem, st>>>(A, P);
 }
-template <int NZ, int MODEL, int INTEG>
+template <int NZ, int MODEL, int INTEG, bool TM>
 const void* stage_ptr() {
-    return reinterpret_cast<const void*>(&stage_kernel<NZ, MODEL, INTEG>);
+    return reinterpret_cast<const void*>(&stage_kernel<NZ, MODEL, INTEG, TM>);
 }
-template <int NZ, int MODEL>
+template <int NZ, int MODEL, bool TM>
 size_t stage_smem(int warps) {
-    return Smem<Geom<NZ>, MODEL>::bytes(warps);
+    using G = Geom<NZ>;
+    using Priv = typename std::conditional<TM, PrivTmem<G, PB_COUNT>, PrivSmem<G, PB_COUNT>>::type;
+    return Smem<G, MODEL, Priv>::bytes(warps);
+}
+template <int NZ, int MODEL, bool TM>
+int stage_tmem(int warps) {
+    using G = Geom<NZ>;
+    using Priv = typename std::conditional<TM, PrivTmem<G, PB_COUNT>, PrivSmem<G, PB_COUNT>>::type;
+    return Smem<G, MODEL, Priv>::tmem_cols(warps);
 }
 template <int NZ>
 void launch_diag(const cplx* lin, const cplx* mf, const double* kx0, const double* ky, const int* kxi, const int* kyi,
@@ -53,30 +63,37 @@ struct Variant {
     stage_launch_fn launch;
     kptr_fn kernel;
     smem_fn smem;
+    tmem_fn tmem;
     diag_launch_fn diag;
     int T;   // threads per mode
     int PL;  // partial vector length
 };
 
-template <int NZ, int MODEL, int INTEG>
+template <int NZ, int MODEL, int INTEG, bool TM>
 Variant make_variant() {
     Variant v;
-    v.launch = &launch_stage<NZ, MODEL, INTEG>;
-    v.kernel = &stage_ptr<NZ, MODEL, INTEG>;
-    v.smem = &stage_smem<NZ, MODEL>;
+    v.launch = &launch_stage<NZ, MODEL, INTEG, TM>;
+    v.kernel = &stage_ptr<NZ, MODEL, INTEG, TM>;
+    v.smem = &stage_smem<NZ, MODEL, TM>;
+    v.tmem = &stage_tmem<NZ, MODEL, TM>;
     v.diag = &launch_diag<NZ>;
     v.T = Geom<NZ>::T;
-    v.PL = Smem<Geom<NZ>, MODEL>::PL;
+    v.PL = (MODEL == MODEL_BQLIN ? 2 : 4) * NZ + 8;
     return v;
 }
 
-bool pick_variant(int NZ, int model, int integ, Variant* out) {
-#define QLGPU_CASE(NZV)                                                                         \
-    if (NZ == NZV) {                                                                            \
-        if (model == MODEL_BQLIN && integ == INTEG_EXP) *out = make_variant<NZV, MODEL_BQLIN, INTEG_EXP>(); \
-        else if (model == MODEL_BQLIN && integ == INTEG_CN) *out = make_variant<NZV, MODEL_BQLIN, INTEG_CN>(); \
-        else return false;                                                                      \
-        return true;                                                                            \
+// QLGPU_PRIV_SMEM=1 in the environment selects the shared-memory private store
+// instead of tensor memory (a debugging / comparison switch).
+bool pick_variant(int NZ, int model, int integ, bool tm, Variant* out) {
+#define QLGPU_CASE(NZV)                                                                                          \
+    if (NZ == NZV) {                                                                                             \
+        if (model == MODEL_BQLIN && integ == INTEG_EXP)                                                          \
+            *out = tm ? make_variant<NZV, MODEL_BQLIN, INTEG_EXP, true>() : make_variant<NZV, MODEL_BQLIN, INTEG_EXP, false>(); \
+        else if (model == MODEL_BQLIN && integ == INTEG_CN)                                                      \
+            *out = tm ? make_variant<NZV, MODEL_BQLIN, INTEG_CN, true>() : make_variant<NZV, MODEL_BQLIN, INTEG_CN, false>(); \
+        else                                                                                                     \
+            return false;                                                                                        \
+        return true;                                                                                             \
     }
     QLGPU_CASE(16)
     QLGPU_CASE(32)
@@ -115,10 +132,15 @@ struct qlgpu_handle {
     int diag_cap = 0;
     double* d_out15 = nullptr;
     double* d_linop = nullptr;
+    double* d_ilap2 = nullptr;
+    int tmem_cols = 0;
+    unsigned long long* d_trace = nullptr;  // QLGPU_TRACE=1: %globaltimer stamps of each stage
     int grid = 0, warps = 4, block = 128;
     size_t smem = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<double> kx_tab, ky_tab;
     std::vector<int> kxi_tab, kyi_tab;
+    std::vector<double> il2_tab;
     std::string err;
 };
 
@@ -182,16 +204,19 @@ StageArgs base_args(qlgpu_t* h) {
     A.kxi = h->d_kxi;
     A.kyi = h->d_kyi;
     A.tw = h->d_tw;
+    A.ilap2 = h->d_ilap2;
     A.partials = h->d_partials;
     A.gpartials = h->d_gpartials;
     A.clk = h->d_clk;
     A.diag_ring = h->d_diag;
     A.diag_cap = h->diag_cap;
+    A.trace = h->d_trace;
     return A;
 }
 
 // One RK3 step = three stage launches (RK3CN_Elin::Step / RK3CN::Step).
-void enqueue_step(qlgpu_t* h) {
+// ev (optional): 4 events recorded before stage 1 and after each stage.
+void enqueue_step(qlgpu_t* h, cudaEvent_t* ev = nullptr) {
     const double dt = h->p.dt;
     const bool cn = h->p.integrator == INTEG_CN;
     const double lcf = cn ? dt / 2 : dt;
@@ -207,6 +232,7 @@ void enqueue_step(qlgpu_t* h) {
     const cplx* Fprev[3] = {nullptr, h->d_F1, h->d_F2};
     cplx* Fmf[3] = {h->d_Fmf1, h->d_Fmf2, h->d_Fmf1};
     const cplx* Fmfp[3] = {nullptr, h->d_Fmf1, h->d_Fmf2};
+    if (ev) cudaEventRecord(ev[0], h->stream);
     for (int s = 0; s < 3; ++s) {
         StageArgs A = base_args(h);
         A.lin_in = h->d_lin[h->cur];
@@ -222,7 +248,9 @@ void enqueue_step(qlgpu_t* h) {
         A.sc.n2 = st[s].n2;
         A.sc.has_prev = st[s].has_prev;
         A.sc.last = (s == 2);
+        if (A.trace) A.trace += 32 * s;
         h->var.launch(A, h->dp, h->grid, h->block, h->smem, h->stream);
+        if (ev) cudaEventRecord(ev[s + 1], h->stream);
         h->cur ^= 1;
     }
 }
@@ -273,7 +301,9 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
     if (p.model == QLGPU_MODEL_MHD_BQLIN && p.nu == 0.0)
         return fail(nullptr, QLGPU_ERR_ARG, "MHD_BQlin divides by nu (MHD_BQlin.cpp:251); nu must be nonzero");
     Variant var;
-    if (!pick_variant(p.NZ, p.model, p.integrator, &var))
+    const char* ps = std::getenv("QLGPU_PRIV_SMEM");
+    const bool use_tmem = !(ps && ps[0] == '1');
+    if (!pick_variant(p.NZ, p.model, p.integrator, use_tmem, &var))
         return fail(nullptr, QLGPU_ERR_UNSUPPORTED,
                     "unsupported (NZ, model): NZ must be a power of two in [16, 256]; model built: MHD_BQlin");
     int ndev = 0;
@@ -337,7 +367,9 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
         h->err = "cudaGetDeviceProperties failed";
         return bail(QLGPU_ERR_CUDA);
     }
+    // 4 warps per CTA when the shared-memory footprint allows, else fewer
     h->warps = 4;
+    while (h->warps > 1 && var.smem(h->warps) > (size_t)prop.sharedMemPerBlockOptin) h->warps >>= 1;
     h->block = 32 * h->warps;
     h->smem = var.smem(h->warps);
     if (cudaFuncSetAttribute(var.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem) != cudaSuccess) {
@@ -346,6 +378,8 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
     }
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, var.kernel(), h->block, h->smem);
+    h->tmem_cols = var.tmem(h->warps);
+    if (h->tmem_cols > 0 && per_sm > 512 / h->tmem_cols) per_sm = 512 / h->tmem_cols;  // TMEM: 512 columns per SM
     if (per_sm < 1) per_sm = 1;
     const int groups_per_cta = h->warps * (32 / var.T);
     int need = (h->nxy + groups_per_cta - 1) / groups_per_cta;
@@ -382,7 +416,7 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
     QLGPU_ALLOC(h->d_gpartials, (size_t)ngroups * var.PL * sizeof(double));
     QLGPU_ALLOC(h->d_clk, sizeof(DevClock));
     QLGPU_ALLOC(h->d_out15, 15 * sizeof(double));
-#undef QLGPU_ALLOC
+    QLGPU_ALLOC(h->d_ilap2, (size_t)(p.ny / 2) * h->nz * sizeof(double));
     // Twiddles tw[n2*T + t] = exp(+2 pi i n2 t/NZ)
     std::vector<cplx> tw(h->NZ);
     const int T = var.T, P = h->NZ / T;
@@ -394,10 +428,37 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
             tw[n2 * T + t].y = std::sin(ang);
         }
     cudaMemcpyAsync(h->d_tw, tw.data(), tw.size() * sizeof(cplx), cudaMemcpyHostToDevice, h->stream);
+    // 1/lap2 per (ky index, stored kz), Kdata.cpp:100-119 (kept for the lifetime of the handle)
+    h->il2_tab.assign((size_t)(p.ny / 2) * h->nz, 0.0);
+    {
+        const double kyL = 2 * kPI / p.L[1], kzL = 2 * kPI / p.L[2];
+        const int nzl = (h->nz - 1) / 2;
+        for (int j = 0; j < p.ny / 2; ++j) {
+            const double kyr = j * kyL;
+            for (int s = 0; s < h->nz; ++s) {
+                const int kzi = s <= nzl ? s : (-2 * nzl + s - 1);
+                const double c = kzi * kzL;
+                const double kz2 = 0.0 * 0.0 - c * c;
+                double l2 = -kyr * kyr + kz2;
+                double il2 = 1 / l2;
+                if (kyr == 0 && s == 0) il2 = 1;
+                h->il2_tab[(size_t)j * h->nz + s] = il2;
+            }
+        }
+    }
+    cudaMemcpyAsync(h->d_ilap2, h->il2_tab.data(), h->il2_tab.size() * sizeof(double), cudaMemcpyHostToDevice,
+                    h->stream);
     cudaMemcpyAsync(h->d_kx0, h->kx_tab.data(), h->nxy * sizeof(double), cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->d_ky, h->ky_tab.data(), h->nxy * sizeof(double), cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->d_kxi, h->kxi_tab.data(), h->nxy * sizeof(int), cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->d_kyi, h->kyi_tab.data(), h->nxy * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    {
+        const char* tr = std::getenv("QLGPU_TRACE");
+        if (tr && tr[0] == '1') {
+            QLGPU_ALLOC(h->d_trace, 3 * 32 * sizeof(unsigned long long));
+        }
+    }
+#undef QLGPU_ALLOC
     rc = reset_clock(h, 0.0);
     if (rc) return bail(rc);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
@@ -414,9 +475,11 @@ int qlgpu_destroy(qlgpu_t* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     void* bufs[] = {h->d_lin[0], h->d_lin[1], h->d_F1, h->d_F2, h->d_mf, h->d_Fmf1, h->d_Fmf2,
                     h->d_kx0, h->d_ky, h->d_kxi, h->d_kyi, h->d_tw, h->d_partials, h->d_gpartials,
-                    h->d_clk, h->d_diag, h->d_out15, h->d_linop};
+                    h->d_clk, h->d_diag, h->d_out15, h->d_linop, h->d_ilap2, h->d_trace};
     for (void* b : bufs)
         if (b) cudaFree(b);
+    for (cudaEvent_t e : h->ev)
+        if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return QLGPU_OK;
@@ -519,6 +582,23 @@ int qlgpu_step(qlgpu_t* h, int nsteps, int diag_every, double* diag_out, int max
     return QLGPU_OK;
 }
 
+int qlgpu_step_timed(qlgpu_t* h, float* stage_ms) {
+    if (!h || !stage_ms) return QLGPU_ERR_ARG;
+    QLGPU_CK(cudaSetDevice(h->device));
+    for (int i = 0; i < 4; ++i)
+        if (!h->ev[i]) QLGPU_CK(cudaEventCreate(&h->ev[i]));
+    h->dp.tv_interval = 0.0;
+    enqueue_step(h, h->ev);
+    int rc = check_launch(h);
+    if (rc) return rc;
+    QLGPU_CK(cudaEventSynchronize(h->ev[3]));
+    for (int s = 0; s < 3; ++s) QLGPU_CK(cudaEventElapsedTime(&stage_ms[s], h->ev[s], h->ev[s + 1]));
+    int st = 0;
+    QLGPU_CK(cudaMemcpy(&st, &h->d_clk->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE)) return fail(h, QLGPU_ERR_STATUS, "device status set");
+    return QLGPU_OK;
+}
+
 int qlgpu_diagnostics(qlgpu_t* h, double* out15) {
     if (!h || !out15) return QLGPU_ERR_ARG;
     QLGPU_CK(cudaSetDevice(h->device));
@@ -576,6 +656,15 @@ int qlgpu_time(qlgpu_t* h, double* t) {
     if (!h || !t) return QLGPU_ERR_ARG;
     QLGPU_CK(cudaSetDevice(h->device));
     QLGPU_CK(cudaMemcpyAsync(t, &h->d_clk->t, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_trace(qlgpu_t* h, unsigned long long* out96) {
+    if (!h || !out96) return QLGPU_ERR_ARG;
+    if (!h->d_trace) return fail(h, QLGPU_ERR_UNSUPPORTED, "tracing is off (set QLGPU_TRACE=1 before qlgpu_create)");
+    QLGPU_CK(cudaSetDevice(h->device));
+    QLGPU_CK(cudaMemcpyAsync(out96, h->d_trace, 96 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
     QLGPU_CK(cudaStreamSynchronize(h->stream));
     return QLGPU_OK;
 }

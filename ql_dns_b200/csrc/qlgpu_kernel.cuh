@@ -2,6 +2,8 @@
 // per-mode loop, the remap / diagnostics epilogue, the fixed-order two-level
 // reduction over CTAs and the mean-field update done by the last CTA.
 #pragma once
+#include <type_traits>
+
 #include "qlgpu_stage.cuh"
 
 namespace qlgpu {
@@ -14,7 +16,7 @@ constexpr int RED_GROUP = 16;  // CTAs per first-level reduction group
 template <class G, int MODEL>
 __device__ __forceinline__ void mean_profiles(const DevParams& P, const cplx* mf, double* mfr, cplx* xch, const cplx* tw,
                                               int gidx, int ngroups, int t, unsigned gmask) {
-    constexpr int NMFR = Smem<G, MODEL>::NMFR;
+    constexpr int NMFR = MODEL == MODEL_BQLIN ? 3 : 8;
     for (int arr = gidx; arr < NMFR; arr += ngroups) {
         int src, deriv;
         if (MODEL == MODEL_BQLIN) {
@@ -82,28 +84,240 @@ __device__ __forceinline__ void mode_diag(const DevParams& P, const cplx* u, int
     }
 }
 
-template <int NZ, int MODEL, int INTEG>
-__global__ void stage_kernel(StageArgs A, DevParams P) {
+// ---------------------------------------------------------------------------
+// Mean-field stage, run by the CTA that arrives last: stress spectra, the
+// mean-field right-hand side and RK update, the time / diagnostic bookkeeping.
+// tot[] holds the stress profiles summed over all modes (real z) followed by
+// the six fluctuation diagnostic sums.
+// ---------------------------------------------------------------------------
+template <class G, int MODEL, int INTEG, int NEMF>
+__device__ __forceinline__ void mean_field_stage(const StageArgs& A, const DevParams& P, const double* tot,
+                                                 double* spec, cplx* xch, const cplx* tw_s, int gidx, int ngc, int t,
+                                                 unsigned gmask, double tclock, double t_new, bool last,
+                                                 bool diag_due) {
+    const StageConst& S = A.sc;
+    const int tid = threadIdx.x;
+    const int nzd = P.nz;
+    // Forward transform of each summed profile, half spectrum k = 0..H
+    // (MHD_BQlin.cpp:228-240 after the sum over modes; the transform is linear)
+    for (int e = gidx; e < NEMF; e += ngc) {
+        cplx x[G::P];
+#pragma unroll
+        for (int j = 0; j < G::P; ++j) x[j] = mk(tot[e * G::NZ + zpos<G>(t, j)], 0.0);
+        fwd_fft<G>(x, xch, tw_s, t, gmask);
+#pragma unroll
+        for (int k2 = 0; k2 < G::P; ++k2) {
+            const int k = t + G::T * k2;
+            if (k <= G::H) {
+                cplx v = cscale(x[k2], P.rs_fac);
+                if (MODEL == MODEL_BQLIN || e < 2) v = imul(v, kzval(k, P.kzL));  // times kz (z derivative)
+                spec[(e * (G::H + 1) + k) * 2 + 0] = v.x;
+                spec[(e * (G::H + 1) + k) * 2 + 1] = v.y;
+            }
+        }
+    }
+    __syncthreads();
+    for (int s = tid; s < nzd; s += blockDim.x) {
+        // unpack: full[s] = half[s] (s <= H) or conj(half[nz - s]) (MHD_BQlin.cpp:264-267)
+        cplx drive[NEMF];
+#pragma unroll
+        for (int e = 0; e < NEMF; ++e) {
+            const int hs = s <= G::H ? s : nzd - s;
+            cplx v = mk(spec[(e * (G::H + 1) + hs) * 2], spec[(e * (G::H + 1) + hs) * 2 + 1]);
+            drive[e] = s <= G::H ? v : conjc(v);
+        }
+        const int kzi = s <= G::H ? s : s - nzd;
+        const double c = kzval(kzi, P.kzL);
+        const double kz2 = kz2val(c);
+        cplx m[4], F[4];
+#pragma unroll
+        for (int mm = 0; mm < 4; ++mm) {
+            m[mm] = (mm < P.nmf) ? ldc_cg(A.mf + mm * nzd + s) : mk(0.0, 0.0);
+            F[mm] = mk(0.0, 0.0);
+        }
+        if (MODEL == MODEL_BQLIN) {
+            // dBy = -q Bx + EMF_y, dBx = EMF_x (MHD_BQlin.cpp:274-280)
+            if (P.ql) {
+                F[0] = drive[0];
+                F[1] = cadd(cscale(m[0], -P.q), drive[1]);
+            }
+        } else {
+            // MHD_FullQlin.cpp:411-423 (B0z kz terms with kz = i c)
+            if (P.ql) {
+                F[1] = cadd(cadd(cscale(m[0], -P.q), imul(m[3], P.B0z * c)), drive[1]);
+                F[0] = cadd(imul(m[2], P.B0z * c), drive[0]);
+                F[2] = cadd(cadd(cscale(m[3], 2.0 * P.Omega), imul(m[0], P.B0z * c)), drive[2]);
+                F[3] = cadd(cadd(cscale(m[2], P.q - 2.0 * P.Omega), imul(m[1], P.B0z * c)), drive[3]);
+            }
+        }
+        for (int mm = 0; mm < P.nmf; ++mm) {
+            if (A.rhs_only) {
+                stc(A.Fmf_out + mm * nzd + s, F[mm]);
+                continue;
+            }
+            const double Lm = P.ql ? __dmul_rn((MODEL == MODEL_FULLQLIN && mm >= 2) ? P.nu : P.eta, kz2) : 0.0;
+            cplx fp = S.has_prev ? ldc_cg(A.Fmf_prev + mm * nzd + s) : mk(0.0, 0.0);
+            cplx nv = rk_update<INTEG>(S, Lm, Lm, F[mm], fp, m[mm], S.has_prev);
+            if (A.Fmf_out) stc(A.Fmf_out + mm * nzd + s, F[mm]);
+            stc(A.mf + mm * nzd + s, nv);
+            const double mag = nv.x * nv.x + nv.y * nv.y;
+            if (!(mag == mag) || isinf(mag)) atomicOr(&A.clk->status, QLGPU_STATUS_NONFINITE);
+            else if (mag > 1e40) atomicOr(&A.clk->status, QLGPU_STATUS_UNSTABLE);
+        }
+    }
+    __syncthreads();
+    if (A.rhs_only || tid != 0) return;
+    DevClock* C = A.clk;
+    // CN bookkeeping: this stage's operator time becomes "old" (RK3CN.cpp:119-122)
+    C->t_old = S.abs_time ? S.t_off : __dadd_rn(tclock, S.t_off);
+    C->dtlin_old = S.dt_lin;
+    C->old_init = 0;
+    if (!last) return;
+    C->t = t_new;
+    C->timevar = __dadd_rn(C->timevar, P.dt);
+    C->since += 1;
+    if (!diag_due) return;
+    // Calc_Energy_AM_Diss (MHD_BQlin.cpp:408-477)
+    double eMB = 0, aMB = 0, dMB = 0, eMU = 0, aMU = 0, dMU = 0;
+    for (int s = 0; s < nzd; ++s) {
+        const int kzi = s <= G::H ? s : s - nzd;
+        const double kz2 = kz2val(kzval(kzi, P.kzL));
+        cplx b0 = ldc_cg(A.mf + s), b1 = ldc_cg(A.mf + nzd + s);
+        eMB += (b0.x * b0.x + b0.y * b0.y) + (b1.x * b1.x + b1.y * b1.y);
+        aMB += b0.x * b1.x + b0.y * b1.y;
+        dMB += -kz2 * (b0.x * b0.x + b0.y * b0.y) - kz2 * (b1.x * b1.x + b1.y * b1.y);
+        if (P.nmf == 4) {
+            cplx u0 = ldc_cg(A.mf + 2 * nzd + s), u1 = ldc_cg(A.mf + 3 * nzd + s);
+            eMU += (u0.x * u0.x + u0.y * u0.y) + (u1.x * u1.x + u1.y * u1.y);
+            aMU += u0.x * u1.x + u0.y * u1.y;
+            dMU += -kz2 * (u0.x * u0.x + u0.y * u0.y) - kz2 * (u1.x * u1.x + u1.y * u1.y);
+        }
+    }
+    eMB *= P.divMF; eMU *= P.divMF; aMB *= P.divMF; aMU *= P.divMF;
+    dMB *= P.divMF * P.eta; dMU *= P.divMF * P.nu;
+    const double* ds = tot + NEMF * G::NZ;
+    const double eu = ds[0] * P.divfac, eb = ds[1] * P.divfac;
+    const double au = ds[2] * P.divfac, abv = ds[3] * P.divfac;
+    const double du = ds[4] * P.divfac, db = ds[5] * P.divfac;
+    const int r = C->ndiag;
+    if (r < A.diag_cap) {
+        double* o = A.diag_ring + (size_t)r * 15;
+        o[0] = t_new;
+        o[1] = eMU / 2; o[2] = eMB / 2; o[3] = eu / 2; o[4] = eb / 2;
+        o[5] = aMU; o[6] = aMB; o[7] = au; o[8] = abv;
+        o[9] = dMU; o[10] = dMB; o[11] = du; o[12] = db;
+        o[13] = pow(P.nu * P.nu * P.nu / (dMU + du), 0.25) * P.kzmax;
+        o[14] = pow(P.eta * P.eta * P.eta / (dMB + db), 0.25) * P.kzmax;
+    } else {
+        C->status |= QLGPU_STATUS_DIAG_FULL;
+    }
+    C->ndiag = r + 1;
+    C->timevar = __dsub_rn(C->timevar, P.tv_interval);
+    C->since = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory carve-up of the stage kernel
+// ---------------------------------------------------------------------------
+template <class G, int MODEL, class Priv>
+struct Smem {
+    static constexpr int SW = 32 / G::T;                        // groups per warp
+    static constexpr int NMFR = MODEL == MODEL_BQLIN ? 3 : 8;   // real-space mean-field profiles
+    static constexpr int NEMF = MODEL == MODEL_BQLIN ? 2 : 4;   // stress profiles summed over modes
+    static constexpr int PL = NEMF * G::NZ + 8;                 // partial vector length (doubles)
+    static constexpr int NZD = G::nz;
+    // offsets in bytes
+    static constexpr size_t o_tw = 0;
+    static constexpr size_t o_mfr = o_tw + sizeof(cplx) * G::NZ;
+    static constexpr size_t o_ekz = o_mfr + sizeof(double) * NMFR * G::NZ;
+    static constexpr size_t o_spec = o_ekz + sizeof(double) * 2 * ((NZD + 1) & ~1);
+    static constexpr size_t o_tot = o_spec + sizeof(double) * 2 * NEMF * (G::H + 1);
+    static constexpr size_t o_work = o_tot + sizeof(double) * ((PL + 1) & ~1);
+    // per group: F_prev prefetch buffer (nz cplx); per pair of groups: R_uz, R_bz (2 NZ cplx)
+    static constexpr size_t GS_BYTES = sizeof(cplx) * (NZD + G::NZ);
+    __host__ __device__ static size_t work_bytes(int warps) {
+        const size_t xch = sizeof(cplx) * (size_t)warps * SW * G::XSIZE;
+        const size_t red = sizeof(double) * ((size_t)warps * SW * NEMF * G::NZ + (size_t)warps * 32 * 6);
+        return xch > red ? xch : red;
+    }
+    __host__ __device__ static size_t bytes(int warps) {
+        return o_work + work_bytes(warps) + Priv::smem_bytes_per_warp() * (size_t)warps +
+               GS_BYTES * (size_t)warps * SW;
+    }
+    __host__ __device__ static int tmem_cols(int warps) {
+        int need = Priv::tmem_cols_per_warp() * ((warps + 3) / 4);
+        if (need == 0) return 0;
+        int c = 32;
+        while (c < need) c <<= 1;
+        return c;
+    }
+};
+
+template <int NZ, int MODEL, int INTEG, bool USE_TMEM>
+__global__ void __launch_bounds__(128, 1) stage_kernel(StageArgs A, DevParams P) {
     using G = Geom<NZ>;
-    using SM = Smem<G, MODEL>;
+    using Priv = typename std::conditional<USE_TMEM, PrivTmem<G, PB_COUNT>, PrivSmem<G, PB_COUNT>>::type;
+    using SM = Smem<G, MODEL, Priv>;
     constexpr int SW = SM::SW;
+    static_assert(SW % 2 == 0, "a warp holds whole pairs of groups");
     constexpr int NEMF = SM::NEMF;
     constexpr int PL = SM::PL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_last;
     const int warps = blockDim.x >> 5;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int slot = lane / G::T, t = lane % G::T;
     const unsigned gmask = (G::T == 32 ? 0xffffffffu : (((1u << G::T) - 1u) << (slot * G::T)));
-    cplx* tw_s = reinterpret_cast<cplx*>(smem_raw);
-    double* mfr = reinterpret_cast<double*>(tw_s + G::NZ);
-    double* spec = mfr + SM::NMFR * G::NZ;
-    cplx* xch_all = reinterpret_cast<cplx*>(spec + 2 * NEMF * (G::H + 1));
-    cplx* priv_all = xch_all + (size_t)warps * SW * G::XSIZE;
-    cplx* xch = xch_all + (size_t)(warp * SW + slot) * G::XSIZE;
-    cplx* priv = priv_all + (size_t)warp * SM::NPRIV * G::P * 32;
-    const int gidx = warp * SW + slot;    // group index in the CTA
-    const int ngc = warps * SW;           // groups per CTA
+    cplx* tw_s = reinterpret_cast<cplx*>(smem_raw + SM::o_tw);
+    double* mfr = reinterpret_cast<double*>(smem_raw + SM::o_mfr);
+    double* ekz = reinterpret_cast<double*>(smem_raw + SM::o_ekz);
+    double* spec = reinterpret_cast<double*>(smem_raw + SM::o_spec);
+    double* tot = reinterpret_cast<double*>(smem_raw + SM::o_tot);
+    unsigned char* work = smem_raw + SM::o_work;
+    cplx* xch = reinterpret_cast<cplx*>(work) + (size_t)(warp * SW + slot) * G::XSIZE;
+    const int gidx = warp * SW + slot;  // group index in the CTA
+    const int ngc = warps * SW;         // groups per CTA
     const StageConst& S = A.sc;
+    const int nzd = P.nz;
+
+    // optional trace (CTA 0 thread 0 and the top CTA): [0] start, [1] prologue done,
+    // [2] mode loop done, [3] partials written, [4] top CTA start, [5] top done,
+    // [8] first mode staged, [9..18] start of pipeline steps 0..9
+    const bool tr = A.trace && blockIdx.x == 0 && tid == 0;
+    if (tr) A.trace[0] = gtimer();
+    // ---- private store: TMEM allocation (one warp) or a shared-memory region
+    Priv pv;
+    const int tcols = SM::tmem_cols(warps);
+    if constexpr (USE_TMEM) {
+        if (warp == 0) tmem_alloc(&s_tmem, (uint32_t)tcols);
+        tmem_fence_before_sync();
+        __syncthreads();
+        tmem_fence_after_sync();
+        pv.init(s_tmem, warp);
+    } else {
+        pv.init(reinterpret_cast<cplx*>(work + SM::work_bytes(warps)) + (size_t)warp * PB_COUNT * G::P * 32, lane);
+    }
+    // pair layout: octet o = lane / T, pair pi = o / 2, role = o % 2 (0: velocity side, 1: magnetic side)
+    const int role = slot & 1;
+    const int pi = slot >> 1;
+    const unsigned pmask = (2 * G::T == 32) ? 0xffffffffu : (((1u << (2 * G::T)) - 1u) << (pi * 2 * G::T));
+    PairShared ps;
+    {
+        unsigned char* gbase = work + SM::work_bytes(warps) + Priv::smem_bytes_per_warp() * (size_t)warps;
+        cplx* fpb_all = reinterpret_cast<cplx*>(gbase);
+        cplx* k_all = fpb_all + (size_t)warps * SW * SM::NZD;
+        ps.fpb = fpb_all + (size_t)gidx * SM::NZD;
+        cplx* kpair = k_all + (size_t)(warp * (SW / 2) + pi) * 2 * G::NZ;
+        ps.KU = kpair;
+        ps.KB = kpair + G::NZ;
+    }
+    {   // zero the stress accumulators
+        cplx z4[4] = {mk(0, 0), mk(0, 0), mk(0, 0), mk(0, 0)};
+#pragma unroll
+        for (int c4 = 0; c4 < G::P / 4; ++c4) pv.st4(PB_E, c4, z4);
+        pv.st_fence();
+    }
 
     for (int i = tid; i < G::NZ; i += blockDim.x) tw_s[i] = A.tw[i];
     const double tclock = __ldcg(&A.clk->t);
@@ -111,9 +325,23 @@ __global__ void stage_kernel(StageArgs A, DevParams P) {
     cn.t_old = __ldcg(&A.clk->t_old);
     cn.dtlin_old = __ldcg(&A.clk->dtlin_old);
     cn.old_init = __ldcg(&A.clk->old_init);
+    // factored integrating factor tables exp(linC c kz2), per stored kz
+    if (INTEG == INTEG_EXP) {
+        for (int s = tid; s < nzd; s += blockDim.x) {
+            const int kzi = s <= G::H ? s : s - nzd;
+            const double kz2 = kz2val(kzval(kzi, P.kzL));
+            ekz[s] = exp(S.linC * P.nu * kz2);
+            ekz[SM::NZD + (SM::NZD & 1) + s] = exp(S.linC * P.etanu * P.nu * kz2);
+        }
+    }
+    StageTables TB;
+    TB.ekz_u = ekz;
+    TB.ekz_b = ekz + SM::NZD + (SM::NZD & 1);
+    TB.ilap2 = A.ilap2;
     __syncthreads();
     mean_profiles<G, MODEL>(P, A.mf, mfr, xch, tw_s, gidx, ngc, t, gmask);
     __syncthreads();
+    if (tr) A.trace[1] = gtimer();
 
     // Last-stage bookkeeping identical in every CTA (main.cpp:111-130)
     const double t_new = __dadd_rn(tclock, P.dt);
@@ -124,18 +352,20 @@ __global__ void stage_kernel(StageArgs A, DevParams P) {
         diag_due = __dsub_rn(tv, P.tv_interval) > -1e-8;
     }
     const double qt = __dmul_rn(P.q, t_new);
-
-    double emfx[G::P], emfy[G::P];
-#pragma unroll
-    for (int j = 0; j < G::P; ++j) { emfx[j] = 0.0; emfy[j] = 0.0; }
     double dacc[6] = {0, 0, 0, 0, 0, 0};
 
-    const int gid = blockIdx.x * ngc + gidx;
-    const int NG = gridDim.x * ngc;
-    for (int mode = gid; mode < P.nxy; mode += NG) {
+    // ---- mode loop: one mode per pair of groups, warp-uniform trip count (TMEM access is warp-wide)
+    constexpr int PW = SW / 2;  // pairs per warp
+    const int wglobal = blockIdx.x * warps + warp;
+    const int WG = gridDim.x * warps;
+    for (int base = wglobal * PW; base < P.nxy; base += WG * PW) {
+        const int mode_raw = base + pi;
+        const bool valid = mode_raw < P.nxy;
+        const int mode = valid ? mode_raw : P.nxy - 1;
         if (MODEL == MODEL_BQLIN)
-            bqlin_mode<G, INTEG>(A, P, mode, t, gmask, xch, priv, lane, tw_s, mfr, emfx, emfy, tclock, cn);
-        if (last) {
+            bqlin_pair<G, INTEG, Priv>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps, pv, tw_s, mfr, tclock,
+                                       cn);
+        if (last && valid && role == 0) {
             // ShearingBox_Remap(q t) after t += dt (main.cpp:122-123, MHD_BQlin.cpp:319-329)
             double kx0 = A.kx0[mode];
             const double ky = __ldg(A.ky + mode);
@@ -146,6 +376,7 @@ __global__ void stage_kernel(StageArgs A, DevParams P) {
                     zeroed = true;
                     kx0 = __dsub_rn(kx0, P.remap_shift);
                     cplx* uo = A.lin_out + (size_t)mode * 4 * P.nz;
+                    __syncwarp(pmask & gmask);
 #pragma unroll
                     for (int k2 = 0; k2 < G::P; ++k2) {
                         const int s = stored_index<G>(t + G::T * k2);
@@ -153,7 +384,6 @@ __global__ void stage_kernel(StageArgs A, DevParams P) {
 #pragma unroll
                         for (int v = 0; v < 4; ++v) stc(uo + v * P.nz + s, mk(0.0, 0.0));
                     }
-                    __syncwarp(gmask);
                     if (t == 0) A.kx0[mode] = kx0;
                 }
             }
@@ -161,21 +391,33 @@ __global__ void stage_kernel(StageArgs A, DevParams P) {
                 mode_diag<G>(P, A.lin_out + (size_t)mode * 4 * P.nz, __ldg(A.kxi + mode), __ldg(A.kyi + mode), kx0,
                              ky, t_new, t, dacc);
         }
+        __syncwarp();
     }
 
     // ---- CTA reduction of the stress profiles and diagnostics (fixed order)
     __syncthreads();
-    double* red = reinterpret_cast<double*>(priv_all);  // [ngc][NEMF][NZ] then [blockDim][6]
+    if (tr) A.trace[2] = gtimer();
+    double* red = reinterpret_cast<double*>(work);  // [ngc][NEMF][NZ] then [blockDim][6]
 #pragma unroll
-    for (int j = 0; j < G::P; ++j) {
-        const int z = zpos<G>(t, j);
-        red[(gidx * NEMF + 0) * G::NZ + z] = emfx[j];
-        red[(gidx * NEMF + 1) * G::NZ + z] = emfy[j];
+    for (int c4 = 0; c4 < G::P / 4; ++c4) {
+        cplx e[4];
+        pv.ld4(PB_E, c4, e);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int z = zpos<G>(t, 4 * c4 + i);
+            red[(gidx * NEMF + 0) * G::NZ + z] = e[i].x;
+            red[(gidx * NEMF + 1) * G::NZ + z] = e[i].y;
+        }
     }
     double* dred = red + (size_t)ngc * NEMF * G::NZ;
 #pragma unroll
     for (int c = 0; c < 6; ++c) dred[tid * 6 + c] = dacc[c];
+    if constexpr (USE_TMEM) tmem_fence_before_sync();
     __syncthreads();
+    if constexpr (USE_TMEM) {
+        tmem_fence_after_sync();
+        if (warp == 0) tmem_dealloc(s_tmem, (uint32_t)tcols);
+    }
     double* part = A.partials + (size_t)blockIdx.x * PL;
     for (int idx = tid; idx < NEMF * G::NZ; idx += blockDim.x) {
         double s = 0.0;
@@ -189,9 +431,9 @@ __global__ void stage_kernel(StageArgs A, DevParams P) {
     }
 
     // ---- two-level last-arriver reduction
-    __shared__ int s_last;
     __threadfence();
     __syncthreads();
+    if (tr) A.trace[3] = gtimer();
     const int ngroups = (gridDim.x + RED_GROUP - 1) / RED_GROUP;
     const int grp = blockIdx.x / RED_GROUP;
     const int c0 = grp * RED_GROUP;
@@ -219,124 +461,17 @@ __global__ void stage_kernel(StageArgs A, DevParams P) {
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    double* tot = red;  // reuse: [PL]
     for (int idx = tid; idx < PL; idx += blockDim.x) {
         double s = 0.0;
         for (int g = 0; g < ngroups; ++g) s += __ldcg(A.gpartials + (size_t)g * PL + idx);
         tot[idx] = s;
     }
     if (tid == 0) A.clk->cnt_top = 0u;
+    if (A.trace && tid == 0) A.trace[4] = gtimer();
     __syncthreads();
-
-    // ---- mean-field stage (top CTA only)
-    // Stress spectra: fwd of the real profiles, half spectrum k = 0..H
-    // (MHD_BQlin.cpp:228-240 after the sum over modes; linear, so one transform)
-    for (int e = gidx; e < NEMF; e += ngc) {
-        cplx x[G::P];
-#pragma unroll
-        for (int j = 0; j < G::P; ++j) x[j] = mk(tot[e * G::NZ + zpos<G>(t, j)], 0.0);
-        fwd_fft<G>(x, xch, tw_s, t, gmask);
-#pragma unroll
-        for (int k2 = 0; k2 < G::P; ++k2) {
-            const int k = t + G::T * k2;
-            if (k <= G::H) {
-                cplx v = cscale(x[k2], P.rs_fac);
-                if (MODEL == MODEL_BQLIN || e < 2) v = imul(v, kzval(k, P.kzL));  // times kz (z derivative)
-                spec[(e * (G::H + 1) + k) * 2 + 0] = v.x;
-                spec[(e * (G::H + 1) + k) * 2 + 1] = v.y;
-            }
-        }
-    }
-    __syncthreads();
-    const int nzd = P.nz;
-    for (int s = tid; s < nzd; s += blockDim.x) {
-        // unpack: full[s] = half[s] (s <= H) or conj(half[nz - s]) (MHD_BQlin.cpp:264-267)
-        cplx drive[NEMF];
-#pragma unroll
-        for (int e = 0; e < NEMF; ++e) {
-            const int hs = s <= G::H ? s : nzd - s;
-            cplx v = mk(spec[(e * (G::H + 1) + hs) * 2], spec[(e * (G::H + 1) + hs) * 2 + 1]);
-            drive[e] = s <= G::H ? v : conjc(v);
-        }
-        const int kzi = s <= G::H ? s : s - nzd;
-        const double c = kzval(kzi, P.kzL);
-        const double kz2 = kz2val(c);
-        cplx m[4], F[4];
-#pragma unroll
-        for (int mm = 0; mm < 4; ++mm) m[mm] = (mm < P.nmf) ? ldc_cg(A.mf + mm * nzd + s) : mk(0.0, 0.0);
-        if (MODEL == MODEL_BQLIN) {
-            // dBy = -q Bx + EMF_y, dBx = EMF_x (MHD_BQlin.cpp:274-280)
-            F[0] = P.ql ? drive[0] : mk(0.0, 0.0);
-            F[1] = P.ql ? cadd(cscale(m[0], -P.q), drive[1]) : mk(0.0, 0.0);
-        }
-        for (int mm = 0; mm < P.nmf; ++mm) {
-            if (A.rhs_only) {
-                stc(A.Fmf_out + mm * nzd + s, F[mm]);
-                continue;
-            }
-            const double Lm = P.ql ? __dmul_rn((MODEL == MODEL_FULLQLIN && mm >= 2) ? P.nu : P.eta, kz2) : 0.0;
-            cplx fp = S.has_prev ? ldc_cg(A.Fmf_prev + mm * nzd + s) : mk(0.0, 0.0);
-            cplx nv = rk_update<INTEG>(S, Lm, Lm, F[mm], fp, m[mm], S.has_prev);
-            if (A.Fmf_out) stc(A.Fmf_out + mm * nzd + s, F[mm]);
-            stc(A.mf + mm * nzd + s, nv);
-            const double mag = nv.x * nv.x + nv.y * nv.y;
-            if (!(mag == mag) || isinf(mag)) atomicOr(&A.clk->status, QLGPU_STATUS_NONFINITE);
-            else if (mag > 1e40) atomicOr(&A.clk->status, QLGPU_STATUS_UNSTABLE);
-        }
-    }
-    __syncthreads();
-    if (A.rhs_only) return;
-    if (tid == 0) {
-        DevClock* C = A.clk;
-        // CN bookkeeping: this stage's operator time becomes "old" (RK3CN.cpp:119-122)
-        C->t_old = S.abs_time ? S.t_off : __dadd_rn(tclock, S.t_off);
-        C->dtlin_old = S.dt_lin;
-        C->old_init = 0;
-        if (last) {
-            C->t = t_new;
-            C->timevar = __dadd_rn(C->timevar, P.dt);
-            C->since += 1;
-            if (diag_due) {
-                // Calc_Energy_AM_Diss (MHD_BQlin.cpp:408-477)
-                double eMB = 0, aMB = 0, dMB = 0, eMU = 0, aMU = 0, dMU = 0;
-                for (int s = 0; s < nzd; ++s) {
-                    const int kzi = s <= G::H ? s : s - nzd;
-                    const double kz2 = kz2val(kzval(kzi, P.kzL));
-                    cplx b0 = ldc_cg(A.mf + s), b1 = ldc_cg(A.mf + nzd + s);
-                    eMB += (b0.x * b0.x + b0.y * b0.y) + (b1.x * b1.x + b1.y * b1.y);
-                    aMB += b0.x * b1.x + b0.y * b1.y;
-                    dMB += -kz2 * (b0.x * b0.x + b0.y * b0.y) - kz2 * (b1.x * b1.x + b1.y * b1.y);
-                    if (P.nmf == 4) {
-                        cplx u0 = ldc_cg(A.mf + 2 * nzd + s), u1 = ldc_cg(A.mf + 3 * nzd + s);
-                        eMU += (u0.x * u0.x + u0.y * u0.y) + (u1.x * u1.x + u1.y * u1.y);
-                        aMU += u0.x * u1.x + u0.y * u1.y;
-                        dMU += -kz2 * (u0.x * u0.x + u0.y * u0.y) - kz2 * (u1.x * u1.x + u1.y * u1.y);
-                    }
-                }
-                eMB *= P.divMF; eMU *= P.divMF; aMB *= P.divMF; aMU *= P.divMF;
-                dMB *= P.divMF * P.eta; dMU *= P.divMF * P.nu;
-                const double* ds = tot + NEMF * G::NZ;
-                const double eu = ds[0] * P.divfac, eb = ds[1] * P.divfac;
-                const double au = ds[2] * P.divfac, abv = ds[3] * P.divfac;
-                const double du = ds[4] * P.divfac, db = ds[5] * P.divfac;
-                const int r = C->ndiag;
-                if (r < A.diag_cap) {
-                    double* o = A.diag_ring + (size_t)r * 15;
-                    o[0] = t_new;
-                    o[1] = eMU / 2; o[2] = eMB / 2; o[3] = eu / 2; o[4] = eb / 2;
-                    o[5] = aMU; o[6] = aMB; o[7] = au; o[8] = abv;
-                    o[9] = dMU; o[10] = dMB; o[11] = du; o[12] = db;
-                    o[13] = pow(P.nu * P.nu * P.nu / (dMU + du), 0.25) * P.kzmax;
-                    o[14] = pow(P.eta * P.eta * P.eta / (dMB + db), 0.25) * P.kzmax;
-                } else {
-                    C->status |= QLGPU_STATUS_DIAG_FULL;
-                }
-                C->ndiag = r + 1;
-                C->timevar = __dsub_rn(C->timevar, P.tv_interval);
-                C->since = 0;
-            }
-        }
-    }
+    mean_field_stage<G, MODEL, INTEG, NEMF>(A, P, tot, spec, xch, tw_s, gidx, ngc, t, gmask, tclock, t_new, last,
+                                           diag_due);
+    if (A.trace && tid == 0) A.trace[5] = gtimer();
 }
 
 // Diagnostics of the current state without stepping (the initial record,

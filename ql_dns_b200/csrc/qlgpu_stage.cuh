@@ -17,6 +17,7 @@
 // FP64.
 #pragma once
 #include "qlgpu_fft.cuh"
+#include "qlgpu_priv.cuh"
 #include "qlgpu_types.h"
 
 namespace qlgpu {
@@ -37,6 +38,24 @@ __device__ __forceinline__ void stc(cplx* p, cplx v) {
 }
 // i*s*a for real s
 __device__ __forceinline__ cplx imul(cplx a, double s) { return mk(-a.y * s, a.x * s); }
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long v;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(v));
+    return v;
+}
+
+// Asynchronous global -> shared copies (cp.async), 16 or 8 bytes each
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // kx(t) = kx0 + (q t) ky, evaluated with the reference's rounding order
 // (MHD_BQlin.cpp:498: K->kx[i] + q_*t*kyctmp_)
@@ -113,35 +132,55 @@ struct CnOld {
 };
 
 // ---------------------------------------------------------------------------
-// Shared-memory carve-up
+// Per-stage tables shared by all modes of a CTA: exp(linC * coef * kz2) for the
+// factored integrating factor of RK3CN_Elin (exp(linC L) = exp(linC c h)
+// exp(linC c kz2) with L = c ((-kx^2 - ky^2) + kz2), MHD_BQlin.cpp:249-252).
 // ---------------------------------------------------------------------------
-template <class G, int MODEL>
-struct Smem {
-    static constexpr int SW = 32 / G::T;          // groups per warp
-    static constexpr int NMFR = MODEL == MODEL_BQLIN ? 3 : 8;  // real-space mean-field profiles
-    static constexpr int NPRIV = MODEL == MODEL_BQLIN ? 4 : 6; // private per-thread buffers (P cplx)
-    static constexpr int NEMF = MODEL == MODEL_BQLIN ? 2 : 4;  // stress profiles summed over modes
-    static constexpr int PL = NEMF * G::NZ + 8;   // partial vector length (doubles)
-    static size_t bytes(int warps) {
-        size_t b = 0;
-        b += sizeof(cplx) * G::NZ;                       // twiddles
-        b += sizeof(double) * NMFR * G::NZ;              // mean-field profiles
-        b += sizeof(double) * 2 * NEMF * (G::H + 1);     // top-CTA spectra scratch
-        b += sizeof(cplx) * (size_t)warps * SW * G::XSIZE;     // exchange
-        b += sizeof(cplx) * (size_t)warps * NPRIV * G::P * 32; // private buffers
-        return b;
-    }
+struct StageTables {
+    const double* ekz_u;  // [nz]  exp(linC nu kz2)
+    const double* ekz_b;  // [nz]  exp(linC (eta/nu) nu kz2)
+    const double* ilap2;  // [Ny/2][nz] 1/lap2 with the ky=kz=0 fix (Kdata.cpp:100-119)
 };
 
+// Buffers of the private store used by the BQlin pipeline
+enum { PB_E = 0, PB_A = 1, PB_S = 2, PB_COUNT = 3 };
+
 // ---------------------------------------------------------------------------
-// Per-mode work for MHD_BQlin (MHD_BQlin.cpp:135-257) fused with the update.
-// Real-space fields R_f = inv(f / NZ); the products follow MHD_BQlin.cpp:153-201
-// with the scalar wavenumbers pulled out of the transforms.
+// MHD_BQlin right-hand side (MHD_BQlin.cpp:135-257) fused with the RK update
+// for one mode, held by a PAIR of transform groups that run the same code on
+// mirrored fields: role 0 ("U") owns the velocity-side transforms, role 1
+// ("B") the magnetic-side ones.  Real-space fields are R_f = inv(f/NZ); the
+// scalar wavenumbers (i kx, i ky) commute with the z transforms and are applied
+// in real space.  Only R_uz and R_bz cross between the two groups (shared
+// memory KU, KB); everything else stays in each thread's private store.
+//
+//   step  U (velocity side)                      B (magnetic side)
+//   0 inv R_uz -> KU                             R_bz -> KB
+//   1 inv R_u : Ex += Re(KB R_u*)                R_b : Ex -= Re(KU R_b*)
+//         A = -i kx dBy R_u                      A = -i kx dBy R_b + ddBy KB
+//     fwd i ky By R_u -> F_b (update b)          i ky By R_b -> S
+//   2 inv R_zeta : A += i ky By R_zeta           R_eta : G = A + i ky By R_eta
+//     fwd (idle)                                 G -> F_zeta (update zeta)
+//   3 inv R_{i kz uz} :                          R_by : Ey -= Re(KU R_by*)
+//         G = A - 2 dBy R - ddBy KU                     G = 2 kx ky dBy KB
+//     fwd G -> F_eta (update eta)                G -> F_u = S + ilapF(...) (update u)
+//   4 inv R_uy : Ey += Re(KB R_uy*)              (idle)
+// The stress profiles Ex, Ey (MHD_BQlin.cpp:212-241) are summed over modes
+// before their forward transform (linear), in each thread's private store.
+// All lanes of a warp run the same step at the same time (warp-convergent);
+// `valid` is false for the padding pairs of the last pass (no stores, no sums).
 // ---------------------------------------------------------------------------
-template <class G, int INTEG>
-__device__ __forceinline__ void bqlin_mode(const StageArgs& A, const DevParams& P, int mode, int t, unsigned gmask,
-                                           cplx* xch, cplx* priv, int lane, const cplx* tw, const double* mfr,
-                                           double* emfx, double* emfy, double tclock, const CnOld& cn) {
+struct PairShared {
+    cplx* KU;   // R_uz, [P][T]
+    cplx* KB;   // R_bz, [P][T]
+    cplx* fpb;  // this group's F_prev prefetch buffer [nz]
+};
+
+template <class G, int INTEG, class Priv>
+__device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& P, const StageTables& TB, int mode,
+                                           bool valid, int role, int t, unsigned gmask, unsigned pmask, cplx* xch,
+                                           const PairShared& ps, const Priv& pv, const cplx* tw, const double* mfr,
+                                           double tclock, const CnOld& cn) {
     constexpr int Pn = G::P;
     const StageConst& S = A.sc;
     const double fac = P.fac;
@@ -149,207 +188,273 @@ __device__ __forceinline__ void bqlin_mode(const StageArgs& A, const DevParams& 
     const double kx0 = A.kx0[mode];
     const int kyi = __ldg(A.kyi + mode), kxi = __ldg(A.kxi + mode);
     const double ts = S.abs_time ? S.t_off : __dadd_rn(tclock, S.t_off);
-    const double a = kx_at(kx0, P.q, ts, ky);         // kx(t_s)
+    const double a = kx_at(kx0, P.q, ts, ky);  // kx(t_s), MHD_BQlin.cpp:498
     const double b = ky;
     const double ab = __dmul_rn(a, b);
     const double Om2 = __dmul_rn(2.0, P.Omega);
-    const double mult = (ky == 0.0) ? 1.0 : 2.0;
-    const cplx* u_in = A.lin_in + (size_t)mode * 4 * P.nz;
+    const double mult = valid ? ((ky == 0.0) ? 1.0 : 2.0) : 0.0;
+    const cplx* __restrict__ u_in = A.lin_in + (size_t)mode * 4 * P.nz;
     cplx* u_out = A.lin_out + (size_t)mode * 4 * P.nz;
-    const cplx* Fp = A.Fprev ? A.Fprev + (size_t)mode * 4 * P.nz : nullptr;
+    const cplx* Fp = (A.Fprev && S.has_prev) ? A.Fprev + (size_t)mode * 4 * P.nz : nullptr;
     cplx* Fo = A.Fout ? A.Fout + (size_t)mode * 4 * P.nz : nullptr;
     const double* By = mfr;
     const double* dBy = mfr + G::NZ;
     const double* ddBy = mfr + 2 * G::NZ;
-    cplx* K1 = priv;                    // R_bz
-    cplx* K2 = priv + 1 * Pn * 32;      // R_uz
-    cplx* A1 = priv + 2 * Pn * 32;      // accumulator for G_eta then G_zeta
-    cplx* A2 = priv + 3 * Pn * 32;      // spectral fwd(i ky By R_b) for F_u
-#define PRIV(buf, j) buf[(j) * 32 + lane]
-    cplx x[Pn];
+    const double* __restrict__ il2row = TB.ilap2 + (size_t)kyi * P.nz;
+    cplx* Kown = role ? ps.KB : ps.KU;
+    const cplx* Koth = role ? ps.KU : ps.KB;
+    const int fbase = role ? 2 : 0;  // u,zeta for U; b,eta for B
 
-    // Stage-end linear operators and update, per spectral register k2
-    const double kxe = __dadd_rn(a, __dmul_rn(__dmul_rn(P.q, S.dt_lin), ky));  // MHD_BQlin.cpp:248
-    double kxo = 0.0;  // CN: kx of the previous stage end (or t0 for the init form)
+    // Stage-end operator: kx' = kx(t_s) + q dt_lin ky (MHD_BQlin.cpp:248)
+    const double kxe = __dadd_rn(a, __dmul_rn(__dmul_rn(P.q, S.dt_lin), ky));
+    const double hxy = __dsub_rn(-__dmul_rn(kxe, kxe), __dmul_rn(ky, ky));
+    double em_u = 1.0, em_b = 1.0;
+    if (INTEG == INTEG_EXP && !A.rhs_only) {
+        em_u = exp(S.linC * P.nu * hxy);
+        em_b = exp(S.linC * P.etanu * P.nu * hxy);
+    }
+    double kxo = 0.0;  // CN: kx of the previous stage end (or of t0 for the init form)
     if (INTEG == INTEG_CN) {
         if (cn.old_init) kxo = kx_at(kx0, P.q, tclock, ky);
         else kxo = __dadd_rn(kx_at(kx0, P.q, cn.t_old, ky), __dmul_rn(__dmul_rn(P.q, cn.dtlin_old), ky));
     }
+    const bool tr = A.trace && blockIdx.x == 0 && threadIdx.x == 0;
+    if (tr) A.trace[8] = gtimer();
 
-    // Load a derived spectral field into x (scaled by 1/NZ), zero in the padding gap.
-    // which: 0 u,1 zeta,2 b,3 eta, 4 uz, 5 bz, 6 i kz uz, 7 uy, 8 by
-    auto load = [&](int which) {
+    cplx x[Pn];
+    __syncwarp(pmask);  // the previous mode's readers of KU / KB are done
+
+#pragma unroll 1
+    for (int step = 0; step < 5; ++step) {
+        if (tr) A.trace[9 + step] = gtimer();
+        // field updated by this group's forward transform at this step (-1: none)
+        int fupd = -1;
+        if (step == 1) fupd = role ? -2 : 2;  // B: S buffer
+        if (step == 2) fupd = role ? 1 : -1;
+        if (step == 3) fupd = role ? 0 : 3;
+        // prefetch F of the previous stage for the field being updated
+        if (Fp && fupd >= 0) {
+            __syncwarp(gmask);
+            const cplx* src = Fp + fupd * P.nz;
+            for (int i = t; i < P.nz; i += G::T) cp_async16(ps.fpb + i, src + i);
+            cp_async_commit();
+        }
+        // ---- inverse transform of this step's field (scaled by 1/NZ)
+        {
+            // kind: 0 plain, 1 z-component (a c f0 - i b f1) il2, 2 i kz z-component,
+            //       3 y-component (ab f0 + i c f1) il2 (MHD_BQlin.cpp:143-146), 4 none
+            int kind, f0;
+            switch (step) {
+                case 0: kind = 1; f0 = fbase; break;
+                case 1: kind = 0; f0 = fbase; break;
+                case 2: kind = 0; f0 = fbase + 1; break;
+                case 3: kind = role ? 3 : 2; f0 = fbase; break;
+                default: kind = role ? 4 : 3; f0 = fbase; break;
+            }
+            const cplx* __restrict__ p0 = u_in + f0 * P.nz;
+            const cplx* __restrict__ p1 = p0 + P.nz;
 #pragma unroll
-        for (int k2 = 0; k2 < Pn; ++k2) {
-            const int k = t + G::T * k2;
-            const int s = stored_index<G>(k);
-            cplx v = mk(0.0, 0.0);
-            if (s >= 0) {
-                if (which < 4) {
-                    v = ldc(u_in + which * P.nz + s);
-                } else {
-                    const bool mag = (which == 5 || which == 8);
-                    cplx f0 = ldc(u_in + (mag ? 2 : 0) * P.nz + s);
-                    cplx f1 = ldc(u_in + (mag ? 3 : 1) * P.nz + s);
-                    const double c = kzval(kz_int<G>(k), P.kzL);
-                    const bool z0 = (kyi == 0 && s == 0);
-                    const double il2 = ilap2val(lap2val(ky, kz2val(c), z0), z0);
-                    if (which == 7 || which == 8) {
-                        // uy = ((-ky kx) f0 + kz f1) ilap2 = (ab f0 + i c f1) ilap2   (MHD_BQlin.cpp:143)
-                        v = cscale(cadd(cscale(f0, ab), imul(f1, c)), il2);
+            for (int k2 = 0; k2 < Pn; ++k2) {
+                const int k = t + G::T * k2;
+                const int s = stored_index<G>(k);
+                cplx v = mk(0.0, 0.0);
+                if (s >= 0 && kind != 4) {
+                    const cplx g0 = ldc(p0 + s);
+                    if (kind == 0) {
+                        v = g0;
                     } else {
-                        // uz = (-kx kz f0 - ky f1) ilap2 = (a c f0 - i b f1) ilap2   (MHD_BQlin.cpp:144)
-                        v = cscale(csub(cscale(f0, __dmul_rn(a, c)), imul(f1, b)), il2);
-                        if (which == 6) v = imul(v, c);
+                        const cplx g1 = ldc(p1 + s);
+                        const double c = kzval(kz_int<G>(k), P.kzL);
+                        const double il2 = __ldg(il2row + s);
+                        if (kind == 3) {
+                            v = cscale(cadd(cscale(g0, ab), imul(g1, c)), il2);
+                        } else {
+                            v = cscale(csub(cscale(g0, __dmul_rn(a, c)), imul(g1, b)), il2);
+                            if (kind == 2) v = imul(v, c);
+                        }
                     }
                 }
+                x[k2] = cscale(v, fac);
             }
-            x[k2] = cscale(v, fac);
+            inv_fft<G>(x, xch, tw, t, gmask);
         }
-    };
-
-    // Finish one field: x holds fwd(G) in spectral layout; F = x + lin(k); update and store.
-    // f: field index; lin: lambda giving the linear rhs contribution at (k2, s, c)
-    auto finish = [&](int f, auto&& lin) {
+        // ---- real-space products (role-dependent values are selected, not branched:
+        // every TMEM access below is executed by the whole warp)
+        __syncwarp();
+        if (step == 0) {
 #pragma unroll
-        for (int k2 = 0; k2 < Pn; ++k2) {
-            const int k = t + G::T * k2;
-            const int s = stored_index<G>(k);
-            if (s < 0) continue;
-            const double c = kzval(kz_int<G>(k), P.kzL);
-            const double kz2 = kz2val(c);
-            cplx F = lin(k2, s, c, x[k2]);
-            cplx uin = ldc(u_in + f * P.nz + s);
-            cplx fp = (Fp && S.has_prev) ? ldc(Fp + f * P.nz + s) : mk(0.0, 0.0);
-            double L = linop_f<MODEL_BQLIN>(P, lap_end<MODEL_BQLIN>(P, kxe, ky, kz2), f);
-            double Lo = 0.0;
-            if (INTEG == INTEG_CN) {
-                const bool z0 = (kyi == 0 && s == 0);
-                const double lo = cn.old_init ? lap_init<MODEL_BQLIN>(P, kxo, lap2val(ky, kz2, z0))
-                                             : lap_end<MODEL_BQLIN>(P, kxo, ky, kz2);
-                Lo = linop_f<MODEL_BQLIN>(P, lo, f);
+            for (int j = 0; j < Pn; ++j) Kown[j * G::T + t] = x[j];
+            __syncwarp();
+        } else if (step == 1) {
+            // U: Ex += Re(R_bz R_u*), A = -i kx dBy R_u
+            // B: Ex -= Re(R_uz R_b*), A = -i kx dBy R_b + ddBy R_bz
+            const double sg = role ? -mult : mult;
+            const double kdd = role ? 1.0 : 0.0;
+#pragma unroll
+            for (int c4 = 0; c4 < Pn / 4; ++c4) {
+                cplx e[4], av[4];
+                pv.ld4(PB_E, c4, e);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int j = 4 * c4 + i;
+                    const int z = zpos<G>(t, j);
+                    const cplx ko = Koth[j * G::T + t];
+                    e[i].x += sg * (ko.x * x[j].x + ko.y * x[j].y);
+                    av[i] = cadd(imul(x[j], -a * dBy[z]), cscale(Kown[j * G::T + t], kdd * ddBy[z]));
+                    x[j] = imul(x[j], b * By[z]);
+                }
+                __syncwarp();
+                pv.st4(PB_E, c4, e);
+                pv.st4(PB_A, c4, av);
             }
-            if (A.rhs_only) {
-                stc(u_out + f * P.nz + s, F);
-                if (A.linop_out) A.linop_out[((size_t)mode * 4 + f) * P.nz + s] = L;
-            } else {
-                if (Fo) stc(Fo + f * P.nz + s, F);
-                stc(u_out + f * P.nz + s, rk_update<INTEG>(S, L, Lo, F, fp, uin, S.has_prev));
+            pv.st_fence();
+        } else if (step == 2) {
+            // U: A += i ky By R_zeta;  B: G_zeta = A + i ky By R_eta
+#pragma unroll
+            for (int c4 = 0; c4 < Pn / 4; ++c4) {
+                cplx av[4];
+                pv.ld4(PB_A, c4, av);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int j = 4 * c4 + i;
+                    av[i] = cadd(av[i], imul(x[j], b * By[zpos<G>(t, j)]));
+                    x[j] = av[i];
+                }
+                pv.st4(PB_A, c4, av);
+            }
+            pv.st_fence();
+        } else if (step == 3) {
+            // U: G_eta = A - 2 dBy R_{i kz uz} - ddBy R_uz       (MHD_BQlin.cpp:189-198)
+            // B: Ey -= Re(R_uz R_by*);  G_u2 = 2ab dBy R_bz       (MHD_BQlin.cpp:156-158,232-240)
+            const double sgy = role ? -mult : 0.0;
+#pragma unroll
+            for (int c4 = 0; c4 < Pn / 4; ++c4) {
+                cplx e[4], av[4];
+                pv.ld4(PB_E, c4, e);
+                pv.ld4(PB_A, c4, av);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int j = 4 * c4 + i;
+                    const int z = zpos<G>(t, j);
+                    const cplx ko = Koth[j * G::T + t];
+                    const cplx kw = Kown[j * G::T + t];
+                    e[i].y += sgy * (ko.x * x[j].x + ko.y * x[j].y);
+                    const cplx gu = csub(cadd(av[i], cscale(x[j], -2.0 * dBy[z])), cscale(kw, ddBy[z]));
+                    const cplx gb = cscale(kw, 2.0 * ab * dBy[z]);
+                    x[j] = role ? gb : gu;
+                }
+                __syncwarp();
+                pv.st4(PB_E, c4, e);
+            }
+            pv.st_fence();
+        } else {
+            // step 4, U: Ey += Re(R_bz R_uy*)  (B contributes zero)
+            const double sgy = role ? 0.0 : mult;
+#pragma unroll
+            for (int c4 = 0; c4 < Pn / 4; ++c4) {
+                cplx e[4];
+                pv.ld4(PB_E, c4, e);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int j = 4 * c4 + i;
+                    const cplx ko = Koth[j * G::T + t];
+                    e[i].y += sgy * (ko.x * x[j].x + ko.y * x[j].y);
+                }
+                pv.st4(PB_E, c4, e);
+            }
+            pv.st_fence();
+            break;
+        }
+        // ---- forward transform and the update of one field
+        fwd_fft<G>(x, xch, tw, t, gmask);
+        __syncwarp();
+        if (step == 1) {
+            // B keeps fwd(i ky By R_b) for F_u (the U lanes store into their own, unused, buffer)
+#pragma unroll
+            for (int c4 = 0; c4 < Pn / 4; ++c4) pv.st4(PB_S, c4, x + 4 * c4);
+            pv.st_fence();
+        }
+        const int f = fupd;  // field this group updates now (-1/-2: none)
+        const cplx* __restrict__ fin = u_in + (f < 0 ? 0 : f) * P.nz;
+        const cplx* __restrict__ lin0 = u_in + (f == 3 ? 2 : 0) * P.nz;
+        const cplx* __restrict__ zin = u_in + P.nz;
+        const cplx* fpp = Fp ? ps.fpb : nullptr;
+        cplx* __restrict__ outp = u_out + (f < 0 ? 0 : f) * P.nz;
+        cplx* __restrict__ fop = Fo ? Fo + (f < 0 ? 0 : f) * P.nz : nullptr;
+        const double* ekzt = (f < 2) ? TB.ekz_u : TB.ekz_b;
+        const double em = (f < 2) ? em_u : em_b;
+        if (Fp) {
+            cp_async_wait_all();
+            __syncwarp(gmask);
+        }
+#pragma unroll
+        for (int c4 = 0; c4 < Pn / 4; ++c4) {
+            cplx sv[4];
+            __syncwarp();
+            if (step == 3) pv.ld4(PB_S, c4, sv);  // warp-uniform
+            if (f < 0 || !valid) continue;
+            cplx uin[4], fpv[4], l0[4], l1[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int s = stored_index<G>(t + G::T * (4 * c4 + i));
+                const int sl = s < 0 ? 0 : s;
+                uin[i] = ldc(fin + sl);
+                fpv[i] = fpp ? fpp[sl] : mk(0.0, 0.0);
+                l0[i] = ldc(lin0 + sl);
+                l1[i] = f == 0 ? ldc(zin + sl) : mk(0.0, 0.0);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int k2 = 4 * c4 + i;
+                const int k = t + G::T * k2;
+                const int s = stored_index<G>(k);
+                if (s < 0) continue;
+                const double c = kzval(kz_int<G>(k), P.kzL);
+                const double kz2 = kz2val(c);
+                cplx F;
+                if (f == 2) {
+                    F = x[k2];                                      // F_b (MHD_BQlin.cpp:182-185)
+                } else if (f == 3) {
+                    F = csub(x[k2], imul(l0[i], P.q * c));          // F_eta (:201)
+                } else if (f == 1) {
+                    F = cadd(x[k2], imul(l0[i], (P.q - Om2) * c));  // F_zeta (:178)
+                } else {
+                    // F_u (:162): ilapF = 1/(-kx^2 + lap2) with the kx=ky=kz=0 fix (:505-507)
+                    const bool z0 = (kyi == 0 && s == 0);
+                    const double lapF = __dadd_rn(-__dmul_rn(a, a), lap2val(ky, kz2, z0));
+                    const double ilapF = (z0 && kxi == 0) ? 1.0 : __drcp_rn(lapF);
+                    const cplx lin = cadd(cadd(cscale(l0[i], __dmul_rn(__dmul_rn(2.0, ab), P.q)),
+                                               imul(l1[i], Om2 * c)),
+                                          x[k2]);
+                    F = cadd(sv[i], cscale(lin, ilapF));
+                }
+                if (A.rhs_only) {
+                    stc(outp + s, F);
+                    if (A.linop_out)
+                        A.linop_out[((size_t)mode * 4 + f) * P.nz + s] =
+                            linop_f<MODEL_BQLIN>(P, lap_end<MODEL_BQLIN>(P, kxe, ky, kz2), f);
+                    continue;
+                }
+                cplx nv;
+                if (INTEG == INTEG_EXP) {
+                    const double e = em * ekzt[s];
+                    const cplx acc = fpp ? cadd(cadd(cscale(F, S.n1), cscale(fpv[i], S.n2)), uin[i])
+                                         : cadd(cscale(F, S.n1), uin[i]);
+                    nv = cscale(acc, e);
+                } else {
+                    const double L = linop_f<MODEL_BQLIN>(P, lap_end<MODEL_BQLIN>(P, kxe, ky, kz2), f);
+                    const bool z0 = (kyi == 0 && s == 0);
+                    const double lo = cn.old_init ? lap_init<MODEL_BQLIN>(P, kxo, lap2val(ky, kz2, z0))
+                                                  : lap_end<MODEL_BQLIN>(P, kxo, ky, kz2);
+                    nv = rk_update<INTEG_CN>(S, L, linop_f<MODEL_BQLIN>(P, lo, f), F, fpv[i], uin[i],
+                                             fpp != nullptr);
+                }
+                if (fop) stc(fop + s, F);
+                stc(outp + s, nv);
             }
         }
-    };
-
-    // 1. R_bz -> K1
-    load(5);
-    inv_fft<G>(x, xch, tw, t, gmask);
-#pragma unroll
-    for (int j = 0; j < Pn; ++j) PRIV(K1, j) = x[j];
-    // 2. R_uz -> K2
-    load(4);
-    inv_fft<G>(x, xch, tw, t, gmask);
-#pragma unroll
-    for (int j = 0; j < Pn; ++j) PRIV(K2, j) = x[j];
-    // 3. R_u: EMF_x += Re(bz conj u); A1 = -i a dzBy R_u; G_b = i b By R_u -> F_b
-    load(0);
-    inv_fft<G>(x, xch, tw, t, gmask);
-#pragma unroll
-    for (int j = 0; j < Pn; ++j) {
-        const int z = zpos<G>(t, j);
-        cplx k1 = PRIV(K1, j);
-        emfx[j] += mult * (k1.x * x[j].x + k1.y * x[j].y);
-        PRIV(A1, j) = imul(x[j], -a * dBy[z]);
-        x[j] = imul(x[j], b * By[z]);
+        __syncwarp();
     }
-    fwd_fft<G>(x, xch, tw, t, gmask);
-    finish(2, [&](int, int, double, cplx g) { return g; });  // F_b = fwd(ky By u)  (MHD_BQlin.cpp:182-185)
-    // 4. R_zeta: A1 += i b By R_zeta
-    load(1);
-    inv_fft<G>(x, xch, tw, t, gmask);
-#pragma unroll
-    for (int j = 0; j < Pn; ++j) {
-        const int z = zpos<G>(t, j);
-        PRIV(A1, j) = cadd(PRIV(A1, j), imul(x[j], b * By[z]));
-    }
-    // 5. R_{i kz uz}: G_eta = A1 - 2 dzBy R_kzuz - ddBy R_uz -> F_eta
-    load(6);
-    inv_fft<G>(x, xch, tw, t, gmask);
-#pragma unroll
-    for (int j = 0; j < Pn; ++j) {
-        const int z = zpos<G>(t, j);
-        cplx g = cadd(PRIV(A1, j), cscale(x[j], -2.0 * dBy[z]));
-        x[j] = csub(g, cscale(PRIV(K2, j), ddBy[z]));
-    }
-    fwd_fft<G>(x, xch, tw, t, gmask);
-    {
-        const cplx* bin = u_in + 2 * P.nz;
-        // F_eta = fwd(..) - q kz b   (MHD_BQlin.cpp:201)
-        finish(3, [&](int, int s, double c, cplx g) { return csub(g, imul(ldc(bin + s), P.q * c)); });
-    }
-    // 6. R_b: EMF_x -= Re(uz conj b); A1 = -i a dzBy R_b + ddBy R_bz; A2 = fwd(i b By R_b)
-    load(2);
-    inv_fft<G>(x, xch, tw, t, gmask);
-#pragma unroll
-    for (int j = 0; j < Pn; ++j) {
-        const int z = zpos<G>(t, j);
-        cplx k2v = PRIV(K2, j);
-        emfx[j] -= mult * (k2v.x * x[j].x + k2v.y * x[j].y);
-        PRIV(A1, j) = cadd(imul(x[j], -a * dBy[z]), cscale(PRIV(K1, j), ddBy[z]));
-        x[j] = imul(x[j], b * By[z]);
-    }
-    fwd_fft<G>(x, xch, tw, t, gmask);
-#pragma unroll
-    for (int k2 = 0; k2 < Pn; ++k2) PRIV(A2, k2) = x[k2];
-    // 7. R_eta: G_zeta = A1 + i b By R_eta -> F_zeta
-    load(3);
-    inv_fft<G>(x, xch, tw, t, gmask);
-#pragma unroll
-    for (int j = 0; j < Pn; ++j) {
-        const int z = zpos<G>(t, j);
-        x[j] = cadd(PRIV(A1, j), imul(x[j], b * By[z]));
-    }
-    fwd_fft<G>(x, xch, tw, t, gmask);
-    {
-        const cplx* uin0 = u_in;
-        const double qm = P.q - Om2;
-        // F_zeta = fwd(..) + (q - 2 Omega) kz u   (MHD_BQlin.cpp:178)
-        finish(1, [&](int, int s, double c, cplx g) { return cadd(g, imul(ldc(uin0 + s), qm * c)); });
-    }
-    // 8. G_u2 = 2ab dzBy R_bz -> F_u = A2 + ilapF (2abq u + 2 Omega kz zeta + fwd(G_u2))
-#pragma unroll
-    for (int j = 0; j < Pn; ++j) {
-        const int z = zpos<G>(t, j);
-        x[j] = cscale(PRIV(K1, j), 2.0 * ab * dBy[z]);
-    }
-    fwd_fft<G>(x, xch, tw, t, gmask);
-    {
-        const cplx* uin0 = u_in;
-        const cplx* zin = u_in + P.nz;
-        const double c2 = __dmul_rn(__dmul_rn(2.0, ab), P.q);
-        finish(0, [&](int k2, int s, double c, cplx g) {
-            // MHD_BQlin.cpp:162, ilapF = 1/(-kx^2 + lap2) with the kx=ky=kz=0 fix (:505-507)
-            const bool z0 = (kyi == 0 && s == 0);
-            const double lapF = __dadd_rn(-__dmul_rn(a, a), lap2val(ky, kz2val(c), z0));
-            const double ilapF = (z0 && kxi == 0) ? 1.0 : __drcp_rn(lapF);
-            cplx lin = cadd(cadd(cscale(ldc(uin0 + s), c2), imul(ldc(zin + s), Om2 * c)), g);
-            return cadd(PRIV(A2, k2), cscale(lin, ilapF));
-        });
-    }
-    // 9-10. EMF_y = Re(bz conj uy) - Re(uz conj by)
-    load(7);
-    inv_fft<G>(x, xch, tw, t, gmask);
-#pragma unroll
-    for (int j = 0; j < Pn; ++j) {
-        cplx k1 = PRIV(K1, j);
-        emfy[j] += mult * (k1.x * x[j].x + k1.y * x[j].y);
-    }
-    load(8);
-    inv_fft<G>(x, xch, tw, t, gmask);
-#pragma unroll
-    for (int j = 0; j < Pn; ++j) {
-        cplx k2v = PRIV(K2, j);
-        emfy[j] -= mult * (k2v.x * x[j].x + k2v.y * x[j].y);
-    }
-#undef PRIV
 }
 
 }  // namespace qlgpu

@@ -71,7 +71,8 @@ struct StageArgs {
     const double* ky;
     const int* kxi;
     const int* kyi;
-    const cplx* tw;  // twiddles exp(2 pi i n2 t/NZ), [P][T]
+    const cplx* tw;         // twiddles exp(2 pi i n2 t/NZ), [P][T]
+    const double* ilap2;    // [Ny/2][nz] 1/lap2 table (Kdata.cpp:100-119)
     double* partials;       // [grid][PL]
     double* gpartials;      // [ngroups][PL]
     DevClock* clk;
@@ -79,6 +80,7 @@ struct StageArgs {
     int diag_cap;
     int rhs_only;           // Model::rhs: write F (and linop) only, no update
     double* linop_out;      // rhs_only: [nxy][4][nz]
+    unsigned long long* trace;  // optional %globaltimer trace (null: off), see qlgpu_kernel.cuh
     StageConst sc;
 };
 

@@ -99,6 +99,12 @@ class QLSolver:
         _capi.check(self.L.qlgpu_step(self.h, int(nsteps), 0, None, 0, None), self.h)
         return np.zeros((0, 15))
 
+    def step_timed(self) -> np.ndarray:
+        """One step; returns the device time (ms) of each of its three stage kernels."""
+        ms = (ctypes.c_float * 3)()
+        _capi.check(self.L.qlgpu_step_timed(self.h, ms), self.h)
+        return np.array(list(ms), dtype=np.float64)
+
     def diagnostics(self) -> np.ndarray:
         out = np.zeros(15)
         _capi.check(self.L.qlgpu_diagnostics(self.h, _capi.dptr(out)), self.h)
