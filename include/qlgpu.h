@@ -117,6 +117,17 @@ int qlgpu_status(qlgpu_t* h, int* status);
  * ql_dns_b200/csrc/qlgpu_kernel.cuh).  Returns QLGPU_ERR_UNSUPPORTED when off. */
 int qlgpu_trace(qlgpu_t* h, unsigned long long* out96);
 
+/* Launch geometry of the stage kernel: info8 = {grid, block, dynamic shared
+ * bytes, CTAs per SM, TMEM columns per CTA, threads per transform, modes, warps
+ * per CTA}. */
+int qlgpu_launch_info(const qlgpu_t* h, int* info8);
+
+/* Compiled attributes of the stage kernel: attrs8 = {registers per thread,
+ * static shared bytes, local bytes per thread, max threads per block,
+ * CTAs per SM without / with the dynamic shared memory, max dynamic shared
+ * bytes, preferred carveout}. */
+int qlgpu_kernel_attrs(const qlgpu_t* h, int* attrs8);
+
 /* Current simulation time and the CUDA stream (cudaStream_t) of the handle. */
 int qlgpu_time(qlgpu_t* h, double* t);
 int qlgpu_stream(qlgpu_t* h, void** stream);

@@ -20,7 +20,9 @@ ERRORS = {1: "QLGPU_ERR_ARG", 2: "QLGPU_ERR_UNSUPPORTED", 3: "QLGPU_ERR_CUDA", 4
 # Every symbol include/qlgpu.h declares.
 EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "qlgpu_get_state",
            "qlgpu_set_state_device", "qlgpu_get_state_device", "qlgpu_step", "qlgpu_step_timed", "qlgpu_diagnostics",
-           "qlgpu_rhs", "qlgpu_status", "qlgpu_time", "qlgpu_trace", "qlgpu_stream", "qlgpu_last_error",
+           "qlgpu_rhs", "qlgpu_status", "qlgpu_time", "qlgpu_trace", "qlgpu_launch_info", "qlgpu_kernel_attrs",
+           "qlgpu_stream",
+           "qlgpu_last_error",
            "qlgpu_version"]
 
 
@@ -71,6 +73,8 @@ def load(path: str = LIB_PATH):
     L.qlgpu_status.argtypes = [vp, ip]
     L.qlgpu_time.argtypes = [vp, dp]
     L.qlgpu_trace.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
+    L.qlgpu_launch_info.argtypes = [vp, ip]
+    L.qlgpu_kernel_attrs.argtypes = [vp, ip]
     L.qlgpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.qlgpu_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.qlgpu_version.restype = ctypes.c_char_p

@@ -134,13 +134,16 @@ struct qlgpu_handle {
     double* d_linop = nullptr;
     double* d_ilap2 = nullptr;
     int tmem_cols = 0;
-    unsigned long long* d_trace = nullptr;  // QLGPU_TRACE=1: %globaltimer stamps of each stage
+    int per_sm = 0;
+    unsigned long long* d_trace = nullptr;
+    double* d_mfr = nullptr;  // [8][NZ] mean-field profile cache
+    double* d_ekz = nullptr;  // [3 stages][2][nz]  // QLGPU_TRACE=1: %globaltimer stamps of each stage
     int grid = 0, warps = 4, block = 128;
     size_t smem = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<double> kx_tab, ky_tab;
     std::vector<int> kxi_tab, kyi_tab;
-    std::vector<double> il2_tab;
+    std::vector<double> il2_tab, ekz_tab;
     std::string err;
 };
 
@@ -211,6 +214,7 @@ StageArgs base_args(qlgpu_t* h) {
     A.diag_ring = h->d_diag;
     A.diag_cap = h->diag_cap;
     A.trace = h->d_trace;
+    A.mfr_cache = h->d_mfr;
     return A;
 }
 
@@ -249,6 +253,7 @@ void enqueue_step(qlgpu_t* h, cudaEvent_t* ev = nullptr) {
         A.sc.has_prev = st[s].has_prev;
         A.sc.last = (s == 2);
         if (A.trace) A.trace += 32 * s;
+        A.ekz_tab = h->d_ekz + (size_t)s * 2 * h->nz;
         h->var.launch(A, h->dp, h->grid, h->block, h->smem, h->stream);
         if (ev) cudaEventRecord(ev[s + 1], h->stream);
         h->cur ^= 1;
@@ -367,22 +372,59 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
         h->err = "cudaGetDeviceProperties failed";
         return bail(QLGPU_ERR_CUDA);
     }
-    // 4 warps per CTA when the shared-memory footprint allows, else fewer
-    h->warps = 4;
-    while (h->warps > 1 && var.smem(h->warps) > (size_t)prop.sharedMemPerBlockOptin) h->warps >>= 1;
+    // CTA width: the number of warps (8, 4, 2 or 1) that maximises resident warps per SM,
+    // given shared memory, registers and (for the TMEM store) 512 TMEM columns per SM.
+    int best_w = 1, best_res = -1, best_per_sm = 1;
+    for (int w = 8; w >= 1; w >>= 1) {
+        const size_t sm_bytes = var.smem(w);
+        if (sm_bytes > (size_t)prop.sharedMemPerBlockOptin) continue;
+        if (cudaFuncSetAttribute(var.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_bytes) !=
+            cudaSuccess)
+            continue;
+        const int tc = var.tmem(w);
+        if (tc > 512) continue;
+        int want = tc > 0 ? 512 / tc : 32;
+        const size_t per_cta = sm_bytes + 1024;
+        while (want > 1 && per_cta * want > (size_t)prop.sharedMemPerMultiprocessor) --want;
+        int pct = (int)((100.0 * per_cta * want) / (double)prop.sharedMemPerMultiprocessor + 0.999);
+        if (pct > 100) pct = 100;
+        cudaFuncSetAttribute(var.kernel(), cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, var.kernel(), 32 * w, sm_bytes);
+        if (tc > 0 && occ > 512 / tc) occ = 512 / tc;
+        if (occ < 1) continue;
+        const int modes_per_cta = w * (32 / var.T) / 2;
+        // resident modes per SM, capped by the work available
+        int res = occ * modes_per_cta;
+        const int per_sm_need = (h->nxy + prop.multiProcessorCount - 1) / prop.multiProcessorCount;
+        if (res > per_sm_need) res = per_sm_need + (occ * w);  // prefer wider CTAs once the work fits
+        if (res > best_res) {
+            best_res = res;
+            best_w = w;
+            best_per_sm = occ;
+        }
+    }
+    h->warps = best_w;
     h->block = 32 * h->warps;
     h->smem = var.smem(h->warps);
     if (cudaFuncSetAttribute(var.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem) != cudaSuccess) {
         h->err = "shared memory request too large";
         return bail(QLGPU_ERR_CUDA);
     }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, var.kernel(), h->block, h->smem);
+    {
+        int want = var.tmem(h->warps) > 0 ? 512 / var.tmem(h->warps) : 32;
+        const size_t per_cta = h->smem + 1024;
+        while (want > 1 && per_cta * want > (size_t)prop.sharedMemPerMultiprocessor) --want;
+        int pct = (int)((100.0 * per_cta * want) / (double)prop.sharedMemPerMultiprocessor + 0.999);
+        if (pct > 100) pct = 100;
+        cudaFuncSetAttribute(var.kernel(), cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    }
     h->tmem_cols = var.tmem(h->warps);
-    if (h->tmem_cols > 0 && per_sm > 512 / h->tmem_cols) per_sm = 512 / h->tmem_cols;  // TMEM: 512 columns per SM
-    if (per_sm < 1) per_sm = 1;
-    const int groups_per_cta = h->warps * (32 / var.T);
-    int need = (h->nxy + groups_per_cta - 1) / groups_per_cta;
+    int per_sm = best_per_sm;
+    h->per_sm = per_sm;
+    // one mode per pair of transform groups
+    const int modes_per_cta = h->warps * (32 / var.T) / 2;
+    int need = (h->nxy + modes_per_cta - 1) / modes_per_cta;
     int cap = prop.multiProcessorCount * per_sm;
     h->grid = need < cap ? need : cap;
     if (h->grid > 64 * RED_GROUP) h->grid = 64 * RED_GROUP;
@@ -417,6 +459,8 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
     QLGPU_ALLOC(h->d_clk, sizeof(DevClock));
     QLGPU_ALLOC(h->d_out15, 15 * sizeof(double));
     QLGPU_ALLOC(h->d_ilap2, (size_t)(p.ny / 2) * h->nz * sizeof(double));
+    QLGPU_ALLOC(h->d_mfr, (size_t)8 * h->NZ * sizeof(double));
+    QLGPU_ALLOC(h->d_ekz, (size_t)6 * h->nz * sizeof(double));
     // Twiddles tw[n2*T + t] = exp(+2 pi i n2 t/NZ)
     std::vector<cplx> tw(h->NZ);
     const int T = var.T, P = h->NZ / T;
@@ -445,6 +489,24 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
                 h->il2_tab[(size_t)j * h->nz + s] = il2;
             }
         }
+    }
+    {
+        // exp(linC nu kz2), exp(linC (eta/nu) nu kz2) per stage (RK3CN_Elin.cpp:89,122,155)
+        const double dt = p.dt;
+        const double linC[3] = {dt * (a0_), dt * (a1_ + b1_), dt * (a2_ + b2_)};
+        const double kzL = 2 * kPI / p.L[2];
+        const int nzl = (h->nz - 1) / 2;
+        h->ekz_tab.assign((size_t)6 * h->nz, 1.0);
+        for (int st = 0; st < 3; ++st)
+            for (int s = 0; s < h->nz; ++s) {
+                const int kzi = s <= nzl ? s : s - h->nz;
+                const double c = kzi * kzL;
+                const double kz2 = -(c * c);
+                h->ekz_tab[(size_t)(st * 2) * h->nz + s] = std::exp(linC[st] * d.nu * kz2);
+                h->ekz_tab[(size_t)(st * 2 + 1) * h->nz + s] = std::exp(linC[st] * d.etanu * d.nu * kz2);
+            }
+        cudaMemcpyAsync(h->d_ekz, h->ekz_tab.data(), h->ekz_tab.size() * sizeof(double), cudaMemcpyHostToDevice,
+                        h->stream);
     }
     cudaMemcpyAsync(h->d_ilap2, h->il2_tab.data(), h->il2_tab.size() * sizeof(double), cudaMemcpyHostToDevice,
                     h->stream);
@@ -475,7 +537,8 @@ int qlgpu_destroy(qlgpu_t* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     void* bufs[] = {h->d_lin[0], h->d_lin[1], h->d_F1, h->d_F2, h->d_mf, h->d_Fmf1, h->d_Fmf2,
                     h->d_kx0, h->d_ky, h->d_kxi, h->d_kyi, h->d_tw, h->d_partials, h->d_gpartials,
-                    h->d_clk, h->d_diag, h->d_out15, h->d_linop, h->d_ilap2, h->d_trace};
+                    h->d_clk, h->d_diag, h->d_out15, h->d_linop, h->d_ilap2, h->d_trace,
+                    h->d_mfr, h->d_ekz};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : h->ev)
@@ -666,6 +729,37 @@ int qlgpu_trace(qlgpu_t* h, unsigned long long* out96) {
     QLGPU_CK(cudaSetDevice(h->device));
     QLGPU_CK(cudaMemcpyAsync(out96, h->d_trace, 96 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
     QLGPU_CK(cudaStreamSynchronize(h->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_launch_info(const qlgpu_t* h, int* info8) {
+    if (!h || !info8) return QLGPU_ERR_ARG;
+    info8[0] = h->grid;
+    info8[1] = h->block;
+    info8[2] = (int)h->smem;
+    info8[3] = h->per_sm;
+    info8[4] = h->tmem_cols;
+    info8[5] = h->var.T;
+    info8[6] = h->nxy;
+    info8[7] = h->warps;
+    return QLGPU_OK;
+}
+
+int qlgpu_kernel_attrs(const qlgpu_t* h, int* attrs8) {
+    if (!h || !attrs8) return QLGPU_ERR_ARG;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, h->var.kernel()) != cudaSuccess) return QLGPU_ERR_CUDA;
+    int occ0 = 0, occs = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, h->var.kernel(), h->block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occs, h->var.kernel(), h->block, h->smem);
+    attrs8[0] = fa.numRegs;
+    attrs8[1] = (int)fa.sharedSizeBytes;
+    attrs8[2] = (int)fa.localSizeBytes;
+    attrs8[3] = fa.maxThreadsPerBlock;
+    attrs8[4] = occ0;
+    attrs8[5] = occs;
+    attrs8[6] = fa.maxDynamicSharedSizeBytes;
+    attrs8[7] = fa.preferredShmemCarveout;
     return QLGPU_OK;
 }
 

@@ -233,11 +233,11 @@ struct Smem {
     static constexpr size_t o_spec = o_ekz + sizeof(double) * 2 * ((NZD + 1) & ~1);
     static constexpr size_t o_tot = o_spec + sizeof(double) * 2 * NEMF * (G::H + 1);
     static constexpr size_t o_work = o_tot + sizeof(double) * ((PL + 1) & ~1);
-    // per group: F_prev prefetch buffer (nz cplx); per pair of groups: R_uz, R_bz (2 NZ cplx)
-    static constexpr size_t GS_BYTES = sizeof(cplx) * (NZD + G::NZ);
+    // per pair of groups: R_uz, R_bz (2 NZ cplx), i.e. NZ cplx per group
+    static constexpr size_t GS_BYTES = sizeof(cplx) * G::NZ;
     __host__ __device__ static size_t work_bytes(int warps) {
         const size_t xch = sizeof(cplx) * (size_t)warps * SW * G::XSIZE;
-        const size_t red = sizeof(double) * ((size_t)warps * SW * NEMF * G::NZ + (size_t)warps * 32 * 6);
+        const size_t red = sizeof(double) * ((size_t)warps * NEMF * G::NZ + (size_t)warps * 32 * 6);
         return xch > red ? xch : red;
     }
     __host__ __device__ static size_t bytes(int warps) {
@@ -254,7 +254,7 @@ struct Smem {
 };
 
 template <int NZ, int MODEL, int INTEG, bool USE_TMEM>
-__global__ void __launch_bounds__(128, 1) stage_kernel(StageArgs A, DevParams P) {
+__global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
     using G = Geom<NZ>;
     using Priv = typename std::conditional<USE_TMEM, PrivTmem<G, PB_COUNT>, PrivSmem<G, PB_COUNT>>::type;
     using SM = Smem<G, MODEL, Priv>;
@@ -285,7 +285,9 @@ __global__ void __launch_bounds__(128, 1) stage_kernel(StageArgs A, DevParams P)
     // [2] mode loop done, [3] partials written, [4] top CTA start, [5] top done,
     // [8] first mode staged, [9..18] start of pipeline steps 0..9
     const bool tr = A.trace && blockIdx.x == 0 && tid == 0;
+    const bool tr2 = A.trace && blockIdx.x == gridDim.x - 1 && tid == 0;
     if (tr) A.trace[0] = gtimer();
+    if (tr2) A.trace[20] = gtimer();
     // ---- private store: TMEM allocation (one warp) or a shared-memory region
     Priv pv;
     const int tcols = SM::tmem_cols(warps);
@@ -305,9 +307,7 @@ __global__ void __launch_bounds__(128, 1) stage_kernel(StageArgs A, DevParams P)
     PairShared ps;
     {
         unsigned char* gbase = work + SM::work_bytes(warps) + Priv::smem_bytes_per_warp() * (size_t)warps;
-        cplx* fpb_all = reinterpret_cast<cplx*>(gbase);
-        cplx* k_all = fpb_all + (size_t)warps * SW * SM::NZD;
-        ps.fpb = fpb_all + (size_t)gidx * SM::NZD;
+        cplx* k_all = reinterpret_cast<cplx*>(gbase);
         cplx* kpair = k_all + (size_t)(warp * (SW / 2) + pi) * 2 * G::NZ;
         ps.KU = kpair;
         ps.KB = kpair + G::NZ;
@@ -328,20 +328,31 @@ __global__ void __launch_bounds__(128, 1) stage_kernel(StageArgs A, DevParams P)
     // factored integrating factor tables exp(linC c kz2), per stored kz
     if (INTEG == INTEG_EXP) {
         for (int s = tid; s < nzd; s += blockDim.x) {
-            const int kzi = s <= G::H ? s : s - nzd;
-            const double kz2 = kz2val(kzval(kzi, P.kzL));
-            ekz[s] = exp(S.linC * P.nu * kz2);
-            ekz[SM::NZD + (SM::NZD & 1) + s] = exp(S.linC * P.etanu * P.nu * kz2);
+            if (A.ekz_tab) {
+                ekz[s] = __ldg(A.ekz_tab + s);
+                ekz[SM::NZD + (SM::NZD & 1) + s] = __ldg(A.ekz_tab + nzd + s);
+            } else {
+                const int kzi = s <= G::H ? s : s - nzd;
+                const double kz2 = kz2val(kzval(kzi, P.kzL));
+                ekz[s] = exp(S.linC * P.nu * kz2);
+                ekz[SM::NZD + (SM::NZD & 1) + s] = exp(S.linC * P.etanu * P.nu * kz2);
+            }
         }
     }
+    const bool mfr_cached = A.mfr_cache && !A.rhs_only && __ldcg(&A.clk->mfr_valid);
+    if (mfr_cached)
+        for (int i = tid; i < SM::NMFR * G::NZ; i += blockDim.x) mfr[i] = __ldcg(A.mfr_cache + i);
     StageTables TB;
     TB.ekz_u = ekz;
     TB.ekz_b = ekz + SM::NZD + (SM::NZD & 1);
     TB.ilap2 = A.ilap2;
     __syncthreads();
-    mean_profiles<G, MODEL>(P, A.mf, mfr, xch, tw_s, gidx, ngc, t, gmask);
-    __syncthreads();
+    if (!mfr_cached) {
+        mean_profiles<G, MODEL>(P, A.mf, mfr, xch, tw_s, gidx, ngc, t, gmask);
+        __syncthreads();
+    }
     if (tr) A.trace[1] = gtimer();
+    if (tr2) A.trace[21] = gtimer();
 
     // Last-stage bookkeeping identical in every CTA (main.cpp:111-130)
     const double t_new = __dadd_rn(tclock, P.dt);
@@ -356,6 +367,7 @@ __global__ void __launch_bounds__(128, 1) stage_kernel(StageArgs A, DevParams P)
 
     // ---- mode loop: one mode per pair of groups, warp-uniform trip count (TMEM access is warp-wide)
     constexpr int PW = SW / 2;  // pairs per warp
+    if (tr) A.trace[6] = gtimer();
     const int wglobal = blockIdx.x * warps + warp;
     const int WG = gridDim.x * warps;
     for (int base = wglobal * PW; base < P.nxy; base += WG * PW) {
@@ -397,19 +409,30 @@ __global__ void __launch_bounds__(128, 1) stage_kernel(StageArgs A, DevParams P)
     // ---- CTA reduction of the stress profiles and diagnostics (fixed order)
     __syncthreads();
     if (tr) A.trace[2] = gtimer();
-    double* red = reinterpret_cast<double*>(work);  // [ngc][NEMF][NZ] then [blockDim][6]
+    if (tr2) A.trace[22] = gtimer();
+    double* red = reinterpret_cast<double*>(work);  // [warps][NEMF][NZ] then [blockDim][6]
 #pragma unroll
     for (int c4 = 0; c4 < G::P / 4; ++c4) {
         cplx e[4];
         pv.ld4(PB_E, c4, e);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int z = zpos<G>(t, 4 * c4 + i);
-            red[(gidx * NEMF + 0) * G::NZ + z] = e[i].x;
-            red[(gidx * NEMF + 1) * G::NZ + z] = e[i].y;
+            // groups of a warp own the same z set (lane t of each group): sum them in lane order
+            double ex = e[i].x, ey = e[i].y;
+            double sx = 0.0, sy = 0.0;
+#pragma unroll
+            for (int g = 0; g < SW; ++g) {
+                sx += __shfl_sync(0xffffffffu, ex, g * G::T + t);
+                sy += __shfl_sync(0xffffffffu, ey, g * G::T + t);
+            }
+            if (slot == 0) {
+                const int z = zpos<G>(t, 4 * c4 + i);
+                red[(warp * NEMF + 0) * G::NZ + z] = sx;
+                red[(warp * NEMF + 1) * G::NZ + z] = sy;
+            }
         }
     }
-    double* dred = red + (size_t)ngc * NEMF * G::NZ;
+    double* dred = red + (size_t)warps * NEMF * G::NZ;
 #pragma unroll
     for (int c = 0; c < 6; ++c) dred[tid * 6 + c] = dacc[c];
     if constexpr (USE_TMEM) tmem_fence_before_sync();
@@ -421,7 +444,7 @@ __global__ void __launch_bounds__(128, 1) stage_kernel(StageArgs A, DevParams P)
     double* part = A.partials + (size_t)blockIdx.x * PL;
     for (int idx = tid; idx < NEMF * G::NZ; idx += blockDim.x) {
         double s = 0.0;
-        for (int g = 0; g < ngc; ++g) s += red[g * NEMF * G::NZ + idx];
+        for (int w = 0; w < warps; ++w) s += red[w * NEMF * G::NZ + idx];
         part[idx] = s;
     }
     if (tid < 6) {
@@ -471,6 +494,16 @@ __global__ void __launch_bounds__(128, 1) stage_kernel(StageArgs A, DevParams P)
     __syncthreads();
     mean_field_stage<G, MODEL, INTEG, NEMF>(A, P, tot, spec, xch, tw_s, gidx, ngc, t, gmask, tclock, t_new, last,
                                            diag_due);
+    if (A.mfr_cache && !A.rhs_only) {
+        // real-space profiles of the updated mean field for the next stage
+        __syncthreads();
+        mean_profiles<G, MODEL>(P, A.mf, mfr, xch, tw_s, gidx, ngc, t, gmask);
+        __syncthreads();
+        for (int i = tid; i < SM::NMFR * G::NZ; i += blockDim.x) A.mfr_cache[i] = mfr[i];
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) A.clk->mfr_valid = 1;
+    }
     if (A.trace && tid == 0) A.trace[5] = gtimer();
 }
 

@@ -41,7 +41,7 @@ __device__ __forceinline__ cplx imul(cplx a, double s) { return mk(-a.y * s, a.x
 
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long v;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(v));
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(v)::"memory");
     return v;
 }
 
@@ -171,9 +171,8 @@ enum { PB_E = 0, PB_A = 1, PB_S = 2, PB_COUNT = 3 };
 // `valid` is false for the padding pairs of the last pass (no stores, no sums).
 // ---------------------------------------------------------------------------
 struct PairShared {
-    cplx* KU;   // R_uz, [P][T]
-    cplx* KB;   // R_bz, [P][T]
-    cplx* fpb;  // this group's F_prev prefetch buffer [nz]
+    cplx* KU;  // R_uz, [P][T]
+    cplx* KB;  // R_bz, [P][T]
 };
 
 template <class G, int INTEG, class Priv>
@@ -184,6 +183,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
     constexpr int Pn = G::P;
     const StageConst& S = A.sc;
     const double fac = P.fac;
+    if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) A.trace[7] = gtimer();
     const double ky = __ldg(A.ky + mode);
     const double kx0 = A.kx0[mode];
     const int kyi = __ldg(A.kyi + mode), kxi = __ldg(A.kxi + mode);
@@ -232,13 +232,6 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
         if (step == 1) fupd = role ? -2 : 2;  // B: S buffer
         if (step == 2) fupd = role ? 1 : -1;
         if (step == 3) fupd = role ? 0 : 3;
-        // prefetch F of the previous stage for the field being updated
-        if (Fp && fupd >= 0) {
-            __syncwarp(gmask);
-            const cplx* src = Fp + fupd * P.nz;
-            for (int i = t; i < P.nz; i += G::T) cp_async16(ps.fpb + i, src + i);
-            cp_async_commit();
-        }
         // ---- inverse transform of this step's field (scaled by 1/NZ)
         {
             // kind: 0 plain, 1 z-component (a c f0 - i b f1) il2, 2 i kz z-component,
@@ -375,18 +368,20 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
             pv.st_fence();
         }
         const int f = fupd;  // field this group updates now (-1/-2: none)
-        const cplx* __restrict__ fin = u_in + (f < 0 ? 0 : f) * P.nz;
+        const int fs = f < 0 ? 0 : f;
+        const cplx* __restrict__ fin = u_in + fs * P.nz;
         const cplx* __restrict__ lin0 = u_in + (f == 3 ? 2 : 0) * P.nz;
         const cplx* __restrict__ zin = u_in + P.nz;
-        const cplx* fpp = Fp ? ps.fpb : nullptr;
-        cplx* __restrict__ outp = u_out + (f < 0 ? 0 : f) * P.nz;
-        cplx* __restrict__ fop = Fo ? Fo + (f < 0 ? 0 : f) * P.nz : nullptr;
+        const cplx* __restrict__ fpp = Fp ? Fp + fs * P.nz : nullptr;
+        cplx* __restrict__ outp = u_out + fs * P.nz;
+        cplx* __restrict__ fop = Fo ? Fo + fs * P.nz : nullptr;
         const double* ekzt = (f < 2) ? TB.ekz_u : TB.ekz_b;
         const double em = (f < 2) ? em_u : em_b;
-        if (Fp) {
-            cp_async_wait_all();
-            __syncwarp(gmask);
-        }
+        // linear terms (MHD_BQlin.cpp:162,178,201): F = fu * S + ilapF^fu (x + i cl c l0 + rl l0 + i co c l1)
+        const bool fu = (f == 0);
+        const double cl = (f == 3) ? -P.q : ((f == 1) ? (P.q - Om2) : 0.0);  // times i kz
+        const double rl = fu ? __dmul_rn(__dmul_rn(2.0, ab), P.q) : 0.0;      // 2 kx ky q u (F_u)
+        const double co = fu ? Om2 : 0.0;                                      // 2 Omega i kz zeta (F_u)
 #pragma unroll
         for (int c4 = 0; c4 < Pn / 4; ++c4) {
             cplx sv[4];
@@ -399,9 +394,9 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
                 const int s = stored_index<G>(t + G::T * (4 * c4 + i));
                 const int sl = s < 0 ? 0 : s;
                 uin[i] = ldc(fin + sl);
-                fpv[i] = fpp ? fpp[sl] : mk(0.0, 0.0);
+                fpv[i] = fpp ? ldc(fpp + sl) : mk(0.0, 0.0);
                 l0[i] = ldc(lin0 + sl);
-                l1[i] = f == 0 ? ldc(zin + sl) : mk(0.0, 0.0);
+                l1[i] = ldc(zin + sl);
             }
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
@@ -411,23 +406,13 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
                 if (s < 0) continue;
                 const double c = kzval(kz_int<G>(k), P.kzL);
                 const double kz2 = kz2val(c);
-                cplx F;
-                if (f == 2) {
-                    F = x[k2];                                      // F_b (MHD_BQlin.cpp:182-185)
-                } else if (f == 3) {
-                    F = csub(x[k2], imul(l0[i], P.q * c));          // F_eta (:201)
-                } else if (f == 1) {
-                    F = cadd(x[k2], imul(l0[i], (P.q - Om2) * c));  // F_zeta (:178)
-                } else {
-                    // F_u (:162): ilapF = 1/(-kx^2 + lap2) with the kx=ky=kz=0 fix (:505-507)
-                    const bool z0 = (kyi == 0 && s == 0);
-                    const double lapF = __dadd_rn(-__dmul_rn(a, a), lap2val(ky, kz2, z0));
-                    const double ilapF = (z0 && kxi == 0) ? 1.0 : __drcp_rn(lapF);
-                    const cplx lin = cadd(cadd(cscale(l0[i], __dmul_rn(__dmul_rn(2.0, ab), P.q)),
-                                               imul(l1[i], Om2 * c)),
-                                          x[k2]);
-                    F = cadd(sv[i], cscale(lin, ilapF));
-                }
+                // ilapF = 1/(-kx^2 + lap2) with the kx=ky=kz=0 fix (MHD_BQlin.cpp:505-507)
+                const bool z0 = (kyi == 0 && s == 0);
+                const double lapF = __dadd_rn(-__dmul_rn(a, a), lap2val(ky, kz2, z0));
+                const double ilapF = fu ? ((z0 && kxi == 0) ? 1.0 : __drcp_rn(lapF)) : 1.0;
+                const cplx lin = cadd(cadd(x[k2], imul(l0[i], cl * c)), cadd(cscale(l0[i], rl), imul(l1[i], co * c)));
+                cplx F = cscale(lin, ilapF);
+                if (fu) F = cadd(sv[i], F);
                 if (A.rhs_only) {
                     stc(outp + s, F);
                     if (A.linop_out)
@@ -443,7 +428,6 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
                     nv = cscale(acc, e);
                 } else {
                     const double L = linop_f<MODEL_BQLIN>(P, lap_end<MODEL_BQLIN>(P, kxe, ky, kz2), f);
-                    const bool z0 = (kyi == 0 && s == 0);
                     const double lo = cn.old_init ? lap_init<MODEL_BQLIN>(P, kxo, lap2val(ky, kz2, z0))
                                                   : lap_end<MODEL_BQLIN>(P, kxo, ky, kz2);
                     nv = rk_update<INTEG_CN>(S, L, linop_f<MODEL_BQLIN>(P, lo, f), F, fpv[i], uin[i],

@@ -42,7 +42,7 @@ struct DevClock {
     int since;         // steps since the last diagnostic record
     int status;        // error bits (QLGPU_STATUS_*)
     unsigned cnt_top;
-    unsigned pad;
+    int mfr_valid;     // mean-field profiles cache holds the current mean field
     unsigned cnt_group[64];
 };
 
@@ -81,6 +81,8 @@ struct StageArgs {
     int rhs_only;           // Model::rhs: write F (and linop) only, no update
     double* linop_out;      // rhs_only: [nxy][4][nz]
     unsigned long long* trace;  // optional %globaltimer trace (null: off), see qlgpu_kernel.cuh
+    double* mfr_cache;      // [NMFR][NZ] real-space mean-field profiles written by the top CTA
+    const double* ekz_tab;  // [2][nz] exp(linC nu kz2), exp(linC eta kz2) for this stage (null: compute)
     StageConst sc;
 };
 

@@ -121,6 +121,19 @@ class QLSolver:
                     self.h)
         return F, Fm, Lop
 
+    def launch_info(self) -> dict:
+        a = (ctypes.c_int * 8)()
+        _capi.check(self.L.qlgpu_launch_info(self.h, a), self.h)
+        keys = ["grid", "block", "smem", "ctas_per_sm", "tmem_cols", "threads_per_transform", "modes", "warps"]
+        return dict(zip(keys, list(a)))
+
+    def kernel_attrs(self) -> dict:
+        a = (ctypes.c_int * 8)()
+        _capi.check(self.L.qlgpu_kernel_attrs(self.h, a), self.h)
+        keys = ["regs", "static_smem", "local_bytes", "max_threads", "ctas_per_sm_no_dyn_smem",
+                "ctas_per_sm", "max_dyn_smem", "carveout"]
+        return dict(zip(keys, list(a)))
+
     def status(self) -> int:
         s = ctypes.c_int()
         _capi.check(self.L.qlgpu_status(self.h, ctypes.byref(s)), self.h)
