@@ -15,6 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libqlgpu.so")
+MAIN = os.path.join(OUT_DIR, "ql_main")
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",
@@ -29,7 +30,8 @@ def sources():
 
 
 def deps():
-    return (glob.glob(os.path.join(CSRC, "*")) + [os.path.join(ROOT, "include", "qlgpu.h")])
+    return (glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(CSRC, "examples", "*")) +
+            glob.glob(os.path.join(ROOT, "include", "*")))
 
 
 def stale() -> bool:
@@ -49,7 +51,20 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
+    build_main(verbose)
     return LIB
+
+
+def build_main(verbose: bool = False) -> str:
+    """The C++ driver (csrc/examples/ql_main.cpp) linked against libqlgpu.so."""
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    src = os.path.join(CSRC, "examples", "ql_main.cpp")
+    cmd = [cxx, "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"), src, "-o", MAIN,
+           "-L" + OUT_DIR, "-lqlgpu", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return MAIN
 
 
 if __name__ == "__main__":

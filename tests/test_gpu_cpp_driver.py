@@ -1,0 +1,70 @@
+"""The C++ drop-in path: include/qlgpu.hpp (Model / Integrator / solution
+mirror) driven by csrc/examples/ql_main.cpp, which reads the reference's
+.DSSinput keys, checked against the oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from gpu_util import rel, require_gpu
+from oracle import oracle as O
+from ql_dns_b200.build import MAIN, build
+from ql_dns_b200.initial import initial_state
+from ql_dns_b200.params import config0
+
+pytestmark = pytest.mark.gpu
+
+
+def write_input(path, p, integ, tv_every):
+    name = "MHD_BQlin" if p.model == 0 else "MHD_FullQlin"
+    txt = f"""equations_to_use_ = {name}
+nx_ = {p.nx}
+ny_ = {p.ny}
+nz_ = {p.NZ}
+lx_ = {p.L[0]!r}
+ly_ = {p.L[1]!r}
+lz_ = {p.L[2]!r}
+dt_ = {p.dt!r}
+tv_save_ = {p.dt * tv_every!r}
+nu_ = {p.nu!r}
+eta_ = {p.eta!r}
+viscosity_order_ = {p.viscosity_order}
+q_ = {p.q!r}
+omega_ = {p.omega!r}
+B0z_ = {p.B0z!r}
+Remap? = {p.remap}
+QuasiLinear? = {p.quasilinear}
+integrator_ = {integ}
+"""
+    open(path, "w").write(txt)
+
+
+@pytest.mark.parametrize("integ", [0, 1])
+def test_cpp_driver_matches_oracle(tmp_path, integ):
+    require_gpu()
+    build()
+    p = config0(integrator=integ)
+    lin, mf, kx0 = initial_state(p, 9, sigma=0.1)
+    inp = tmp_path / "case.DSSinput"
+    write_input(inp, p, integ, 1)
+    st = tmp_path / "state.bin"
+    with open(st, "wb") as f:
+        np.array([0.0]).tofile(f)
+        lin.tofile(f)
+        mf.tofile(f)
+        kx0.tofile(f)
+    out, dg = tmp_path / "out.bin", tmp_path / "diag.bin"
+    r = subprocess.run([MAIN, str(inp), str(st), "100", str(out), str(dg)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    raw = np.fromfile(out, dtype=np.float64)
+    n_lin, n_mf = lin.size * 2, mf.size * 2
+    t = raw[0]
+    lo = raw[1:1 + n_lin].view(np.complex128).reshape(lin.shape)
+    mo = raw[1 + n_lin:1 + n_lin + n_mf].view(np.complex128).reshape(mf.shape)
+    ko = raw[1 + n_lin + n_mf:]
+    d = np.fromfile(dg, dtype=np.float64).reshape(-1, 15)
+    t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, 100, diag_every=1)
+    assert t == t2 and np.array_equal(ko, ko2)
+    assert rel(lo, lo2) < 1e-10 and rel(mo, mo2) < 1e-10
+    assert d.shape == d2.shape and rel(d[:, 1:13], d2[:, 1:13]) < 1e-10
