@@ -44,13 +44,15 @@ const void* stage_ptr() {
 template <int NZ, int MODEL, bool TM>
 size_t stage_smem(int warps) {
     using G = Geom<NZ>;
-    using Priv = typename std::conditional<TM, PrivTmem<G, PB_COUNT>, PrivSmem<G, PB_COUNT>>::type;
+    constexpr int NB = MODEL == MODEL_BQLIN ? (int)PB_COUNT : (int)PF_COUNT;
+    using Priv = typename std::conditional<TM, PrivTmem<G, NB>, PrivSmem<G, NB>>::type;
     return Smem<G, MODEL, Priv>::bytes(warps);
 }
 template <int NZ, int MODEL, bool TM>
 int stage_tmem(int warps) {
     using G = Geom<NZ>;
-    using Priv = typename std::conditional<TM, PrivTmem<G, PB_COUNT>, PrivSmem<G, PB_COUNT>>::type;
+    constexpr int NB = MODEL == MODEL_BQLIN ? (int)PB_COUNT : (int)PF_COUNT;
+    using Priv = typename std::conditional<TM, PrivTmem<G, NB>, PrivSmem<G, NB>>::type;
     return Smem<G, MODEL, Priv>::tmem_cols(warps);
 }
 template <int NZ>
@@ -91,6 +93,10 @@ bool pick_variant(int NZ, int model, int integ, bool tm, Variant* out) {
             *out = tm ? make_variant<NZV, MODEL_BQLIN, INTEG_EXP, true>() : make_variant<NZV, MODEL_BQLIN, INTEG_EXP, false>(); \
         else if (model == MODEL_BQLIN && integ == INTEG_CN)                                                      \
             *out = tm ? make_variant<NZV, MODEL_BQLIN, INTEG_CN, true>() : make_variant<NZV, MODEL_BQLIN, INTEG_CN, false>(); \
+        else if (model == MODEL_FULLQLIN && integ == INTEG_EXP)                                                  \
+            *out = tm ? make_variant<NZV, MODEL_FULLQLIN, INTEG_EXP, true>() : make_variant<NZV, MODEL_FULLQLIN, INTEG_EXP, false>(); \
+        else if (model == MODEL_FULLQLIN && integ == INTEG_CN)                                                   \
+            *out = tm ? make_variant<NZV, MODEL_FULLQLIN, INTEG_CN, true>() : make_variant<NZV, MODEL_FULLQLIN, INTEG_CN, false>(); \
         else                                                                                                     \
             return false;                                                                                        \
         return true;                                                                                             \
@@ -310,7 +316,7 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
     const bool use_tmem = !(ps && ps[0] == '1');
     if (!pick_variant(p.NZ, p.model, p.integrator, use_tmem, &var))
         return fail(nullptr, QLGPU_ERR_UNSUPPORTED,
-                    "unsupported (NZ, model): NZ must be a power of two in [16, 256]; model built: MHD_BQlin");
+                    "unsupported NZ: must be a power of two in [16, 256]");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(nullptr, QLGPU_ERR_NODEVICE, "no CUDA device");
     h = new (std::nothrow) qlgpu_handle();
@@ -345,6 +351,9 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
     d.nu = p.nu;
     d.eta = p.eta;
     d.etanu = p.model == QLGPU_MODEL_MHD_BQLIN ? p.eta / p.nu : p.eta;
+    d.cb = p.model == QLGPU_MODEL_MHD_BQLIN ? (p.eta / p.nu) * p.nu : p.eta;
+    // -|(-kx^2-ky^2)+kz2|^(order/2) is linear in kz2 only for order/2 == 1 (MHD_FullQlin.cpp:372)
+    d.factored = (p.model == QLGPU_MODEL_MHD_BQLIN || p.viscosity_order / 2 == 1) ? 1 : 0;
     d.B0z = p.B0z;
     d.visc_half = p.viscosity_order / 2;
     d.ql = p.quasilinear ? 1 : 0;
@@ -503,7 +512,7 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
                 const double c = kzi * kzL;
                 const double kz2 = -(c * c);
                 h->ekz_tab[(size_t)(st * 2) * h->nz + s] = std::exp(linC[st] * d.nu * kz2);
-                h->ekz_tab[(size_t)(st * 2 + 1) * h->nz + s] = std::exp(linC[st] * d.etanu * d.nu * kz2);
+                h->ekz_tab[(size_t)(st * 2 + 1) * h->nz + s] = std::exp(linC[st] * d.cb * kz2);
             }
         cudaMemcpyAsync(h->d_ekz, h->ekz_tab.data(), h->ekz_tab.size() * sizeof(double), cudaMemcpyHostToDevice,
                         h->stream);

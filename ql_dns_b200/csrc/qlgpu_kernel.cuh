@@ -233,8 +233,8 @@ struct Smem {
     static constexpr size_t o_spec = o_ekz + sizeof(double) * 2 * ((NZD + 1) & ~1);
     static constexpr size_t o_tot = o_spec + sizeof(double) * 2 * NEMF * (G::H + 1);
     static constexpr size_t o_work = o_tot + sizeof(double) * ((PL + 1) & ~1);
-    // per pair of groups: R_uz, R_bz (2 NZ cplx), i.e. NZ cplx per group
-    static constexpr size_t GS_BYTES = sizeof(cplx) * G::NZ;
+    // per pair of groups: BQlin R_uz, R_bz (2 NZ cplx); FullQlin the six components (6 NZ cplx)
+    static constexpr size_t GS_BYTES = sizeof(cplx) * G::NZ * (MODEL == MODEL_BQLIN ? 1 : 3);
     __host__ __device__ static size_t work_bytes(int warps) {
         const size_t xch = sizeof(cplx) * (size_t)warps * SW * G::XSIZE;
         const size_t red = sizeof(double) * ((size_t)warps * NEMF * G::NZ + (size_t)warps * 32 * 6);
@@ -256,7 +256,8 @@ struct Smem {
 template <int NZ, int MODEL, int INTEG, bool USE_TMEM>
 __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
     using G = Geom<NZ>;
-    using Priv = typename std::conditional<USE_TMEM, PrivTmem<G, PB_COUNT>, PrivSmem<G, PB_COUNT>>::type;
+    constexpr int NB = MODEL == MODEL_BQLIN ? (int)PB_COUNT : (int)PF_COUNT;
+    using Priv = typename std::conditional<USE_TMEM, PrivTmem<G, NB>, PrivSmem<G, NB>>::type;
     using SM = Smem<G, MODEL, Priv>;
     constexpr int SW = SM::SW;
     static_assert(SW % 2 == 0, "a warp holds whole pairs of groups");
@@ -298,7 +299,7 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
         tmem_fence_after_sync();
         pv.init(s_tmem, warp);
     } else {
-        pv.init(reinterpret_cast<cplx*>(work + SM::work_bytes(warps)) + (size_t)warp * PB_COUNT * G::P * 32, lane);
+        pv.init(reinterpret_cast<cplx*>(work + SM::work_bytes(warps)) + (size_t)warp * NB * G::P * 32, lane);
     }
     // pair layout: octet o = lane / T, pair pi = o / 2, role = o % 2 (0: velocity side, 1: magnetic side)
     const int role = slot & 1;
@@ -308,14 +309,17 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
     {
         unsigned char* gbase = work + SM::work_bytes(warps) + Priv::smem_bytes_per_warp() * (size_t)warps;
         cplx* k_all = reinterpret_cast<cplx*>(gbase);
-        cplx* kpair = k_all + (size_t)(warp * (SW / 2) + pi) * 2 * G::NZ;
+        cplx* kpair = k_all + (size_t)(warp * (SW / 2) + pi) * 2 * G::NZ * (MODEL == MODEL_BQLIN ? 1 : 3);
         ps.KU = kpair;
         ps.KB = kpair + G::NZ;
     }
     {   // zero the stress accumulators
         cplx z4[4] = {mk(0, 0), mk(0, 0), mk(0, 0), mk(0, 0)};
 #pragma unroll
-        for (int c4 = 0; c4 < G::P / 4; ++c4) pv.st4(PB_E, c4, z4);
+        for (int c4 = 0; c4 < G::P / 4; ++c4) {
+            pv.st4(0, c4, z4);  // PB_E / PF_E
+            if (MODEL == MODEL_FULLQLIN) pv.st4(PF_E2, c4, z4);
+        }
         pv.st_fence();
     }
 
@@ -335,7 +339,7 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
                 const int kzi = s <= G::H ? s : s - nzd;
                 const double kz2 = kz2val(kzval(kzi, P.kzL));
                 ekz[s] = exp(S.linC * P.nu * kz2);
-                ekz[SM::NZD + (SM::NZD & 1) + s] = exp(S.linC * P.etanu * P.nu * kz2);
+                ekz[SM::NZD + (SM::NZD & 1) + s] = exp(S.linC * P.cb * kz2);
             }
         }
     }
@@ -374,9 +378,12 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
         const int mode_raw = base + pi;
         const bool valid = mode_raw < P.nxy;
         const int mode = valid ? mode_raw : P.nxy - 1;
-        if (MODEL == MODEL_BQLIN)
+        if constexpr (MODEL == MODEL_BQLIN)
             bqlin_pair<G, INTEG, Priv>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps, pv, tw_s, mfr, tclock,
                                        cn);
+        else
+            fullqlin_pair<G, INTEG, Priv>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps.KU, pv, tw_s, mfr,
+                                          tclock, cn);
         if (last && valid && role == 0) {
             // ShearingBox_Remap(q t) after t += dt (main.cpp:122-123, MHD_BQlin.cpp:319-329)
             double kx0 = A.kx0[mode];
@@ -412,23 +419,26 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
     if (tr2) A.trace[22] = gtimer();
     double* red = reinterpret_cast<double*>(work);  // [warps][NEMF][NZ] then [blockDim][6]
 #pragma unroll
-    for (int c4 = 0; c4 < G::P / 4; ++c4) {
-        cplx e[4];
-        pv.ld4(PB_E, c4, e);
+    for (int eb = 0; eb < NEMF / 2; ++eb) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            // groups of a warp own the same z set (lane t of each group): sum them in lane order
-            double ex = e[i].x, ey = e[i].y;
-            double sx = 0.0, sy = 0.0;
+        for (int c4 = 0; c4 < G::P / 4; ++c4) {
+            cplx e[4];
+            pv.ld4(eb, c4, e);  // PB_E / PF_E, then PF_E2
 #pragma unroll
-            for (int g = 0; g < SW; ++g) {
-                sx += __shfl_sync(0xffffffffu, ex, g * G::T + t);
-                sy += __shfl_sync(0xffffffffu, ey, g * G::T + t);
-            }
-            if (slot == 0) {
-                const int z = zpos<G>(t, 4 * c4 + i);
-                red[(warp * NEMF + 0) * G::NZ + z] = sx;
-                red[(warp * NEMF + 1) * G::NZ + z] = sy;
+            for (int i = 0; i < 4; ++i) {
+                // groups of a warp own the same z set (lane t of each group): sum them in lane order
+                double ex = e[i].x, ey = e[i].y;
+                double sx = 0.0, sy = 0.0;
+#pragma unroll
+                for (int g = 0; g < SW; ++g) {
+                    sx += __shfl_sync(0xffffffffu, ex, g * G::T + t);
+                    sy += __shfl_sync(0xffffffffu, ey, g * G::T + t);
+                }
+                if (slot == 0) {
+                    const int z = zpos<G>(t, 4 * c4 + i);
+                    red[(warp * NEMF + 2 * eb + 0) * G::NZ + z] = sx;
+                    red[(warp * NEMF + 2 * eb + 1) * G::NZ + z] = sy;
+                }
             }
         }
     }

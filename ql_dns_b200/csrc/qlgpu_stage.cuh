@@ -211,7 +211,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
     double em_u = 1.0, em_b = 1.0;
     if (INTEG == INTEG_EXP && !A.rhs_only) {
         em_u = exp(S.linC * P.nu * hxy);
-        em_b = exp(S.linC * P.etanu * P.nu * hxy);
+        em_b = exp(S.linC * P.cb * hxy);
     }
     double kxo = 0.0;  // CN: kx of the previous stage end (or of t0 for the init form)
     if (INTEG == INTEG_CN) {
@@ -439,6 +439,271 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
         }
         __syncwarp();
     }
+}
+
+// ---------------------------------------------------------------------------
+// One coefficient update of field f at stored index s (the RK3 stage update of
+// RK3CN_Elin.cpp:102-104 / RK3CN.cpp:105-107), writing F (stages 1,2) and the
+// new value; rhs-only mode writes F and the linear operator instead.
+// ---------------------------------------------------------------------------
+template <int MODEL, int INTEG>
+__device__ __forceinline__ void update_coef(const StageArgs& A, const DevParams& P, const StageConst& S,
+                                            const StageTables& TB, const CnOld& cn, int mode, int f, int s, double c,
+                                            double kz2, double kxe, double kxo, double ky, int kyi, double em,
+                                            cplx F, cplx uin, const cplx* fpp, cplx* outp, cplx* fop) {
+    if (A.rhs_only) {
+        stc(outp + s, F);
+        if (A.linop_out)
+            A.linop_out[((size_t)mode * 4 + f) * P.nz + s] = linop_f<MODEL>(P, lap_end<MODEL>(P, kxe, ky, kz2), f);
+        return;
+    }
+    const cplx fpv = fpp ? ldc(fpp + s) : mk(0.0, 0.0);
+    cplx nv;
+    if (INTEG == INTEG_EXP) {
+        double e;
+        if (P.factored) e = em * ((f < 2) ? TB.ekz_u : TB.ekz_b)[s];
+        else e = exp(__dmul_rn(S.linC, linop_f<MODEL>(P, lap_end<MODEL>(P, kxe, ky, kz2), f)));
+        const cplx acc = fpp ? cadd(cadd(cscale(F, S.n1), cscale(fpv, S.n2)), uin) : cadd(cscale(F, S.n1), uin);
+        nv = cscale(acc, e);
+    } else {
+        const double L = linop_f<MODEL>(P, lap_end<MODEL>(P, kxe, ky, kz2), f);
+        const bool z0 = (kyi == 0 && s == 0);
+        const double lo = cn.old_init ? lap_init<MODEL>(P, kxo, lap2val(ky, kz2, z0)) : lap_end<MODEL>(P, kxo, ky, kz2);
+        nv = rk_update<INTEG_CN>(S, L, linop_f<MODEL>(P, lo, f), F, fpv, uin, fpp != nullptr);
+    }
+    if (fop) stc(fop + s, F);
+    stc(outp + s, nv);
+}
+
+// ---------------------------------------------------------------------------
+// MHD_FullQlin right-hand side (MHD_FullQlin.cpp:209-381) fused with the RK
+// update for one mode held by a pair of transform groups.  The six real-space
+// components U = (Ux, Uy, Uz), B = (Bx, By, Bz) are shared through shared
+// memory (SH[6][P][T]); d/dx and d/dy are the scalars i kx, i ky applied in z
+// space, so only 10 inverse transforms are needed (the reference does 22).
+// With aU = i(kx MUx + ky MUy), aB = i(kx MBx + ky MBy) (MHD_FullQlin.cpp:271-299):
+//   T1 = aU Ux + Uz dzMUx - aB Bx - Bz dzMBx    S1 = aU Bx + Uz dzMBx - aB Ux - Bz dzMUx
+//   T2 = aU Uy + Uz dzMUy - aB By - Bz dzMBy    S2 = aU By + Uz dzMBy - aB Uy - Bz dzMUy
+//   T3 = aU Uz - aB Bz                          S3 = aU Bz - aB Uz
+//   step  U (velocity side)                     B (magnetic side)
+//   0-2 inv Ux, Uy, Uz -> SH                    Bx, By, Bz -> SH
+//   3 inv dz Ux : stresses; fwd T1 -> S_1       dz Bx : stresses; fwd S1 -> F_b
+//   4 inv dz Uy : stresses; fwd T2 -> S_2       dz By : stresses; fwd S2 -> S_2
+//   5 fwd T3 -> F_u, F_zeta                     fwd S3 -> F_eta
+// Stresses (MHD_FullQlin.cpp:314-362): E.x Bx drive, E.y By drive (U side,
+// differentiated in z after the sum), E2.x Ux drive, E2.y Uy drive.
+// ---------------------------------------------------------------------------
+enum { PF_E = 0, PF_E2 = 1, PF_S1 = 2, PF_S2 = 3, PF_COUNT = 4 };
+
+template <class G, int INTEG, class Priv>
+__device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParams& P, const StageTables& TB, int mode,
+                                              bool valid, int role, int t, unsigned gmask, unsigned pmask, cplx* xch,
+                                              cplx* SH, const Priv& pv, const cplx* tw, const double* mfr,
+                                              double tclock, const CnOld& cn) {
+    constexpr int Pn = G::P;
+    const StageConst& S = A.sc;
+    const double fac = P.fac;
+    const double ky = __ldg(A.ky + mode);
+    const double kx0 = A.kx0[mode];
+    const int kyi = __ldg(A.kyi + mode), kxi = __ldg(A.kxi + mode);
+    const double ts = S.abs_time ? S.t_off : __dadd_rn(tclock, S.t_off);
+    const double a = kx_at(kx0, P.q, ts, ky);  // kx(t_s), MHD_FullQlin.cpp:727
+    const double b = ky;
+    const double ab = __dmul_rn(a, b);
+    const double Om2 = __dmul_rn(2.0, P.Omega);
+    const double mult = valid ? ((ky == 0.0) ? 1.0 : 2.0) : 0.0;
+    const cplx* __restrict__ u_in = A.lin_in + (size_t)mode * 4 * P.nz;
+    cplx* u_out = A.lin_out + (size_t)mode * 4 * P.nz;
+    const cplx* Fp = (A.Fprev && S.has_prev) ? A.Fprev + (size_t)mode * 4 * P.nz : nullptr;
+    cplx* Fo = A.Fout ? A.Fout + (size_t)mode * 4 * P.nz : nullptr;
+    const double *MBx = mfr, *dMBx = mfr + G::NZ, *MBy = mfr + 2 * G::NZ, *dMBy = mfr + 3 * G::NZ;
+    const double *MUx = mfr + 4 * G::NZ, *dMUx = mfr + 5 * G::NZ, *MUy = mfr + 6 * G::NZ, *dMUy = mfr + 7 * G::NZ;
+    const double* __restrict__ il2row = TB.ilap2 + (size_t)kyi * P.nz;
+    const int fbase = role ? 2 : 0;
+    const double kxe = __dadd_rn(a, __dmul_rn(__dmul_rn(P.q, S.dt_lin), ky));  // MHD_FullQlin.cpp:371
+    const double hxy = __dsub_rn(-__dmul_rn(kxe, kxe), __dmul_rn(ky, ky));
+    double em_u = 1.0, em_b = 1.0;
+    if (INTEG == INTEG_EXP && !A.rhs_only && P.factored) {
+        em_u = exp(S.linC * P.nu * hxy);
+        em_b = exp(S.linC * P.cb * hxy);
+    }
+    double kxo = 0.0;
+    if (INTEG == INTEG_CN) {
+        if (cn.old_init) kxo = kx_at(kx0, P.q, tclock, ky);
+        else kxo = __dadd_rn(kx_at(kx0, P.q, cn.t_old, ky), __dmul_rn(__dmul_rn(P.q, cn.dtlin_old), ky));
+    }
+#define SHV(f, j) SH[((f) * Pn + (j)) * G::T + t]
+    cplx x[Pn];
+    __syncwarp(pmask);  // the previous mode's readers of SH are done
+
+#pragma unroll 1
+    for (int step = 0; step < 6; ++step) {
+        // ---- inverse transform (steps 0-4): kind 0 plain, 3 y-component, 1 z-component,
+        //      5 i kz * plain, 6 i kz * y-component
+        if (step < 5) {
+            int kind;
+            switch (step) {
+                case 0: kind = 0; break;
+                case 1: kind = 3; break;
+                case 2: kind = 1; break;
+                case 3: kind = 5; break;
+                default: kind = 6; break;
+            }
+            const cplx* __restrict__ p0 = u_in + fbase * P.nz;
+            const cplx* __restrict__ p1 = p0 + P.nz;
+#pragma unroll
+            for (int k2 = 0; k2 < Pn; ++k2) {
+                const int k = t + G::T * k2;
+                const int s = stored_index<G>(k);
+                cplx v = mk(0.0, 0.0);
+                if (s >= 0) {
+                    const cplx g0 = ldc(p0 + s);
+                    const double c = kzval(kz_int<G>(k), P.kzL);
+                    if (kind == 0 || kind == 5) {
+                        v = g0;
+                    } else {
+                        const cplx g1 = ldc(p1 + s);
+                        const double il2 = __ldg(il2row + s);
+                        if (kind == 1) v = cscale(csub(cscale(g0, __dmul_rn(a, c)), imul(g1, b)), il2);
+                        else v = cscale(cadd(cscale(g0, ab), imul(g1, c)), il2);  // (MHD_FullQlin.cpp:220-221)
+                    }
+                    if (kind >= 5) v = imul(v, c);
+                }
+                x[k2] = cscale(v, fac);
+            }
+            inv_fft<G>(x, xch, tw, t, gmask);
+        }
+        __syncwarp();
+        if (step < 3) {
+#pragma unroll
+            for (int j = 0; j < Pn; ++j) SHV(role * 3 + step, j) = x[j];
+            __syncwarp();
+            continue;
+        }
+        // ---- stresses (steps 3, 4) and the forward-transform input
+        if (step < 5) {
+            const double sgn = role ? mult : -mult;  // minus the u part, plus the b part
+            const double semf = role ? 0.0 : mult;   // EMFs computed once, by the U lanes
+#pragma unroll
+            for (int c4 = 0; c4 < Pn / 4; ++c4) {
+                cplx e[4], e2[4];
+                pv.ld4(PF_E, c4, e);
+                pv.ld4(PF_E2, c4, e2);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int j = 4 * c4 + i;
+                    const cplx Ux = SHV(0, j), Uy = SHV(1, j), Uz = SHV(2, j);
+                    const cplx Bx = SHV(3, j), By = SHV(4, j), Bz = SHV(5, j);
+                    const cplx Fx = role ? Bx : Ux, Fy = role ? By : Uy, Fz = role ? Bz : Uz;
+                    // Re(a conj b)
+                    auto rc = [](cplx p, cplx q) { return p.x * q.x + p.y * q.y; };
+                    if (step == 3) {
+                        // EMF (MHD_FullQlin.cpp:322,330): Re(bz ux*) - Re(uz bx*), Re(bz uy*) - Re(uz by*)
+                        e[i].x += semf * (rc(Bz, Ux) - rc(Uz, Bx));
+                        e[i].y += semf * (rc(Bz, Uy) - rc(Uz, By));
+                        // x drive (:342-343): Re(Fx (i kx Fx)*) + Re(Fy (i ky Fx)*) + Re(Fz (dz Fx)*)
+                        e2[i].x += sgn * (rc(Fx, imul(Fx, a)) + rc(Fy, imul(Fx, b)) + rc(Fz, x[j]));
+                    } else {
+                        // y drive (:357-358): Re(Fx (i kx Fy)*) + Re(Fy (i ky Fy)*) + Re(Fz (dz Fy)*)
+                        e2[i].y += sgn * (rc(Fx, imul(Fy, a)) + rc(Fy, imul(Fy, b)) + rc(Fz, x[j]));
+                    }
+                }
+                __syncwarp();
+                pv.st4(PF_E, c4, e);
+                pv.st4(PF_E2, c4, e2);
+            }
+            pv.st_fence();
+        }
+        // forward input: U -> T(step-2), B -> S(step-2)
+#pragma unroll
+        for (int j = 0; j < Pn; ++j) {
+            const int z = zpos<G>(t, j);
+            const cplx Ux = SHV(0, j), Uy = SHV(1, j), Uz = SHV(2, j);
+            const cplx Bx = SHV(3, j), By = SHV(4, j), Bz = SHV(5, j);
+            const double aU = a * MUx[z] + b * MUy[z], aB = a * MBx[z] + b * MBy[z];  // times i
+            const cplx Fx = role ? Bx : Ux, Gx = role ? Ux : Bx;   // own / other x component
+            const cplx Fy = role ? By : Uy, Gy = role ? Uy : By;
+            const cplx Fz = role ? Bz : Uz, Gz = role ? Uz : Bz;
+            // T_n: aU U - aB B (+ z terms);  S_n: aU B - aB U (+ z terms)
+            const cplx own = role ? Bx : Ux;
+            (void)own;
+            cplx v;
+            if (step == 3) {
+                const double d1 = role ? dMBx[z] : dMUx[z], d2 = role ? dMUx[z] : dMBx[z];
+                v = csub(cadd(imul(Fx, aU), cscale(Uz, d1)), cadd(imul(Gx, aB), cscale(Bz, d2)));
+            } else if (step == 4) {
+                const double d1 = role ? dMBy[z] : dMUy[z], d2 = role ? dMUy[z] : dMBy[z];
+                v = csub(cadd(imul(Fy, aU), cscale(Uz, d1)), cadd(imul(Gy, aB), cscale(Bz, d2)));
+            } else {
+                v = csub(imul(Fz, aU), imul(Gz, aB));
+            }
+            x[j] = v;
+        }
+        fwd_fft<G>(x, xch, tw, t, gmask);
+        __syncwarp();
+        if (step == 3 || step == 4) {
+            // U keeps T1 (step 3) and T2 (step 4); B keeps S2 (step 4)
+#pragma unroll
+            for (int c4 = 0; c4 < Pn / 4; ++c4) pv.st4(step == 3 ? PF_S1 : PF_S2, c4, x + 4 * c4);
+            pv.st_fence();
+        }
+        // ---- updates: step 3 B -> F_b; step 5 U -> F_u, F_zeta; B -> F_eta
+#pragma unroll
+        for (int c4 = 0; c4 < Pn / 4; ++c4) {
+            cplx s1v[4], s2v[4];
+            __syncwarp();
+            if (step == 5) {
+                pv.ld4(PF_S1, c4, s1v);
+                pv.ld4(PF_S2, c4, s2v);
+            }
+            if (!valid || step == 4 || (step == 3 && role == 0)) continue;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int k2 = 4 * c4 + i;
+                const int k = t + G::T * k2;
+                const int s = stored_index<G>(k);
+                if (s < 0) continue;
+                const double c = kzval(kz_int<G>(k), P.kzL);
+                const double kz2 = kz2val(c);
+                const cplx u0 = ldc(u_in + s), ze = ldc(u_in + P.nz + s), b0 = ldc(u_in + 2 * P.nz + s),
+                           et = ldc(u_in + 3 * P.nz + s);
+                if (step == 3) {
+                    // F_b = B0z kz u - s1 (MHD_FullQlin.cpp:303)
+                    const cplx F = csub(imul(u0, P.B0z * c), x[k2]);
+                    update_coef<MODEL_FULLQLIN, INTEG>(A, P, S, TB, cn, mode, 2, s, c, kz2, kxe, kxo, ky, kyi, em_b,
+                                                       F, b0, Fp ? Fp + 2 * P.nz : nullptr, u_out + 2 * P.nz,
+                                                       Fo ? Fo + 2 * P.nz : nullptr);
+                } else if (role == 0) {
+                    // F_u, F_zeta (MHD_FullQlin.cpp:283-285) with t1 = S1, t2 = S2, t3 = x
+                    const cplx t1 = s1v[i], t2 = s2v[i], t3 = x[k2];
+                    const bool z0 = (kyi == 0 && s == 0);
+                    const double lapF = __dadd_rn(-__dmul_rn(a, a), lap2val(ky, kz2, z0));
+                    const double ilapF = (z0 && kxi == 0) ? 1.0 : __drcp_rn(lapF);
+                    // (-2 kx ky q) u + 2 Om kz zeta + kx^2 t1 + kx ky t2 + kx kz t3, kx = i a etc.
+                    cplx inner = cadd(cscale(u0, __dmul_rn(__dmul_rn(2.0, ab), P.q)), imul(ze, Om2 * c));
+                    inner = csub(inner, cadd(cadd(cscale(t1, a * a), cscale(t2, ab)), cscale(t3, a * c)));
+                    const cplx Fu = csub(cadd(cscale(inner, ilapF), imul(b0, P.B0z * c)), t1);
+                    // zeta: (q - 2 Om) kz u + B0z kz eta - (kz t2 - ky t3)
+                    const cplx Fz = csub(cadd(imul(u0, (P.q - Om2) * c), imul(et, P.B0z * c)),
+                                         csub(imul(t2, c), imul(t3, b)));
+                    update_coef<MODEL_FULLQLIN, INTEG>(A, P, S, TB, cn, mode, 0, s, c, kz2, kxe, kxo, ky, kyi, em_u,
+                                                       Fu, u0, Fp, u_out, Fo);
+                    update_coef<MODEL_FULLQLIN, INTEG>(A, P, S, TB, cn, mode, 1, s, c, kz2, kxe, kxo, ky, kyi, em_u,
+                                                       Fz, ze, Fp ? Fp + P.nz : nullptr, u_out + P.nz,
+                                                       Fo ? Fo + P.nz : nullptr);
+                } else {
+                    // F_eta = -q kz b + B0z kz zeta - (kz s2 - ky s3) (MHD_FullQlin.cpp:305)
+                    const cplx s2 = s2v[i], s3 = x[k2];
+                    const cplx Fe = csub(cadd(imul(b0, -P.q * c), imul(ze, P.B0z * c)), csub(imul(s2, c), imul(s3, b)));
+                    update_coef<MODEL_FULLQLIN, INTEG>(A, P, S, TB, cn, mode, 3, s, c, kz2, kxe, kxo, ky, kyi, em_b,
+                                                       Fe, et, Fp ? Fp + 3 * P.nz : nullptr, u_out + 3 * P.nz,
+                                                       Fo ? Fo + 3 * P.nz : nullptr);
+                }
+            }
+        }
+        __syncwarp();
+    }
+#undef SHV
 }
 
 }  // namespace qlgpu

@@ -15,6 +15,8 @@ struct DevParams {
     double q;       // shear
     double Omega;   // rotation: 2q/3 for MHD_BQlin (MHD_BQlin.cpp:19), input omega for FullQlin
     double nu, eta, etanu;  // etanu = eta/nu (MHD_BQlin.cpp:251)
+    double cb;              // L_b = cb * lap: (eta/nu) nu for MHD_BQlin, eta for MHD_FullQlin
+    int factored;           // the integrating factor exp(linC L) factors as exp(linC c h) exp(linC c kz2)
     double B0z;
     int visc_half;  // viscosity_order/2 (integer division, MHD_FullQlin.cpp:372)
     int ql;         // QuasiLinear?

@@ -38,10 +38,7 @@ def series_rel(dg, do):
     return max(errs)
 
 
-BQLIN_GOLDEN = [n for n in names() if not n.startswith("fullqlin")]
-
-
-@pytest.mark.parametrize("name", BQLIN_GOLDEN)
+@pytest.mark.parametrize("name", names())
 def test_golden_fixture(name):
     p, g = load(name)
     n = int(g["nsteps"])
@@ -55,11 +52,12 @@ def test_golden_fixture(name):
     assert series_rel(d, g["diag"]) < TOL
 
 
+@pytest.mark.parametrize("model", [0, 1])
 @pytest.mark.parametrize("integ", [0, 1])
-def test_rhs_matches_oracle(integ):
+def test_rhs_matches_oracle(model, integ):
     require_gpu()
-    p = config0(nx=8, ny=8, NZ=32, integrator=integ)
-    lin, mf, kx0 = initial_state(p, 21, sigma=0.5)
+    p = config0(nx=8, ny=8, NZ=32, integrator=integ, model=model, B0z=0.03 if model else 0.0, omega=0.8)
+    lin, mf, kx0 = initial_state(p, 21, sigma=0.5, mean_u=0.02)
     with QLSolver(p) as s:
         s.set_state(0.0, lin, mf, kx0)
         F, Fm, Lop = s.rhs(0.731, 0.0023, lin, mf)
@@ -69,10 +67,11 @@ def test_rhs_matches_oracle(integ):
     assert rel(Lop, L2) < 1e-15
 
 
+@pytest.mark.parametrize("model", [0, 1])
 @pytest.mark.parametrize("NZ", [16, 32, 64, 128, 256])
-def test_each_nz_one_step(NZ):
-    p = config0(nx=8, ny=6, NZ=NZ)
-    lin, mf, kx0 = initial_state(p, NZ, sigma=0.3)
+def test_each_nz_three_steps(NZ, model):
+    p = config0(nx=8, ny=6, NZ=NZ, model=model, B0z=0.02 if model else 0.0)
+    lin, mf, kx0 = initial_state(p, NZ, sigma=0.3, mean_u=0.02)
     _, lo, mo, ko, d = run_gpu(p, lin, mf, kx0, 3)
     _, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, 3, diag_every=1)
     assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL
@@ -136,3 +135,17 @@ def test_nonfinite_state_reports_status():
         s.set_state(0.0, lin, mf, kx0)
         s.step(1)
         assert s.status() == 0
+
+
+@pytest.mark.parametrize("integ", [0, 1])
+@pytest.mark.parametrize("order", [2, 4])
+def test_fullqlin_200_steps(integ, order):
+    # MHD_FullQlin with a vertical field, rotation, mean U and (order 4) hyper-dissipation
+    p = config0(model=1, integrator=integ, B0z=0.05, omega=1.0, viscosity_order=order,
+                nu=1e-4 if order == 4 else 1 / 2000, eta=2e-4 if order == 4 else 1 / 2000)
+    lin, mf, kx0 = initial_state(p, 3, sigma=0.05, mean_u=0.02)
+    t, lo, mo, ko, d = run_gpu(p, lin, mf, kx0, 200)
+    t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, 200, diag_every=1)
+    assert t == t2 and np.array_equal(ko, ko2)
+    assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL
+    assert series_rel(d, d2) < TOL
