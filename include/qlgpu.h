@@ -106,6 +106,27 @@ int qlgpu_diagnostics(qlgpu_t* h, double* out15);
 int qlgpu_rhs(qlgpu_t* h, double t, double dt_lin, const double* lin_in, const double* mf_in, double* lin_rhs,
               double* mf_rhs, double* linop);
 
+/* Model::rhs on caller-owned DEVICE buffers that allocates no device memory.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc while the step runs (a pre-sized device memory pool or arena, a
+ * host framework that owns every device buffer, latency-critical loops where
+ * an allocation or the synchronisation of cudaFree is not acceptable).
+ * Inputs lin_in[nxy][4][nz], mf_in[nmf][nz] and kx0[nxy] (may be NULL: the
+ * unsheared wavenumber table), outputs lin_rhs, mf_rhs and linop (nxy*4*nz
+ * doubles, may be NULL); all pointers are device pointers on the current
+ * device; the work is queued on `stream` (a cudaStream_t, NULL = legacy
+ * default stream) and the call returns without synchronising.
+ * Scratch: one fixed 4 MiB device array in the library, held by every GPU that
+ * loads the library until the process exits.  Limits: at most 8192 (kx,ky)
+ * modes and ny <= 256 (larger cases return QLGPU_ERR_ARG; use qlgpu_rhs).
+ * The first call on each device looks up the scratch address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the scratch: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller.  Errors are
+ * reported through qlgpu_last_error(NULL, ...). */
+int qlgpu_rhs_noalloc(const qlgpu_params* p, double t, double dt_lin, const void* lin_in, const void* mf_in,
+                      const void* kx0, void* lin_rhs, void* mf_rhs, void* linop, void* stream);
+
 /* Device status word (solution::Check_Solution, QL_DNS/solution.cpp:169-203):
  * bit 1 non-finite mean field, bit 2 |mean field| > 1e20, bit 4 diagnostic
  * records dropped.  Reading does not clear it; set_state clears it. */

@@ -20,7 +20,7 @@ ERRORS = {1: "QLGPU_ERR_ARG", 2: "QLGPU_ERR_UNSUPPORTED", 3: "QLGPU_ERR_CUDA", 4
 # Every symbol include/qlgpu.h declares.
 EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "qlgpu_get_state",
            "qlgpu_set_state_device", "qlgpu_get_state_device", "qlgpu_step", "qlgpu_step_timed", "qlgpu_diagnostics",
-           "qlgpu_rhs", "qlgpu_status", "qlgpu_time", "qlgpu_trace", "qlgpu_launch_info", "qlgpu_kernel_attrs",
+           "qlgpu_rhs", "qlgpu_rhs_noalloc", "qlgpu_status", "qlgpu_time", "qlgpu_trace", "qlgpu_launch_info", "qlgpu_kernel_attrs",
            "qlgpu_stream",
            "qlgpu_last_error",
            "qlgpu_version"]
@@ -70,6 +70,8 @@ def load(path: str = LIB_PATH):
     L.qlgpu_step_timed.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     L.qlgpu_diagnostics.argtypes = [vp, dp]
     L.qlgpu_rhs.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp, dp]
+    L.qlgpu_rhs_noalloc.argtypes = [ctypes.POINTER(qlgpu_params), ctypes.c_double, ctypes.c_double,
+                                    vp, vp, vp, vp, vp, vp, vp]
     L.qlgpu_status.argtypes = [vp, ip]
     L.qlgpu_time.argtypes = [vp, dp]
     L.qlgpu_trace.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]

@@ -779,3 +779,207 @@ int qlgpu_stream(qlgpu_t* h, void** stream) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// qlgpu_rhs_noalloc: Model::rhs on caller-owned device buffers with no device
+// allocation at all.
+//
+// Some callers cannot allocate device memory while they run this step: code
+// executing inside a pre-sized memory pool or arena that forbids cudaMalloc
+// after start-up, callers that own every device buffer themselves (a host
+// framework passing in pointers it manages), and latency-critical loops where
+// an allocation (and the implicit device synchronisation of cudaFree) is not
+// acceptable.  For them the scratch the stage kernel needs (wavenumber and
+// twiddle tables, per-CTA partial sums, the reduction counters) lives in one
+// file-scope device array of a fixed size, loaded with the library and held by
+// every GPU that loads it until the process exits.
+// ============================================================================
+#include <mutex>
+
+namespace {
+
+// Fixed scratch for qlgpu_rhs_noalloc (4 MiB per device).
+#define QLGPU_NOALLOC_SCRATCH_BYTES (4u << 20)
+#define QLGPU_NOALLOC_MAX_MODES 8192
+#define QLGPU_NOALLOC_MAX_KY 128
+#define QLGPU_NOALLOC_MAX_GRID 256
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[QLGPU_NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch, looked up once per device.  In host code
+// the symbol g_noalloc_scratch is only a host-side stand-in; handing it to a
+// kernel would read the wrong memory.
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[64] = {nullptr};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct NoallocLayout {
+    size_t tw, ky, kxi, kyi, kx0, il2, partials, gpartials, clk, end;
+};
+
+NoallocLayout noalloc_layout(int NZ, int nxy, int nyh, int nz, int grid, int PL) {
+    NoallocLayout L;
+    size_t o = 0;
+    L.tw = o; o = align256(o + sizeof(cplx) * NZ);
+    L.ky = o; o = align256(o + sizeof(double) * nxy);
+    L.kxi = o; o = align256(o + sizeof(int) * nxy);
+    L.kyi = o; o = align256(o + sizeof(int) * nxy);
+    L.kx0 = o; o = align256(o + sizeof(double) * nxy);
+    L.il2 = o; o = align256(o + sizeof(double) * (size_t)nyh * nz);
+    L.partials = o; o = align256(o + sizeof(double) * (size_t)grid * PL);
+    L.gpartials = o; o = align256(o + sizeof(double) * (size_t)((grid + RED_GROUP - 1) / RED_GROUP) * PL);
+    L.clk = o; o = align256(o + sizeof(DevClock));
+    L.end = o;
+    return L;
+}
+
+// Fills the wavenumber tables (Kdata.cpp:24-46,100-119), the twiddles of the
+// transform layout and the default kx0, and zeroes the reduction counters.
+__global__ void noalloc_tables_kernel(unsigned char* base, NoallocLayout L, int NZ, int T, int nx, int ny, int nz,
+                                      double kxL, double kyL, double kzL, int fill_kx0) {
+    const int nxy = (nx - 1) * (ny / 2);
+    const int nyh = ny / 2, nxh = nx / 2;
+    cplx* tw = reinterpret_cast<cplx*>(base + L.tw);
+    double* ky = reinterpret_cast<double*>(base + L.ky);
+    int* kxi = reinterpret_cast<int*>(base + L.kxi);
+    int* kyi = reinterpret_cast<int*>(base + L.kyi);
+    double* kx0 = reinterpret_cast<double*>(base + L.kx0);
+    double* il2 = reinterpret_cast<double*>(base + L.il2);
+    DevClock* clk = reinterpret_cast<DevClock*>(base + L.clk);
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const int P = NZ / T;
+    for (int i = tid; i < NZ; i += nth) {
+        const int n2 = i / T, t = i % T;
+        const int m = (n2 * t) % NZ;
+        double sn, cs;
+        sincospi(2.0 * (double)m / (double)NZ, &sn, &cs);
+        tw[i] = mk(cs, sn);
+    }
+    (void)P;
+    for (int i = tid; i < nxy; i += nth) {
+        // mode index j + (Ny/2) i with the kx Nyquist column dropped
+        const int col = i / nyh, j = i % nyh;
+        const int ix = col < nxh ? col : col + 1;  // skip the Nyquist index nx/2
+        const int kxint = ix < nxh ? ix : (-2 * nxh + ix);
+        ky[i] = j * kyL;
+        kxi[i] = kxint;
+        kyi[i] = j;
+        if (fill_kx0) kx0[i] = kxint * kxL;
+    }
+    const int nzl = (nz - 1) / 2;
+    for (int i = tid; i < nyh * nz; i += nth) {
+        const int j = i / nz, s = i % nz;
+        const double kyr = j * kyL;
+        const int kzi = s <= nzl ? s : (-2 * nzl + s - 1);
+        const double c = kzi * kzL;
+        const double kz2 = -(c * c);
+        double v = 1 / (-kyr * kyr + kz2);
+        if (kyr == 0 && s == 0) v = 1;
+        il2[i] = v;
+    }
+    unsigned* w = reinterpret_cast<unsigned*>(clk);
+    for (int i = tid; i < (int)(sizeof(DevClock) / sizeof(unsigned)); i += nth) w[i] = 0u;
+}
+
+}  // namespace
+
+extern "C" int qlgpu_rhs_noalloc(const qlgpu_params* pp, double t, double dt_lin, const void* lin_in,
+                                 const void* mf_in, const void* kx0, void* lin_rhs, void* mf_rhs, void* linop,
+                                 void* stream) {
+    if (!pp || !lin_in || !mf_in || !lin_rhs || !mf_rhs) return fail(nullptr, QLGPU_ERR_ARG, "null argument");
+    const qlgpu_params& p = *pp;
+    if (p.model != QLGPU_MODEL_MHD_BQLIN && p.model != QLGPU_MODEL_MHD_FULLQLIN)
+        return fail(nullptr, QLGPU_ERR_ARG, "unknown model");
+    if (p.nx < 2 || (p.nx % 2) || p.ny < 2 || (p.ny % 2))
+        return fail(nullptr, QLGPU_ERR_ARG, "nx and ny must be even and >= 2");
+    if (!(p.L[0] > 0 && p.L[1] > 0 && p.L[2] > 0)) return fail(nullptr, QLGPU_ERR_ARG, "box lengths must be > 0");
+    if (p.model == QLGPU_MODEL_MHD_BQLIN && p.nu == 0.0)
+        return fail(nullptr, QLGPU_ERR_ARG, "MHD_BQlin divides by nu (MHD_BQlin.cpp:251); nu must be nonzero");
+    Variant var;
+    if (!pick_variant(p.NZ, p.model, QLGPU_INTEG_RK3CN_ELIN, true, &var))
+        return fail(nullptr, QLGPU_ERR_UNSUPPORTED, "unsupported NZ: must be a power of two in [16, 256]");
+    const int nz = 1 + 2 * int(p.NZ / 3.0), nxy = (p.nx - 1) * (p.ny / 2), nyh = p.ny / 2;
+    const int nmf = p.model == QLGPU_MODEL_MHD_BQLIN ? 2 : 4;
+    if (nxy > QLGPU_NOALLOC_MAX_MODES || nyh > QLGPU_NOALLOC_MAX_KY)
+        return fail(nullptr, QLGPU_ERR_ARG,
+                    "too large for the fixed no-allocation scratch: at most 8192 (kx,ky) modes and ny <= 256 "
+                    "(use qlgpu_create / qlgpu_rhs for larger grids)");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return fail(nullptr, QLGPU_ERR_NODEVICE, "no CUDA device");
+    void* base = nullptr;
+    {
+        // One-time set-up on this device: the device address of the scratch array.
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            void* ptr = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess || !ptr)
+                return fail(nullptr, QLGPU_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_noalloc_ptr[dev] = ptr;
+        }
+        base = g_noalloc_ptr[dev];
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return fail(nullptr, QLGPU_ERR_CUDA, "device properties");
+    // Launch geometry: as in qlgpu_create, at most one CTA per SM and one mode per pair of groups.
+    int warps = 8;
+    while (warps > 1 && var.smem(warps) > (size_t)prop.sharedMemPerBlockOptin) warps >>= 1;
+    const size_t smem = var.smem(warps);
+    if (cudaFuncSetAttribute(var.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return fail(nullptr, QLGPU_ERR_CUDA, "shared memory request too large");
+    const int modes_per_cta = warps * (32 / var.T) / 2;
+    int grid = (nxy + modes_per_cta - 1) / modes_per_cta;
+    if (grid > prop.multiProcessorCount) grid = prop.multiProcessorCount;
+    if (grid > QLGPU_NOALLOC_MAX_GRID) grid = QLGPU_NOALLOC_MAX_GRID;
+    const NoallocLayout L = noalloc_layout(p.NZ, nxy, nyh, nz, grid, var.PL);
+    if (L.end > QLGPU_NOALLOC_SCRATCH_BYTES)
+        return fail(nullptr, QLGPU_ERR_ARG, "case exceeds the 4 MiB no-allocation scratch");
+    // Run constants (as qlgpu_create)
+    DevParams d;
+    std::memset(&d, 0, sizeof(d));
+    d.nxy = nxy; d.nz = nz; d.NZ = p.NZ; d.nmf = nmf;
+    d.q = p.q;
+    d.Omega = p.model == QLGPU_MODEL_MHD_BQLIN ? 2.0 / 3.0 * p.q : p.omega;
+    d.nu = p.nu; d.eta = p.eta;
+    d.etanu = p.model == QLGPU_MODEL_MHD_BQLIN ? p.eta / p.nu : p.eta;
+    d.cb = p.model == QLGPU_MODEL_MHD_BQLIN ? (p.eta / p.nu) * p.nu : p.eta;
+    d.factored = (p.model == QLGPU_MODEL_MHD_BQLIN || p.viscosity_order / 2 == 1) ? 1 : 0;
+    d.B0z = p.B0z;
+    d.visc_half = p.viscosity_order / 2;
+    d.ql = p.quasilinear ? 1 : 0;
+    d.remap = p.remap ? 1 : 0;
+    d.kzL = 2 * kPI / p.L[2];
+    d.fac = 1.0 / p.NZ;
+    const int Nx = p.nx, Ny = (p.ny / 2) * 2;
+    d.rs_fac = 1.0 / (Ny * Nx) / (Ny * Nx);
+    d.dt = p.dt;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    unsigned char* b = static_cast<unsigned char*>(base);
+    noalloc_tables_kernel<<<32, 256, 0, st>>>(b, L, p.NZ, var.T, p.nx, p.ny, nz, 2 * kPI / p.L[0], 2 * kPI / p.L[1],
+                                             d.kzL, kx0 ? 0 : 1);
+    StageArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.lin_in = static_cast<const cplx*>(lin_in);
+    A.lin_out = static_cast<cplx*>(lin_rhs);
+    A.mf = const_cast<cplx*>(static_cast<const cplx*>(mf_in));  // read only in rhs mode
+    A.Fmf_out = static_cast<cplx*>(mf_rhs);
+    A.kx0 = kx0 ? const_cast<double*>(static_cast<const double*>(kx0)) : reinterpret_cast<double*>(b + L.kx0);
+    A.ky = reinterpret_cast<const double*>(b + L.ky);
+    A.kxi = reinterpret_cast<const int*>(b + L.kxi);
+    A.kyi = reinterpret_cast<const int*>(b + L.kyi);
+    A.tw = reinterpret_cast<const cplx*>(b + L.tw);
+    A.ilap2 = reinterpret_cast<const double*>(b + L.il2);
+    A.partials = reinterpret_cast<double*>(b + L.partials);
+    A.gpartials = reinterpret_cast<double*>(b + L.gpartials);
+    A.clk = reinterpret_cast<DevClock*>(b + L.clk);
+    A.rhs_only = 1;
+    A.linop_out = static_cast<double*>(linop);
+    A.sc.t_off = t;
+    A.sc.abs_time = 1;
+    A.sc.dt_lin = dt_lin;
+    var.launch(A, d, grid, 32 * warps, smem, st);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(nullptr, QLGPU_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return QLGPU_OK;
+}
