@@ -160,6 +160,74 @@ int qlgpu_last_error(const qlgpu_t* h, char* buf, int buflen);
 /* Library version string. */
 const char* qlgpu_version(void);
 
+/* ------------------------------------------------------------------------
+ * Batched ensemble.  No counterpart in the reference, which runs one case per
+ * MPI job (QL_DNS/main.cpp:23-180): here many independent cases, each with
+ * its own qlgpu_params (mode grid, NZ, nu, eta, q, dt, ...), step together in
+ * ONE persistent cooperative kernel launch per call.  All cases share the
+ * model and the integrator.  Per case the step is the same fused RK3 step as
+ * qlgpu_step (the same stage code); only the order of the floating-point sums
+ * over CTAs depends on how many CTAs a case gets.  Every wait inside the
+ * kernel is bounded (a status bit, never a hang).
+ * ------------------------------------------------------------------------ */
+typedef struct qlgpu_batch qlgpu_batch_t;
+
+#define QLGPU_STATUS_BATCH_TIMEOUT 8 /* a CTA gave up waiting for the others of its case */
+
+/* Creates the batch (device memory, wavenumber tables, an initial CTA
+ * mapping from the cost model).  All cases zero; t = 0. */
+int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_batch_t** out);
+int qlgpu_batch_destroy(qlgpu_batch_t* b);
+int qlgpu_batch_dims(const qlgpu_batch_t* b, int c, int* nxy, int* nz, int* nmf);
+
+/* State of case c, as qlgpu_set_state / qlgpu_get_state (host buffers; kx0 may be NULL). */
+int qlgpu_batch_set_state(qlgpu_batch_t* b, int c, double t, const double* lin, const double* mf, const double* kx0);
+int qlgpu_batch_get_state(qlgpu_batch_t* b, int c, double* t, double* lin, double* mf, double* kx0);
+
+/* Initial diagnostic record of case c (15 doubles, as qlgpu_diagnostics). */
+int qlgpu_batch_diagnostics(qlgpu_batch_t* b, int c, double* out15);
+
+/* nsteps steps of every case in one launch (replayed from a CUDA graph).
+ * diag_every > 0: case c writes a record every diag_every steps to
+ * diag_out + c*max_diag*15 and its count to ndiag[c]. */
+int qlgpu_batch_step(qlgpu_batch_t* b, int nsteps, int diag_every, double* diag_out, int max_diag, int* ndiag);
+
+/* As qlgpu_batch_step without diagnostics; *ms = device time of the launch
+ * (CUDA events on the batch stream). */
+int qlgpu_batch_step_timed(qlgpu_batch_t* b, int nsteps, float* ms);
+
+/* Autotuner: times probe_steps-step launches of candidate mappings (CTA
+ * width, CTAs per case, cases per CTA) on a copy of the state, fits the cost
+ * model to the per-case times and keeps the fastest mapping.  The state is
+ * unchanged.  *best_ms (may be NULL) = time of the kept mapping's probe. */
+int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms);
+
+/* Current mapping: info4 = {warps per CTA, CTAs launched, CTAs per SM,
+ * dynamic shared bytes}; ncta[c] = CTAs that step case c (may be NULL). */
+int qlgpu_batch_mapping(const qlgpu_batch_t* b, int* info4, int* ncta);
+
+/* Fixed mapping: ncta[c] CTAs for case c at `warps` warps per CTA (4 or 8);
+ * cases are packed onto the launch's CTAs by the cost model. */
+int qlgpu_batch_set_mapping(qlgpu_batch_t* b, int warps, const int* ncta);
+
+/* Per-case device status words (bits as qlgpu_status) and the launch status
+ * of the most recent step (QLGPU_STATUS_BATCH_TIMEOUT). */
+int qlgpu_batch_status(qlgpu_batch_t* b, int* case_status, int* launch_status);
+
+/* Bound on one in-kernel wait (default 2 s). */
+int qlgpu_batch_set_wait(qlgpu_batch_t* b, double seconds);
+
+/* Failure-detection test aid: removes the last work item of case c (a case
+ * with two or more CTAs) from the current mapping, so that the case's other
+ * CTAs wait for a stage that never completes.  The next step call must return
+ * QLGPU_ERR_STATUS with QLGPU_STATUS_BATCH_TIMEOUT after the wait bound; the
+ * batch stays usable after qlgpu_batch_set_mapping / qlgpu_batch_tune and
+ * qlgpu_batch_set_state. */
+int qlgpu_batch_debug_drop_item(qlgpu_batch_t* b, int c);
+
+int qlgpu_batch_stream(qlgpu_batch_t* b, void** stream);
+int qlgpu_batch_last_error(const qlgpu_batch_t* b, char* buf, int buflen);
+
 #ifdef __cplusplus
 }
 #endif

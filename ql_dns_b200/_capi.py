@@ -23,7 +23,12 @@ EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "ql
            "qlgpu_rhs", "qlgpu_rhs_noalloc", "qlgpu_status", "qlgpu_time", "qlgpu_trace", "qlgpu_launch_info", "qlgpu_kernel_attrs",
            "qlgpu_stream",
            "qlgpu_last_error",
-           "qlgpu_version"]
+           "qlgpu_version",
+           "qlgpu_batch_create", "qlgpu_batch_destroy", "qlgpu_batch_dims", "qlgpu_batch_set_state",
+           "qlgpu_batch_get_state", "qlgpu_batch_diagnostics", "qlgpu_batch_step", "qlgpu_batch_step_timed",
+           "qlgpu_batch_tune", "qlgpu_batch_mapping", "qlgpu_batch_set_mapping", "qlgpu_batch_status",
+           "qlgpu_batch_set_wait", "qlgpu_batch_debug_drop_item", "qlgpu_batch_stream",
+           "qlgpu_batch_last_error"]
 
 
 class qlgpu_params(ctypes.Structure):
@@ -80,6 +85,22 @@ def load(path: str = LIB_PATH):
     L.qlgpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.qlgpu_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.qlgpu_version.restype = ctypes.c_char_p
+    L.qlgpu_batch_create.argtypes = [ctypes.POINTER(qlgpu_params), ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.qlgpu_batch_destroy.argtypes = [vp]
+    L.qlgpu_batch_dims.argtypes = [vp, ctypes.c_int, ip, ip, ip]
+    L.qlgpu_batch_set_state.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, dp, dp]
+    L.qlgpu_batch_get_state.argtypes = [vp, ctypes.c_int, dp, dp, dp, dp]
+    L.qlgpu_batch_diagnostics.argtypes = [vp, ctypes.c_int, dp]
+    L.qlgpu_batch_step.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ip]
+    L.qlgpu_batch_step_timed.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.qlgpu_batch_tune.argtypes = [vp, ctypes.c_int, dp]
+    L.qlgpu_batch_mapping.argtypes = [vp, ip, ip]
+    L.qlgpu_batch_set_mapping.argtypes = [vp, ctypes.c_int, ip]
+    L.qlgpu_batch_status.argtypes = [vp, ip, ip]
+    L.qlgpu_batch_set_wait.argtypes = [vp, ctypes.c_double]
+    L.qlgpu_batch_debug_drop_item.argtypes = [vp, ctypes.c_int]
+    L.qlgpu_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.qlgpu_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     for name in EXPORTS:
         if name not in ("qlgpu_version",):
             getattr(L, name).restype = ctypes.c_int
@@ -101,4 +122,13 @@ def check(rc: int, h=None):
         L = load()
         buf = ctypes.create_string_buffer(512)
         L.qlgpu_last_error(h, buf, 512)
+        raise QLGPUError(rc, buf.value.decode(errors="replace"))
+
+
+def check_batch(rc: int, b=None):
+    """As check() for the qlgpu_batch_* entry points (their own error message)."""
+    if rc != QLGPU_OK:
+        L = load()
+        buf = ctypes.create_string_buffer(512)
+        L.qlgpu_batch_last_error(b, buf, 512)
         raise QLGPUError(rc, buf.value.decode(errors="replace"))

@@ -1,0 +1,163 @@
+"""Batched ensemble of quasi-linear cases on one GPU (qlgpu_batch_* of include/qlgpu.h).
+
+Many independent cases (their own mode grid, NZ, nu, eta, mean field) step
+together in one persistent cooperative kernel launch per call.  The reference
+runs one case per MPI job (QL_DNS/main.cpp); per case the arithmetic is the
+same fused RK3 step as ``QLSolver``.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _capi
+from .params import QLParams
+
+
+class QLBatch:
+    """A batch of cases resident on one GPU."""
+
+    def __init__(self, cases: list[QLParams], device: int = -1):
+        self.cases = list(cases)
+        self.L = _capi.load()
+        arr = (_capi.qlgpu_params * len(cases))(*[_capi.to_c(p) for p in cases])
+        b = ctypes.c_void_p()
+        _capi.check_batch(self.L.qlgpu_batch_create(arr, len(cases), device, ctypes.byref(b)), None)
+        self.b = b
+        self.dims = []
+        for c in range(len(cases)):
+            nxy, nz, nmf = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            self.L.qlgpu_batch_dims(b, c, ctypes.byref(nxy), ctypes.byref(nz), ctypes.byref(nmf))
+            self.dims.append((nxy.value, nz.value, nmf.value))
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.L.qlgpu_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __len__(self):
+        return len(self.cases)
+
+    # -- state ---------------------------------------------------------------
+    def set_state(self, c: int, t: float, lin: np.ndarray, mf: np.ndarray, kx0: np.ndarray | None = None):
+        nxy, nz, nmf = self.dims[c]
+        lin = np.ascontiguousarray(lin, dtype=np.complex128)
+        mf = np.ascontiguousarray(mf, dtype=np.complex128)
+        assert lin.shape == (nxy, 4, nz) and mf.shape == (nmf, nz)
+        k = None
+        if kx0 is not None:
+            kx0 = np.ascontiguousarray(kx0, dtype=np.float64)
+            k = _capi.dptr(kx0)
+        _capi.check_batch(self.L.qlgpu_batch_set_state(self.b, c, float(t), _capi.dptr(lin), _capi.dptr(mf), k),
+                          self.b)
+
+    def get_state(self, c: int):
+        nxy, nz, nmf = self.dims[c]
+        lin = np.empty((nxy, 4, nz), dtype=np.complex128)
+        mf = np.empty((nmf, nz), dtype=np.complex128)
+        kx0 = np.empty(nxy)
+        t = ctypes.c_double()
+        _capi.check_batch(self.L.qlgpu_batch_get_state(self.b, c, ctypes.byref(t), _capi.dptr(lin), _capi.dptr(mf),
+                                                       _capi.dptr(kx0)), self.b)
+        return t.value, lin, mf, kx0
+
+    def diagnostics(self, c: int) -> np.ndarray:
+        out = np.zeros(15)
+        _capi.check_batch(self.L.qlgpu_batch_diagnostics(self.b, c, _capi.dptr(out)), self.b)
+        return out
+
+    # -- stepping ------------------------------------------------------------
+    def step(self, nsteps: int, diag_every: int = 0) -> list[np.ndarray]:
+        """nsteps steps of every case; per case the diagnostic records [n, 15]."""
+        nc = len(self.cases)
+        if diag_every > 0:
+            cap = nsteps // diag_every + 2
+            out = np.zeros((nc, cap, 15))
+            nd = (ctypes.c_int * nc)()
+            _capi.check_batch(self.L.qlgpu_batch_step(self.b, int(nsteps), int(diag_every), _capi.dptr(out), cap, nd),
+                              self.b)
+            return [out[c, : nd[c]] for c in range(nc)]
+        _capi.check_batch(self.L.qlgpu_batch_step(self.b, int(nsteps), 0, None, 0, None), self.b)
+        return [np.zeros((0, 15)) for _ in range(nc)]
+
+    def step_timed(self, nsteps: int) -> float:
+        """nsteps steps without diagnostics; device time of the launch in ms."""
+        ms = ctypes.c_float()
+        _capi.check_batch(self.L.qlgpu_batch_step_timed(self.b, int(nsteps), ctypes.byref(ms)), self.b)
+        return float(ms.value)
+
+    def tune(self, probe_steps: int = 3) -> float:
+        best = ctypes.c_double()
+        _capi.check_batch(self.L.qlgpu_batch_tune(self.b, int(probe_steps), ctypes.byref(best)), self.b)
+        return best.value
+
+    def mapping(self) -> dict:
+        info = (ctypes.c_int * 4)()
+        nc = len(self.cases)
+        k = (ctypes.c_int * nc)()
+        _capi.check_batch(self.L.qlgpu_batch_mapping(self.b, info, k), self.b)
+        return {"warps": info[0], "grid": info[1], "ctas_per_sm": info[2], "smem": info[3], "ncta": list(k)}
+
+    def set_mapping(self, warps: int, ncta: list[int]):
+        k = (ctypes.c_int * len(ncta))(*ncta)
+        _capi.check_batch(self.L.qlgpu_batch_set_mapping(self.b, int(warps), k), self.b)
+
+    def status(self):
+        nc = len(self.cases)
+        st = (ctypes.c_int * nc)()
+        ls = ctypes.c_int()
+        _capi.check_batch(self.L.qlgpu_batch_status(self.b, st, ctypes.byref(ls)), self.b)
+        return list(st), ls.value
+
+    def set_wait(self, seconds: float):
+        _capi.check_batch(self.L.qlgpu_batch_set_wait(self.b, float(seconds)), self.b)
+
+    def debug_drop_item(self, c: int):
+        """Failure-detection test aid (qlgpu_batch_debug_drop_item)."""
+        _capi.check_batch(self.L.qlgpu_batch_debug_drop_item(self.b, int(c)), self.b)
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _capi.check_batch(self.L.qlgpu_batch_stream(self.b, ctypes.byref(s)), self.b)
+        return s.value or 0
+
+
+# Mode grids, NZ and Pm of the ensemble law.
+ENSEMBLE_GRIDS = (16, 32, 48, 64)
+ENSEMBLE_NZ = (32, 64, 128)
+ENSEMBLE_PM = (1, 2, 4)
+
+
+def mri_ensemble(ncases: int = 48, draw_seed: int = 12345, dt: float = 0.01, **kw):
+    """The QL MRI ensemble: per case a square mode grid from {16, 32, 48, 64},
+    NZ from {32, 64, 128}, Rm log-uniform in [500, 16000], Pm from {1, 2, 4}
+    (eta = 1/Rm, nu = Pm/Rm, as Python/WriteMRIDNSinput.py:22-23 sets them) and
+    a mean-field amplitude B0 uniform in [0.01, 0.1], all drawn from one numpy
+    generator seeded with draw_seed.  Case c uses initial-condition seed c.
+
+    Returns (cases, b0s, seeds)."""
+    rng = np.random.default_rng(draw_seed)
+    cases, b0s = [], []
+    for _ in range(ncases):
+        n = int(rng.choice(ENSEMBLE_GRIDS))
+        NZ = int(rng.choice(ENSEMBLE_NZ))
+        Rm = float(math.exp(rng.uniform(math.log(500.0), math.log(16000.0))))
+        Pm = int(rng.choice(ENSEMBLE_PM))
+        B0 = float(rng.uniform(0.01, 0.1))
+        cases.append(QLParams(nx=n, ny=n, NZ=NZ, nu=Pm / Rm, eta=1.0 / Rm, dt=dt).replace(**kw))
+        b0s.append(B0)
+    return cases, b0s, list(range(ncases))

@@ -5,6 +5,7 @@ Usage: python -m ql_dns_b200.build [--force] [--verbose]
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -20,13 +21,15 @@ MAIN = os.path.join(OUT_DIR, "ql_main")
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
     "--expt-relaxed-constexpr",
 ]
+OBJ_DIR = os.path.join(OUT_DIR, "obj")
 
 
 def sources():
-    return [os.path.join(CSRC, "qlgpu.cu")]
+    """Translation units of libqlgpu.so: the host code and one file per kernel family, compiled in parallel."""
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
 def deps():
@@ -41,14 +44,44 @@ def stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps())
 
 
-def build(force: bool = False, verbose: bool = False, extra=None) -> str:
+def _headers_mtime() -> float:
+    hs = [d for d in deps() if not d.endswith(".cu") and os.path.isfile(d)]
+    return max(os.path.getmtime(h) for h in hs) if hs else 0.0
+
+
+def build(force: bool = False, verbose: bool = False, extra=None, jobs: int | None = None) -> str:
     if not force and not stale():
         return LIB
-    os.makedirs(OUT_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + (extra or []) + ["-I" + os.path.join(ROOT, "include"), "-o", LIB + ".tmp"] + sources()
+    hdr_t = _headers_mtime()
+    inc = ["-I" + os.path.join(ROOT, "include")]
+
+    def compile_one(src):
+        obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
+        if (not force and extra is None and os.path.exists(obj) and os.path.getmtime(obj) > os.path.getmtime(src)
+                and os.path.getmtime(obj) > hdr_t):
+            return obj
+        cmd = [nvcc] + NVCC_FLAGS + (extra or []) + inc + ["-c", "-o", obj + ".tmp.o", src]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.stdout or r.stderr:
+            sys.stderr.write(r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise subprocess.CalledProcessError(r.returncode, cmd)
+        os.replace(obj + ".tmp.o", obj)
+        return obj
+
+    # the kernel translation units are the slow ones: start them first
+    srcs = sorted(sources(), key=lambda f: -os.path.getsize(f) if os.path.basename(f) != "qlgpu.cu" else 0)
+    n = jobs or max(1, min(len(srcs), os.cpu_count() or 1))
+    with concurrent.futures.ThreadPoolExecutor(max_workers=n) as ex:
+        objs = list(ex.map(compile_one, srcs))
+    cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC", "-o",
+           LIB + ".tmp"] + objs
     if verbose:
-        print(" ".join(cmd))
+        print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
     build_main(verbose)

@@ -12,103 +12,14 @@
 #include <vector>
 
 #include "../../include/qlgpu.h"
+#include "qlgpu_host.h"
 #include "qlgpu_kernel.cuh"
 
 using namespace qlgpu;
 
 namespace {
 
-const double kPI = 3.14159265358979323846;  // General_Definitions.h PI
-
 thread_local std::string g_create_error;
-
-// RK3 coefficients (RK3CN_Elin.cpp:19-20, RK3CN.cpp:19-20)
-const double a0_ = 8.0 / 15.0, a1_ = 5.0 / 12.0, a2_ = 3.0 / 4.0, b1_ = -17.0 / 60.0, b2_ = -5.0 / 12.0;
-const double p1_ = 8.0 / 15.0, p2_ = 2.0 / 3.0;
-
-typedef void (*stage_launch_fn)(const StageArgs&, const DevParams&, int grid, int block, size_t smem, cudaStream_t);
-typedef void (*diag_launch_fn)(const cplx*, const cplx*, const double*, const double*, const int*, const int*,
-                               const DevParams&, double, double*, cudaStream_t);
-typedef size_t (*smem_fn)(int warps);
-typedef int (*tmem_fn)(int warps);
-typedef const void* (*kptr_fn)();
-
-template <int NZ, int MODEL, int INTEG, bool TM>
-void launch_stage(const StageArgs& A, const DevParams& P, int grid, int block, size_t smem, cudaStream_t st) {
-    stage_kernel<NZ, MODEL, INTEG, TM><<<grid, block, smem, st>>>(A, P);
-}
-template <int NZ, int MODEL, int INTEG, bool TM>
-const void* stage_ptr() {
-    return reinterpret_cast<const void*>(&stage_kernel<NZ, MODEL, INTEG, TM>);
-}
-template <int NZ, int MODEL, bool TM>
-size_t stage_smem(int warps) {
-    using G = Geom<NZ>;
-    constexpr int NB = MODEL == MODEL_BQLIN ? (int)PB_COUNT : (int)PF_COUNT;
-    using Priv = typename std::conditional<TM, PrivTmem<G, NB>, PrivSmem<G, NB>>::type;
-    return Smem<G, MODEL, Priv>::bytes(warps);
-}
-template <int NZ, int MODEL, bool TM>
-int stage_tmem(int warps) {
-    using G = Geom<NZ>;
-    constexpr int NB = MODEL == MODEL_BQLIN ? (int)PB_COUNT : (int)PF_COUNT;
-    using Priv = typename std::conditional<TM, PrivTmem<G, NB>, PrivSmem<G, NB>>::type;
-    return Smem<G, MODEL, Priv>::tmem_cols(warps);
-}
-template <int NZ>
-void launch_diag(const cplx* lin, const cplx* mf, const double* kx0, const double* ky, const int* kxi, const int* kyi,
-                 const DevParams& P, double t, double* out, cudaStream_t st) {
-    diag_kernel<NZ><<<1, 128, 0, st>>>(lin, mf, kx0, ky, kxi, kyi, P, t, out);
-}
-
-struct Variant {
-    stage_launch_fn launch;
-    kptr_fn kernel;
-    smem_fn smem;
-    tmem_fn tmem;
-    diag_launch_fn diag;
-    int T;   // threads per mode
-    int PL;  // partial vector length
-};
-
-template <int NZ, int MODEL, int INTEG, bool TM>
-Variant make_variant() {
-    Variant v;
-    v.launch = &launch_stage<NZ, MODEL, INTEG, TM>;
-    v.kernel = &stage_ptr<NZ, MODEL, INTEG, TM>;
-    v.smem = &stage_smem<NZ, MODEL, TM>;
-    v.tmem = &stage_tmem<NZ, MODEL, TM>;
-    v.diag = &launch_diag<NZ>;
-    v.T = Geom<NZ>::T;
-    v.PL = (MODEL == MODEL_BQLIN ? 2 : 4) * NZ + 8;
-    return v;
-}
-
-// QLGPU_PRIV_SMEM=1 in the environment selects the shared-memory private store
-// instead of tensor memory (a debugging / comparison switch).
-bool pick_variant(int NZ, int model, int integ, bool tm, Variant* out) {
-#define QLGPU_CASE(NZV)                                                                                          \
-    if (NZ == NZV) {                                                                                             \
-        if (model == MODEL_BQLIN && integ == INTEG_EXP)                                                          \
-            *out = tm ? make_variant<NZV, MODEL_BQLIN, INTEG_EXP, true>() : make_variant<NZV, MODEL_BQLIN, INTEG_EXP, false>(); \
-        else if (model == MODEL_BQLIN && integ == INTEG_CN)                                                      \
-            *out = tm ? make_variant<NZV, MODEL_BQLIN, INTEG_CN, true>() : make_variant<NZV, MODEL_BQLIN, INTEG_CN, false>(); \
-        else if (model == MODEL_FULLQLIN && integ == INTEG_EXP)                                                  \
-            *out = tm ? make_variant<NZV, MODEL_FULLQLIN, INTEG_EXP, true>() : make_variant<NZV, MODEL_FULLQLIN, INTEG_EXP, false>(); \
-        else if (model == MODEL_FULLQLIN && integ == INTEG_CN)                                                   \
-            *out = tm ? make_variant<NZV, MODEL_FULLQLIN, INTEG_CN, true>() : make_variant<NZV, MODEL_FULLQLIN, INTEG_CN, false>(); \
-        else                                                                                                     \
-            return false;                                                                                        \
-        return true;                                                                                             \
-    }
-    QLGPU_CASE(16)
-    QLGPU_CASE(32)
-    QLGPU_CASE(64)
-    QLGPU_CASE(128)
-    QLGPU_CASE(256)
-#undef QLGPU_CASE
-    return false;
-}
 
 }  // namespace
 
@@ -150,6 +61,7 @@ struct qlgpu_handle {
     std::vector<double> kx_tab, ky_tab;
     std::vector<int> kxi_tab, kyi_tab;
     std::vector<double> il2_tab, ekz_tab;
+    StageConst sc[3];
     std::string err;
 };
 
@@ -167,32 +79,6 @@ int fail(qlgpu_t* h, int code, const std::string& msg) {
         if (e_ != cudaSuccess)                                                                  \
             return fail(h, QLGPU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
-
-// Kdata tables (QL_DNS/Auxiliary/Kdata.cpp:24-46)
-void ktables(const qlgpu_params& p, std::vector<double>& kx, std::vector<double>& ky, std::vector<int>& kxi,
-             std::vector<int>& kyi) {
-    const double kxL = 2 * kPI / p.L[0], kyL = 2 * kPI / p.L[1];
-    const int ny = ((p.ny / 2) * 2) / 2, nx = p.nx / 2;
-    const int nxy = (p.nx - 1) * (p.ny / 2);
-    kx.assign(nxy, 0.0);
-    ky.assign(nxy, 0.0);
-    kxi.assign(nxy, 0);
-    kyi.assign(nxy, 0);
-    for (int i = 0; i < nx; ++i)
-        for (int j = 0; j < ny; ++j) {
-            kx[j + ny * i] = i * kxL;
-            ky[j + ny * i] = j * kyL;
-            kxi[j + ny * i] = i;
-            kyi[j + ny * i] = j;
-        }
-    for (int i = nx + 1; i < 2 * nx; ++i)
-        for (int j = 0; j < ny; ++j) {
-            kx[j + ny * (i - 1)] = (-2 * nx + i) * kxL;
-            ky[j + ny * (i - 1)] = j * kyL;
-            kxi[j + ny * (i - 1)] = -2 * nx + i;
-            kyi[j + ny * (i - 1)] = j;
-        }
-}
 
 int reset_clock(qlgpu_t* h, double t) {
     DevClock c;
@@ -227,17 +113,6 @@ StageArgs base_args(qlgpu_t* h) {
 // One RK3 step = three stage launches (RK3CN_Elin::Step / RK3CN::Step).
 // ev (optional): 4 events recorded before stage 1 and after each stage.
 void enqueue_step(qlgpu_t* h, cudaEvent_t* ev = nullptr) {
-    const double dt = h->p.dt;
-    const bool cn = h->p.integrator == INTEG_CN;
-    const double lcf = cn ? dt / 2 : dt;
-    struct {
-        double t_off, dt_lin, linC, n1, n2;
-        int has_prev;
-    } st[3] = {
-        {0.0, dt * p1_, lcf * (a0_), a0_ * dt, 0.0, 0},
-        {dt * p1_, dt * (p2_ - p1_), lcf * (a1_ + b1_), a1_ * dt, b1_ * dt, 1},
-        {dt * p2_, dt * (1.0 - p2_), lcf * (a2_ + b2_), a2_ * dt, b2_ * dt, 1},
-    };
     cplx* Fbuf[3] = {h->d_F1, h->d_F2, nullptr};
     const cplx* Fprev[3] = {nullptr, h->d_F1, h->d_F2};
     cplx* Fmf[3] = {h->d_Fmf1, h->d_Fmf2, h->d_Fmf1};
@@ -251,13 +126,7 @@ void enqueue_step(qlgpu_t* h, cudaEvent_t* ev = nullptr) {
         A.Fout = Fbuf[s];
         A.Fmf_prev = Fmfp[s];
         A.Fmf_out = (s < 2) ? Fmf[s] : nullptr;
-        A.sc.t_off = st[s].t_off;
-        A.sc.dt_lin = st[s].dt_lin;
-        A.sc.linC = st[s].linC;
-        A.sc.n1 = st[s].n1;
-        A.sc.n2 = st[s].n2;
-        A.sc.has_prev = st[s].has_prev;
-        A.sc.last = (s == 2);
+        A.sc = h->sc[s];
         if (A.trace) A.trace += 32 * s;
         A.ekz_tab = h->d_ekz + (size_t)s * 2 * h->nz;
         h->var.launch(A, h->dp, h->grid, h->block, h->smem, h->stream);
@@ -300,17 +169,11 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
     if (!pp || !out) return fail(nullptr, QLGPU_ERR_ARG, "null argument");
     *out = nullptr;
     const qlgpu_params& p = *pp;
-    if (p.model != QLGPU_MODEL_MHD_BQLIN && p.model != QLGPU_MODEL_MHD_FULLQLIN)
-        return fail(nullptr, QLGPU_ERR_ARG, "unknown model (no matching model found, main.cpp:71-74)");
-    if (p.integrator != QLGPU_INTEG_RK3CN_ELIN && p.integrator != QLGPU_INTEG_RK3CN)
-        return fail(nullptr, QLGPU_ERR_ARG, "unknown integrator");
-    if (p.nx < 2 || (p.nx % 2) || p.ny < 2 || (p.ny % 2))
-        return fail(nullptr, QLGPU_ERR_ARG, "nx and ny must be even and >= 2");
-    if (!(p.dt > 0))
-        return fail(nullptr, QLGPU_ERR_UNSUPPORTED, "dt must be > 0 (variable CFL time step not supported)");
-    if (!(p.L[0] > 0 && p.L[1] > 0 && p.L[2] > 0)) return fail(nullptr, QLGPU_ERR_ARG, "box lengths must be > 0");
-    if (p.model == QLGPU_MODEL_MHD_BQLIN && p.nu == 0.0)
-        return fail(nullptr, QLGPU_ERR_ARG, "MHD_BQlin divides by nu (MHD_BQlin.cpp:251); nu must be nonzero");
+    {
+        std::string msg;
+        const int prc = check_params(p, &msg);
+        if (prc != QLGPU_OK) return fail(nullptr, prc, msg);
+    }
     Variant var;
     const char* ps = std::getenv("QLGPU_PRIV_SMEM");
     const bool use_tmem = !(ps && ps[0] == '1');
@@ -336,43 +199,12 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
         return bail(QLGPU_ERR_NODEVICE);
     }
     h->NZ = p.NZ;
-    h->nz = 1 + 2 * int(p.NZ / 3.0);
-    h->nxy = (p.nx - 1) * (p.ny / 2);
-    h->nmf = p.model == QLGPU_MODEL_MHD_BQLIN ? 2 : 4;
-    // Device parameters
-    DevParams& d = h->dp;
-    std::memset(&d, 0, sizeof(d));
-    d.nxy = h->nxy;
-    d.nz = h->nz;
-    d.NZ = h->NZ;
-    d.nmf = h->nmf;
-    d.q = p.q;
-    d.Omega = p.model == QLGPU_MODEL_MHD_BQLIN ? 2.0 / 3.0 * p.q : p.omega;
-    d.nu = p.nu;
-    d.eta = p.eta;
-    d.etanu = p.model == QLGPU_MODEL_MHD_BQLIN ? p.eta / p.nu : p.eta;
-    d.cb = p.model == QLGPU_MODEL_MHD_BQLIN ? (p.eta / p.nu) * p.nu : p.eta;
-    // -|(-kx^2-ky^2)+kz2|^(order/2) is linear in kz2 only for order/2 == 1 (MHD_FullQlin.cpp:372)
-    d.factored = (p.model == QLGPU_MODEL_MHD_BQLIN || p.viscosity_order / 2 == 1) ? 1 : 0;
-    d.B0z = p.B0z;
-    d.visc_half = p.viscosity_order / 2;
-    d.ql = p.quasilinear ? 1 : 0;
-    d.remap = p.remap ? 1 : 0;
-    d.kzL = 2 * kPI / p.L[2];
-    d.fac = 1.0 / p.NZ;
-    const int Nx = p.nx, Ny = (p.ny / 2) * 2;
-    d.rs_fac = 1.0 / (Ny * Nx) / (Ny * Nx);
-    long totalN2 = (long)Nx * Ny * p.NZ;
-    totalN2 = totalN2 * totalN2;
-    d.divfac = p.L[2] / (double)totalN2;
-    d.divMF = p.L[2] / ((double)p.NZ * p.NZ);
-    const double kxLfac = 2 * kPI / p.L[0];
-    const int nxm1 = Nx - 1;
-    d.remap_thresh = nxm1 / 2.0 * kxLfac;
-    d.remap_shift = nxm1 * kxLfac;
-    d.dt = p.dt;
-    d.tv_interval = 0.0;
-    d.kzmax = 2 * kPI / p.L[2] * (p.NZ / 3);
+    h->nz = stored_nz(p.NZ);
+    h->nxy = mode_count(p);
+    h->nmf = mean_field_count(p);
+    h->dp = make_devparams(p);
+    for (int s = 0; s < 3; ++s) h->sc[s] = stage_const(p, s);
+    const DevParams& d = h->dp;
 
     ktables(p, h->kx_tab, h->ky_tab, h->kxi_tab, h->kyi_tab);
     // Launch geometry: as many CTAs as fit, at most one mode per group
@@ -470,53 +302,12 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
     QLGPU_ALLOC(h->d_ilap2, (size_t)(p.ny / 2) * h->nz * sizeof(double));
     QLGPU_ALLOC(h->d_mfr, (size_t)8 * h->NZ * sizeof(double));
     QLGPU_ALLOC(h->d_ekz, (size_t)6 * h->nz * sizeof(double));
-    // Twiddles tw[n2*T + t] = exp(+2 pi i n2 t/NZ)
-    std::vector<cplx> tw(h->NZ);
-    const int T = var.T, P = h->NZ / T;
-    for (int n2 = 0; n2 < P; ++n2)
-        for (int t = 0; t < T; ++t) {
-            const int m = (n2 * t) % h->NZ;
-            const double ang = 2.0 * kPI * (double)m / (double)h->NZ;
-            tw[n2 * T + t].x = std::cos(ang);
-            tw[n2 * T + t].y = std::sin(ang);
-        }
-    cudaMemcpyAsync(h->d_tw, tw.data(), tw.size() * sizeof(cplx), cudaMemcpyHostToDevice, h->stream);
-    // 1/lap2 per (ky index, stored kz), Kdata.cpp:100-119 (kept for the lifetime of the handle)
-    h->il2_tab.assign((size_t)(p.ny / 2) * h->nz, 0.0);
-    {
-        const double kyL = 2 * kPI / p.L[1], kzL = 2 * kPI / p.L[2];
-        const int nzl = (h->nz - 1) / 2;
-        for (int j = 0; j < p.ny / 2; ++j) {
-            const double kyr = j * kyL;
-            for (int s = 0; s < h->nz; ++s) {
-                const int kzi = s <= nzl ? s : (-2 * nzl + s - 1);
-                const double c = kzi * kzL;
-                const double kz2 = 0.0 * 0.0 - c * c;
-                double l2 = -kyr * kyr + kz2;
-                double il2 = 1 / l2;
-                if (kyr == 0 && s == 0) il2 = 1;
-                h->il2_tab[(size_t)j * h->nz + s] = il2;
-            }
-        }
-    }
-    {
-        // exp(linC nu kz2), exp(linC (eta/nu) nu kz2) per stage (RK3CN_Elin.cpp:89,122,155)
-        const double dt = p.dt;
-        const double linC[3] = {dt * (a0_), dt * (a1_ + b1_), dt * (a2_ + b2_)};
-        const double kzL = 2 * kPI / p.L[2];
-        const int nzl = (h->nz - 1) / 2;
-        h->ekz_tab.assign((size_t)6 * h->nz, 1.0);
-        for (int st = 0; st < 3; ++st)
-            for (int s = 0; s < h->nz; ++s) {
-                const int kzi = s <= nzl ? s : s - h->nz;
-                const double c = kzi * kzL;
-                const double kz2 = -(c * c);
-                h->ekz_tab[(size_t)(st * 2) * h->nz + s] = std::exp(linC[st] * d.nu * kz2);
-                h->ekz_tab[(size_t)(st * 2 + 1) * h->nz + s] = std::exp(linC[st] * d.cb * kz2);
-            }
-        cudaMemcpyAsync(h->d_ekz, h->ekz_tab.data(), h->ekz_tab.size() * sizeof(double), cudaMemcpyHostToDevice,
-                        h->stream);
-    }
+    const std::vector<double> tw = twiddles(h->NZ, var.T);
+    cudaMemcpyAsync(h->d_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    h->il2_tab = ilap2_table(p, h->nz);
+    h->ekz_tab = ekz_table(p, d);
+    cudaMemcpyAsync(h->d_ekz, h->ekz_tab.data(), h->ekz_tab.size() * sizeof(double), cudaMemcpyHostToDevice,
+                    h->stream);
     cudaMemcpyAsync(h->d_ilap2, h->il2_tab.data(), h->il2_tab.size() * sizeof(double), cudaMemcpyHostToDevice,
                     h->stream);
     cudaMemcpyAsync(h->d_kx0, h->kx_tab.data(), h->nxy * sizeof(double), cudaMemcpyHostToDevice, h->stream);

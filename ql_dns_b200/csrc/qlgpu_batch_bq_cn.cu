@@ -1,0 +1,6 @@
+// Persistent batch kernel for MHD_BQlin with RK3CN (NZ = 16 ... 256 in one kernel).
+#include "qlgpu_batch_inst.cuh"
+
+namespace qlgpu {
+bool batch_kernel_bq_cn(BatchKernel* out) { return make_batch_kernel<MODEL_BQLIN, INTEG_CN>(out); }
+}  // namespace qlgpu

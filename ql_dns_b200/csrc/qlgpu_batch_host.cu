@@ -1,0 +1,1036 @@
+// qlgpu_batch_host.cu -- host side of the batched ensemble (qlgpu_batch_* in
+// include/qlgpu.h): per-case device buffers in one arena, the case
+// descriptors of the persistent kernel, the CTA mapping and its autotuner, and
+// the CUDA-graph launch of the persistent kernel.
+//
+// Mapping model.  A CTA of w warps steps mpc = w*(32/T)/2 modes of a case at a
+// time (one mode per pair of transform groups).  Giving case c k CTAs costs it
+// rounds(c, k) = ceil(nxy_c / (k*mpc)) passes of its stage pipeline per stage.
+// A CTA that owns several work items runs them one after the other, so its
+// stage time is modelled as the sum over its items of
+//     beta + rounds * r[NZ],
+// and the launch time per stage as the largest CTA time plus a per-stage
+// constant alpha (reduction, mean-field stage, release / wait).  The planner
+// binary-searches the smallest per-CTA budget M for which every case's CTA
+// count k_c(M) fits and first-fit-decreasing packs all items onto the launch's
+// CTAs.  The autotuner measures the per-case finishing times of probe launches
+// (%globaltimer stamps written by the kernel), fits alpha, beta and r[NZ] by
+// least squares, re-plans, and keeps the fastest measured mapping over the CTA
+// widths 8 and 4 warps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/qlgpu.h"
+#include "qlgpu_host.h"
+#include "qlgpu_kernel.cuh"
+
+using namespace qlgpu;
+
+namespace {
+
+thread_local std::string g_batch_create_error;
+
+constexpr int NCLASS = 5;  // NZ = 16, 32, 64, 128, 256
+inline int nz_class(int NZ) {
+    switch (NZ) {
+        case 16: return 0;
+        case 32: return 1;
+        case 64: return 2;
+        case 128: return 3;
+        default: return 4;
+    }
+}
+
+struct CaseHost {
+    qlgpu_params p;
+    DevParams dp;
+    StageConst sc[3];
+    int nxy = 0, nz = 0, NZ = 0, nmf = 0, T = 0, PL = 0, max_cta = 0;
+    Variant var;  // single-case variant of the same NZ (initial diagnostics)
+    // device pointers into the arena
+    cplx* lin[2] = {nullptr, nullptr};
+    cplx *F1 = nullptr, *F2 = nullptr, *mf = nullptr, *Fmf1 = nullptr, *Fmf2 = nullptr, *tw = nullptr;
+    double *kx0 = nullptr, *ky = nullptr, *il2 = nullptr, *partials = nullptr, *gpartials = nullptr;
+    double *mfr = nullptr, *ekz = nullptr;
+    int *kxi = nullptr, *kyi = nullptr;
+    DevClock* clk = nullptr;
+    double* diag = nullptr;
+    int diag_cap = 0;
+    std::vector<double> kx_tab;
+};
+
+// One work item of the planner: CTA number i of the k given to case c.
+struct Item {
+    int c, i, k;
+    double cost;
+};
+
+struct CostModel {
+    double alpha = 12.0;                              // us per stage, per launch
+    double beta = 2.5;                                // us per work item per stage
+    double r[NCLASS] = {4.0, 6.0, 14.0, 30.0, 70.0};  // us per pipeline pass, per NZ class
+};
+
+// Zeroes the launch control words, the case stage counters and the reduction
+// counters (left non-zero only by a launch that gave up), and optionally the
+// diagnostic record counts.
+__global__ void batch_reset_kernel(const BatchCase* cases, int ncases, unsigned* epoch, BatchCtl* ctl,
+                                   int reset_ndiag) {
+    const int c = blockIdx.x;
+    if (c == 0 && threadIdx.x == 0) {
+        ctl->status = 0;
+        ctl->abort = 0;
+        ctl->fail_case = -1;
+        ctl->fail_stage = -1;
+        ctl->t_start = 0;
+    }
+    if (c >= ncases) return;
+    DevClock* clk = cases[c].A[0].clk;
+    if (threadIdx.x < 64) clk->cnt_group[threadIdx.x] = 0u;
+    if (threadIdx.x == 0) {
+        clk->cnt_top = 0u;
+        epoch[(size_t)c * BATCH_EPOCH_STRIDE] = 0u;
+        if (reset_ndiag) clk->ndiag = 0;
+    }
+}
+
+// Gathers every case's status word and diagnostic record count.
+__global__ void batch_collect_kernel(const BatchCase* cases, int ncases, int* out /* [ncases][2] */) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncases; c += gridDim.x * blockDim.x) {
+        const DevClock* clk = cases[c].A[0].clk;
+        out[2 * c] = clk->status;
+        out[2 * c + 1] = clk->ndiag;
+    }
+}
+
+}  // namespace
+
+struct qlgpu_batch {
+    int device = 0, model = 0, integ = 0, ncases = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<CaseHost> cs;
+    unsigned char* arena = nullptr;
+    size_t arena_bytes = 0;
+    BatchCase* d_cases = nullptr;
+    BatchCta* d_ctas = nullptr;
+    unsigned* d_epoch = nullptr;
+    BatchCtl* d_ctl = nullptr;
+    unsigned long long* d_case_end = nullptr;
+    int* d_collect = nullptr;
+    double* d_out15 = nullptr;
+    BatchKernel bk;
+    int sms = 0;
+    size_t smem_optin = 0;
+    // current mapping
+    int warps = 8, per_sm = 1, grid = 0;
+    size_t smem = 0;
+    std::vector<BatchCta> ctas;
+    std::vector<int> ncta;
+    CostModel cost;
+    int cur = 0;
+    long long wait_ns = 2000000000LL;
+    bool use_graph = true;
+    std::map<std::tuple<int, int, int>, cudaGraphExec_t> graphs;  // (nsteps, parity, reset_ndiag)
+    std::vector<double> tv_set;  // diagnostic interval in each case's uploaded descriptor
+    bool descr_dirty = true;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    std::string err;
+};
+
+namespace {
+
+int bfail(qlgpu_batch_t* b, int code, const std::string& msg) {
+    if (b) b->err = msg;
+    else g_batch_create_error = msg;
+    return code;
+}
+
+#define QB_CK(call)                                                                              \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return bfail(b, QLGPU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+int modes_per_cta(int warps, int T) { return warps * (32 / T) / 2; }
+
+int rounds_of(const CaseHost& c, int k, int warps) {
+    const int m = modes_per_cta(warps, c.T) * k;
+    return (c.nxy + m - 1) / m;
+}
+
+void drop_graphs(qlgpu_batch_t* b) {
+    for (auto& kv : b->graphs)
+        if (kv.second) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+}
+
+// CTAs per SM and dynamic shared memory of a CTA width over the NZ classes present.
+bool width_limits(qlgpu_batch_t* b, int warps, int* per_sm, size_t* smem) {
+    size_t sm = 0;
+    int tc = 0;
+    for (const CaseHost& c : b->cs) {
+        sm = std::max(sm, b->bk.smem(c.NZ, warps));
+        tc = std::max(tc, b->bk.tmem(c.NZ, warps));
+    }
+    if (sm > b->smem_optin || tc > 512) return false;
+    if (cudaFuncSetAttribute(b->bk.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+        return false;
+    cudaFuncSetAttribute(b->bk.kernel(), cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b->bk.kernel(), 32 * warps, sm) != cudaSuccess) return false;
+    if (tc > 0) occ = std::min(occ, 512 / tc);  // TMEM columns per SM: an allocation beyond them would wait
+    if (occ < 1) return false;
+    *per_sm = occ;
+    *smem = sm;
+    return true;
+}
+
+// Plan: CTAs per case and the packing of work items onto at most G CTAs.
+// fixed_k (optional) pins the CTA count of every case.
+bool plan(const qlgpu_batch_t* b, int warps, int G, const CostModel& cm, const int* fixed_k, std::vector<int>& k_out,
+          std::vector<std::vector<Item>>& bins_out, double* makespan) {
+    const int nc = b->ncases;
+    auto item_cost = [&](int c, int k) {
+        const CaseHost& h = b->cs[c];
+        return cm.beta + rounds_of(h, k, warps) * cm.r[nz_class(h.NZ)];
+    };
+    auto try_budget = [&](double M, std::vector<int>& k, std::vector<std::vector<Item>>& bins) -> bool {
+        k.assign(nc, 1);
+        std::vector<Item> items;
+        for (int c = 0; c < nc; ++c) {
+            const CaseHost& h = b->cs[c];
+            if (fixed_k) {
+                k[c] = fixed_k[c];
+            } else {
+                const int kmax = std::min(h.max_cta, G);
+                int kk = 1;
+                while (kk < kmax && item_cost(c, kk) > M) {
+                    // next CTA count that lowers the number of passes
+                    const int r = rounds_of(h, kk, warps);
+                    const int m = modes_per_cta(warps, h.T);
+                    int nk = r > 1 ? (h.nxy + m * (r - 1) - 1) / (m * (r - 1)) : kk + 1;
+                    if (nk <= kk) nk = kk + 1;
+                    kk = std::min(nk, kmax);
+                }
+                if (item_cost(c, kk) > M) return false;
+                k[c] = kk;
+            }
+            for (int i = 0; i < k[c]; ++i) items.push_back(Item{c, i, k[c], item_cost(c, k[c])});
+        }
+        std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.cost > y.cost; });
+        bins.clear();
+        std::vector<double> load;
+        for (const Item& it : items) {
+            int best = -1;
+            for (size_t j = 0; j < bins.size(); ++j)
+                if ((int)bins[j].size() < BATCH_MAX_SLOTS && load[j] + it.cost <= M) {
+                    best = (int)j;
+                    break;
+                }
+            if (best < 0) {
+                if ((int)bins.size() >= G) return false;
+                bins.emplace_back();
+                load.push_back(0.0);
+                best = (int)bins.size() - 1;
+            }
+            bins[best].push_back(it);
+            load[best] += it.cost;
+        }
+        return true;
+    };
+    double lo = 0.0, hi = 0.0;
+    for (int c = 0; c < nc; ++c) {
+        const int kmin = fixed_k ? fixed_k[c] : 1;
+        const int kbest = fixed_k ? fixed_k[c] : std::min(b->cs[c].max_cta, G);
+        lo = std::max(lo, item_cost(c, kbest));
+        hi += item_cost(c, kmin) * kmin;
+    }
+    hi = std::max(hi, lo) * 1.0001 + 1.0;
+    std::vector<int> kb;
+    std::vector<std::vector<Item>> bb;
+    if (!try_budget(hi, kb, bb)) return false;  // more items than CTA slots
+    for (int it = 0; it < 60 && hi - lo > 1e-3 * hi; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        std::vector<int> k;
+        std::vector<std::vector<Item>> bins;
+        if (try_budget(mid, k, bins)) {
+            hi = mid;
+            kb.swap(k);
+            bb.swap(bins);
+        } else {
+            lo = mid;
+        }
+    }
+    k_out = kb;
+    bins_out = bb;
+    if (makespan) *makespan = hi;
+    return true;
+}
+
+// Device descriptors of every case.
+int upload_descriptors(qlgpu_batch_t* b) {
+    std::vector<BatchCase> hc(b->ncases);
+    for (int c = 0; c < b->ncases; ++c) {
+        CaseHost& h = b->cs[c];
+        BatchCase& d = hc[c];
+        std::memset(&d, 0, sizeof(d));
+        d.P = h.dp;
+        d.P.tv_interval = b->tv_set[c];
+        cplx* Fbuf[3] = {h.F1, h.F2, nullptr};
+        const cplx* Fprev[3] = {nullptr, h.F1, h.F2};
+        cplx* Fmf[3] = {h.Fmf1, h.Fmf2, nullptr};
+        const cplx* Fmfp[3] = {nullptr, h.Fmf1, h.Fmf2};
+        for (int s = 0; s < 3; ++s) {
+            StageArgs& A = d.A[s];
+            A.lin_in = h.lin[s & 1];
+            A.lin_out = h.lin[(s & 1) ^ 1];
+            A.Fprev = Fprev[s];
+            A.Fout = Fbuf[s];
+            A.mf = h.mf;
+            A.Fmf_prev = Fmfp[s];
+            A.Fmf_out = Fmf[s];
+            A.kx0 = h.kx0;
+            A.ky = h.ky;
+            A.kxi = h.kxi;
+            A.kyi = h.kyi;
+            A.tw = h.tw;
+            A.ilap2 = h.il2;
+            A.partials = h.partials;
+            A.gpartials = h.gpartials;
+            A.clk = h.clk;
+            A.diag_ring = h.diag;
+            A.diag_cap = h.diag_cap;
+            A.mfr_cache = h.mfr;
+            A.ekz_tab = h.ekz + (size_t)s * 2 * h.nz;
+            A.sc = h.sc[s];
+        }
+    }
+    QB_CK(cudaMemcpyAsync(b->d_cases, hc.data(), sizeof(BatchCase) * hc.size(), cudaMemcpyHostToDevice, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    b->descr_dirty = false;
+    return QLGPU_OK;
+}
+
+// Install a mapping (CTA width + packed work items).
+int apply_mapping(qlgpu_batch_t* b, int warps, int per_sm, size_t smem, const std::vector<int>& k,
+                  const std::vector<std::vector<Item>>& bins) {
+    std::vector<BatchCta> ctas(bins.size());
+    for (size_t j = 0; j < bins.size(); ++j) {
+        BatchCta& m = ctas[j];
+        std::memset(&m, 0, sizeof(m));
+        m.nslots = (int)bins[j].size();
+        int tc = 0;
+        for (int i = 0; i < m.nslots; ++i) {
+            const Item& it = bins[j][i];
+            m.slot[i].c = it.c;
+            m.slot[i].cta = it.i;
+            m.slot[i].ncta = it.k;
+            m.slot[i].NZ = b->cs[it.c].NZ;
+            tc = std::max(tc, b->bk.tmem(b->cs[it.c].NZ, warps));
+        }
+        m.tcols = tc;
+    }
+    if (cudaFuncSetAttribute(b->bk.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return bfail(b, QLGPU_ERR_CUDA, "batch kernel: shared memory request too large");
+    QB_CK(cudaMemcpyAsync(b->d_ctas, ctas.data(), sizeof(BatchCta) * ctas.size(), cudaMemcpyHostToDevice, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    b->ctas = ctas;
+    b->ncta = k;
+    b->warps = warps;
+    b->per_sm = per_sm;
+    b->smem = smem;
+    b->grid = (int)ctas.size();
+    drop_graphs(b);
+    return QLGPU_OK;
+}
+
+int plan_and_apply(qlgpu_batch_t* b, int warps, const int* fixed_k) {
+    int per_sm = 0;
+    size_t smem = 0;
+    if (!width_limits(b, warps, &per_sm, &smem))
+        return bfail(b, QLGPU_ERR_UNSUPPORTED, "batch: CTA width does not fit (shared memory / TMEM)");
+    const int G = std::min(b->sms * per_sm, b->sms * 2);
+    std::vector<int> k;
+    std::vector<std::vector<Item>> bins;
+    if (fixed_k)
+        for (int c = 0; c < b->ncases; ++c)
+            if (fixed_k[c] < 1 || fixed_k[c] > b->cs[c].max_cta)
+                return bfail(b, QLGPU_ERR_ARG, "batch mapping: CTAs per case out of range");
+    if (!plan(b, warps, G, b->cost, fixed_k, k, bins, nullptr))
+        return bfail(b, QLGPU_ERR_UNSUPPORTED,
+                     "batch: the cases do not fit one launch (at most 8 work items on each co-resident CTA)");
+    return apply_mapping(b, warps, per_sm, smem, k, bins);
+}
+
+BatchLaunch launch_args(qlgpu_batch_t* b, int nsteps) {
+    BatchLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.cases = b->d_cases;
+    L.ctas = b->d_ctas;
+    L.epoch = b->d_epoch;
+    L.ctl = b->d_ctl;
+    L.case_end = b->d_case_end;
+    L.nsteps = nsteps;
+    L.parity = b->cur;
+    L.wait_ns = b->wait_ns;
+    return L;
+}
+
+// Enqueue the reset kernel and the persistent launch on the batch stream.
+cudaError_t enqueue_launch(qlgpu_batch_t* b, int nsteps, int reset_ndiag) {
+    batch_reset_kernel<<<b->ncases, 64, 0, b->stream>>>(b->d_cases, b->ncases, b->d_epoch, b->d_ctl, reset_ndiag);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return b->bk.launch(launch_args(b, nsteps), b->grid, 32 * b->warps, b->smem, b->stream);
+}
+
+int run_launch(qlgpu_batch_t* b, int nsteps, int reset_ndiag) {
+    if (b->descr_dirty) {
+        int rc = upload_descriptors(b);
+        if (rc) return rc;
+    }
+    if (nsteps == 0) return QLGPU_OK;
+    // the dynamic shared memory attribute belongs to the kernel, not to this batch
+    QB_CK(cudaFuncSetAttribute(b->bk.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+    if (b->use_graph) {
+        const auto key = std::make_tuple(nsteps, b->cur, reset_ndiag);
+        auto itg = b->graphs.find(key);
+        if (itg == b->graphs.end()) {
+            if (b->graphs.size() >= 8) drop_graphs(b);
+            cudaGraph_t g = nullptr;
+            QB_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            const cudaError_t le = enqueue_launch(b, nsteps, reset_ndiag);
+            const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+            if (le != cudaSuccess || ce != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                return bfail(b, QLGPU_ERR_CUDA,
+                             std::string("batch graph capture: ") + cudaGetErrorString(le != cudaSuccess ? le : ce));
+            }
+            cudaGraphExec_t ex = nullptr;
+            const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) return bfail(b, QLGPU_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(ie));
+            itg = b->graphs.emplace(key, ex).first;
+        }
+        QB_CK(cudaGraphLaunch(itg->second, b->stream));
+    } else {
+        QB_CK(enqueue_launch(b, nsteps, reset_ndiag));
+    }
+    b->cur = (b->cur + nsteps) & 1;
+    return QLGPU_OK;
+}
+
+int check_launch_status(qlgpu_batch_t* b) {
+    BatchCtl ctl;
+    QB_CK(cudaMemcpyAsync(&ctl, b->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    if (ctl.status & QLGPU_STATUS_TIMEOUT) {
+        char buf[200];
+        std::snprintf(buf, sizeof(buf),
+                      "batch: a CTA gave up waiting for case %d at stage %d (wait bound %.3g s); the state of the "
+                      "batch is undefined",
+                      ctl.fail_case, ctl.fail_stage, b->wait_ns * 1e-9);
+        return bfail(b, QLGPU_ERR_STATUS, buf);
+    }
+    return QLGPU_OK;
+}
+
+int reset_case_clock(qlgpu_batch_t* b, int c, double t) {
+    DevClock k;
+    std::memset(&k, 0, sizeof(k));
+    k.t = t;
+    k.old_init = 1;
+    QB_CK(cudaMemcpyAsync(b->cs[c].clk, &k, sizeof(k), cudaMemcpyHostToDevice, b->stream));
+    return QLGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qlgpu_batch_last_error(const qlgpu_batch_t* b, char* buf, int buflen) {
+    const std::string& s = b ? b->err : g_batch_create_error;
+    if (buf && buflen > 0) std::snprintf(buf, (size_t)buflen, "%s", s.c_str());
+    return (int)s.size();
+}
+
+int qlgpu_batch_destroy(qlgpu_batch_t* b) {
+    if (!b) return QLGPU_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    drop_graphs(b);
+    for (CaseHost& c : b->cs)
+        if (c.diag) cudaFree(c.diag);
+    void* bufs[] = {b->arena, b->d_cases, b->d_ctas, b->d_epoch, b->d_ctl, b->d_case_end, b->d_collect, b->d_out15};
+    for (void* p : bufs)
+        if (p) cudaFree(p);
+    for (cudaEvent_t e : b->ev)
+        if (e) cudaEventDestroy(e);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_batch_t** out) {
+    qlgpu_batch_t* b = nullptr;
+    if (!cases || !out || ncases < 1) return bfail(nullptr, QLGPU_ERR_ARG, "null argument or ncases < 1");
+    *out = nullptr;
+    for (int c = 0; c < ncases; ++c) {
+        std::string msg;
+        const int rc = check_params(cases[c], &msg);
+        if (rc) return bfail(nullptr, rc, "case " + std::to_string(c) + ": " + msg);
+        if (cases[c].model != cases[0].model || cases[c].integrator != cases[0].integrator)
+            return bfail(nullptr, QLGPU_ERR_UNSUPPORTED, "all cases of a batch share the model and the integrator");
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return bfail(nullptr, QLGPU_ERR_NODEVICE, "no CUDA device");
+    b = new (std::nothrow) qlgpu_batch();
+    if (!b) return bfail(nullptr, QLGPU_ERR_ARG, "out of host memory");
+    auto bail = [&](int code) {
+        g_batch_create_error = b->err;
+        qlgpu_batch_destroy(b);
+        return code;
+    };
+    if (device < 0) cudaGetDevice(&device);
+    b->device = device;
+    b->model = cases[0].model;
+    b->integ = cases[0].integrator;
+    b->ncases = ncases;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        b->err = "cudaSetDevice failed";
+        return bail(QLGPU_ERR_NODEVICE);
+    }
+    if (!pick_batch_kernel(b->model, b->integ, &b->bk)) {
+        b->err = "no batch kernel for this model / integrator";
+        return bail(QLGPU_ERR_UNSUPPORTED);
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        b->err = "cudaGetDeviceProperties failed";
+        return bail(QLGPU_ERR_CUDA);
+    }
+    if (!prop.cooperativeLaunch) {
+        b->err = "device does not support cooperative launches";
+        return bail(QLGPU_ERR_UNSUPPORTED);
+    }
+    b->sms = prop.multiProcessorCount;
+    b->smem_optin = prop.sharedMemPerBlockOptin;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        b->err = "stream create failed";
+        return bail(QLGPU_ERR_CUDA);
+    }
+    {
+        const char* g = std::getenv("QLGPU_BATCH_GRAPH");
+        b->use_graph = !(g && g[0] == '0');
+    }
+    // Per-case sizes and the arena layout
+    b->cs.resize(ncases);
+    b->tv_set.assign(ncases, 0.0);
+    const int max_grid = 2 * b->sms;  // widest launch: 4-warp CTAs, two per SM
+    std::vector<size_t> off(ncases);
+    size_t o = 0;
+    for (int c = 0; c < ncases; ++c) {
+        CaseHost& h = b->cs[c];
+        h.p = cases[c];
+        h.dp = make_devparams(h.p);
+        for (int s = 0; s < 3; ++s) h.sc[s] = stage_const(h.p, s);
+        h.nxy = h.dp.nxy;
+        h.nz = h.dp.nz;
+        h.NZ = h.p.NZ;
+        h.nmf = h.dp.nmf;
+        h.T = group_threads(h.NZ);
+        h.PL = (h.nmf == 2 ? 2 : 4) * h.NZ + 8;
+        h.max_cta = std::min(max_grid, (h.nxy + modes_per_cta(4, h.T) - 1) / modes_per_cta(4, h.T));
+        h.max_cta = std::min(h.max_cta, 64 * RED_GROUP);
+        if (!pick_variant(h.NZ, b->model, b->integ, true, &h.var)) {
+            b->err = "unsupported NZ";
+            return bail(QLGPU_ERR_UNSUPPORTED);
+        }
+        const size_t nlin = (size_t)h.nxy * 4 * h.nz, nmfe = (size_t)h.nmf * h.nz;
+        off[c] = o;
+        o += 4 * al256(nlin * sizeof(cplx));                       // lin[2], F1, F2
+        o += 3 * al256(nmfe * sizeof(cplx));                       // mf, Fmf1, Fmf2
+        o += 2 * al256(h.nxy * sizeof(double));                    // kx0, ky
+        o += 2 * al256(h.nxy * sizeof(int));                       // kxi, kyi
+        o += al256(h.NZ * sizeof(cplx));                           // twiddles
+        o += al256((size_t)(h.p.ny / 2) * h.nz * sizeof(double));  // 1/lap2
+        o += al256((size_t)h.max_cta * h.PL * sizeof(double));     // partials
+        o += al256((size_t)((h.max_cta + RED_GROUP - 1) / RED_GROUP) * h.PL * sizeof(double));
+        o += al256(sizeof(DevClock));
+        o += al256((size_t)8 * h.NZ * sizeof(double));  // mean-field profile cache
+        o += al256((size_t)6 * h.nz * sizeof(double));  // integrating-factor tables
+    }
+    b->arena_bytes = o;
+    if (cudaMalloc(&b->arena, o) != cudaSuccess) {
+        b->err = "cudaMalloc of the batch arena failed (" + std::to_string(o >> 20) + " MiB)";
+        return bail(QLGPU_ERR_CUDA);
+    }
+    cudaMemsetAsync(b->arena, 0, o, b->stream);
+    for (int c = 0; c < ncases; ++c) {
+        CaseHost& h = b->cs[c];
+        unsigned char* p = b->arena + off[c];
+        const size_t nlin = (size_t)h.nxy * 4 * h.nz, nmfe = (size_t)h.nmf * h.nz;
+        auto take = [&](size_t bytes) {
+            unsigned char* r = p;
+            p += al256(bytes);
+            return r;
+        };
+        h.lin[0] = reinterpret_cast<cplx*>(take(nlin * sizeof(cplx)));
+        h.lin[1] = reinterpret_cast<cplx*>(take(nlin * sizeof(cplx)));
+        h.F1 = reinterpret_cast<cplx*>(take(nlin * sizeof(cplx)));
+        h.F2 = reinterpret_cast<cplx*>(take(nlin * sizeof(cplx)));
+        h.mf = reinterpret_cast<cplx*>(take(nmfe * sizeof(cplx)));
+        h.Fmf1 = reinterpret_cast<cplx*>(take(nmfe * sizeof(cplx)));
+        h.Fmf2 = reinterpret_cast<cplx*>(take(nmfe * sizeof(cplx)));
+        h.kx0 = reinterpret_cast<double*>(take(h.nxy * sizeof(double)));
+        h.ky = reinterpret_cast<double*>(take(h.nxy * sizeof(double)));
+        h.kxi = reinterpret_cast<int*>(take(h.nxy * sizeof(int)));
+        h.kyi = reinterpret_cast<int*>(take(h.nxy * sizeof(int)));
+        h.tw = reinterpret_cast<cplx*>(take(h.NZ * sizeof(cplx)));
+        h.il2 = reinterpret_cast<double*>(take((size_t)(h.p.ny / 2) * h.nz * sizeof(double)));
+        h.partials = reinterpret_cast<double*>(take((size_t)h.max_cta * h.PL * sizeof(double)));
+        h.gpartials = reinterpret_cast<double*>(
+            take((size_t)((h.max_cta + RED_GROUP - 1) / RED_GROUP) * h.PL * sizeof(double)));
+        h.clk = reinterpret_cast<DevClock*>(take(sizeof(DevClock)));
+        h.mfr = reinterpret_cast<double*>(take((size_t)8 * h.NZ * sizeof(double)));
+        h.ekz = reinterpret_cast<double*>(take((size_t)6 * h.nz * sizeof(double)));
+        // tables (Kdata.cpp:24-46,100-119; twiddles; exp(linC nu kz2) per stage)
+        std::vector<double> ky;
+        std::vector<int> kxi, kyi;
+        ktables(h.p, h.kx_tab, ky, kxi, kyi);
+        const std::vector<double> tw = twiddles(h.NZ, h.T);
+        const std::vector<double> il2 = ilap2_table(h.p, h.nz);
+        const std::vector<double> ekz = ekz_table(h.p, h.dp);
+        cudaMemcpyAsync(h.kx0, h.kx_tab.data(), h.nxy * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+        cudaMemcpyAsync(h.ky, ky.data(), h.nxy * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+        cudaMemcpyAsync(h.kxi, kxi.data(), h.nxy * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+        cudaMemcpyAsync(h.kyi, kyi.data(), h.nxy * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+        cudaMemcpyAsync(h.tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+        cudaMemcpyAsync(h.il2, il2.data(), il2.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+        cudaMemcpyAsync(h.ekz, ekz.data(), ekz.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+        if (reset_case_clock(b, c, 0.0)) return bail(QLGPU_ERR_CUDA);
+        // the host vectors above die at the end of this iteration: finish the copies first
+        if (cudaStreamSynchronize(b->stream) != cudaSuccess) {
+            b->err = "table upload failed";
+            return bail(QLGPU_ERR_CUDA);
+        }
+    }
+#define QB_ALLOC(ptr, bytes)                          \
+    if (cudaMalloc(&(ptr), (bytes)) != cudaSuccess) { \
+        b->err = "cudaMalloc failed for " #ptr;       \
+        return bail(QLGPU_ERR_CUDA);                  \
+    }                                                 \
+    cudaMemsetAsync((ptr), 0, (bytes), b->stream);
+    QB_ALLOC(b->d_cases, sizeof(BatchCase) * ncases);
+    QB_ALLOC(b->d_ctas, sizeof(BatchCta) * (size_t)max_grid);
+    QB_ALLOC(b->d_epoch, sizeof(unsigned) * BATCH_EPOCH_STRIDE * (size_t)ncases);
+    QB_ALLOC(b->d_ctl, sizeof(BatchCtl));
+    QB_ALLOC(b->d_case_end, sizeof(unsigned long long) * ncases);
+    QB_ALLOC(b->d_collect, sizeof(int) * 2 * ncases);
+    QB_ALLOC(b->d_out15, sizeof(double) * 15);
+#undef QB_ALLOC
+    if (cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess) {
+        b->err = "event create failed";
+        return bail(QLGPU_ERR_CUDA);
+    }
+    // initial mapping from the cost model: the widest CTA that fits
+    int rc = plan_and_apply(b, 8, nullptr);
+    if (rc) rc = plan_and_apply(b, 4, nullptr);
+    if (rc) return bail(rc);
+    rc = upload_descriptors(b);
+    if (rc) return bail(rc);
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) {
+        b->err = "initialisation failed";
+        return bail(QLGPU_ERR_CUDA);
+    }
+    *out = b;
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_dims(const qlgpu_batch_t* b, int c, int* nxy, int* nz, int* nmf) {
+    if (!b || c < 0 || c >= b->ncases) return QLGPU_ERR_ARG;
+    if (nxy) *nxy = b->cs[c].nxy;
+    if (nz) *nz = b->cs[c].nz;
+    if (nmf) *nmf = b->cs[c].nmf;
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_set_state(qlgpu_batch_t* b, int c, double t, const double* lin, const double* mf, const double* kx0) {
+    if (!b) return QLGPU_ERR_ARG;
+    if (c < 0 || c >= b->ncases || !lin || !mf) return bfail(b, QLGPU_ERR_ARG, "bad case index or null state");
+    QB_CK(cudaSetDevice(b->device));
+    CaseHost& h = b->cs[c];
+    const size_t nlin = (size_t)h.nxy * 4 * h.nz, nmfe = (size_t)h.nmf * h.nz;
+    QB_CK(cudaMemcpyAsync(h.lin[b->cur], lin, nlin * sizeof(cplx), cudaMemcpyHostToDevice, b->stream));
+    QB_CK(cudaMemcpyAsync(h.mf, mf, nmfe * sizeof(cplx), cudaMemcpyHostToDevice, b->stream));
+    QB_CK(cudaMemcpyAsync(h.kx0, kx0 ? kx0 : h.kx_tab.data(), h.nxy * sizeof(double), cudaMemcpyHostToDevice,
+                          b->stream));
+    int rc = reset_case_clock(b, c, t);
+    if (rc) return rc;
+    QB_CK(cudaStreamSynchronize(b->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_get_state(qlgpu_batch_t* b, int c, double* t, double* lin, double* mf, double* kx0) {
+    if (!b) return QLGPU_ERR_ARG;
+    if (c < 0 || c >= b->ncases) return bfail(b, QLGPU_ERR_ARG, "bad case index");
+    QB_CK(cudaSetDevice(b->device));
+    CaseHost& h = b->cs[c];
+    const size_t nlin = (size_t)h.nxy * 4 * h.nz, nmfe = (size_t)h.nmf * h.nz;
+    if (lin) QB_CK(cudaMemcpyAsync(lin, h.lin[b->cur], nlin * sizeof(cplx), cudaMemcpyDeviceToHost, b->stream));
+    if (mf) QB_CK(cudaMemcpyAsync(mf, h.mf, nmfe * sizeof(cplx), cudaMemcpyDeviceToHost, b->stream));
+    if (kx0) QB_CK(cudaMemcpyAsync(kx0, h.kx0, h.nxy * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    double tt = 0;
+    QB_CK(cudaMemcpyAsync(&tt, &h.clk->t, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    if (t) *t = tt;
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_diagnostics(qlgpu_batch_t* b, int c, double* out15) {
+    if (!b || !out15) return QLGPU_ERR_ARG;
+    if (c < 0 || c >= b->ncases) return bfail(b, QLGPU_ERR_ARG, "bad case index");
+    QB_CK(cudaSetDevice(b->device));
+    CaseHost& h = b->cs[c];
+    double t = 0;
+    QB_CK(cudaMemcpyAsync(&t, &h.clk->t, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    h.var.diag(h.lin[b->cur], h.mf, h.kx0, h.ky, h.kxi, h.kyi, h.dp, t, b->d_out15, b->stream);
+    QB_CK(cudaGetLastError());
+    QB_CK(cudaMemcpyAsync(out15, b->d_out15, 15 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_step(qlgpu_batch_t* b, int nsteps, int diag_every, double* diag_out, int max_diag, int* ndiag) {
+    if (!b) return QLGPU_ERR_ARG;
+    if (nsteps < 0) return bfail(b, QLGPU_ERR_ARG, "nsteps < 0");
+    if (diag_every > 0 && (!diag_out || !ndiag || max_diag < 1))
+        return bfail(b, QLGPU_ERR_ARG, "diag_out, ndiag and max_diag >= 1 required");
+    QB_CK(cudaSetDevice(b->device));
+    for (int c = 0; c < b->ncases; ++c) {
+        CaseHost& h = b->cs[c];
+        const double tv = diag_every > 0 ? diag_every * h.p.dt : 0.0;
+        if (tv != b->tv_set[c]) {
+            b->tv_set[c] = tv;
+            b->descr_dirty = true;
+        }
+        if (diag_every > 0 && h.diag_cap < max_diag) {
+            if (h.diag) cudaFree(h.diag);
+            h.diag = nullptr;
+            h.diag_cap = 0;
+            QB_CK(cudaMalloc(&h.diag, sizeof(double) * 15 * (size_t)max_diag));
+            h.diag_cap = max_diag;
+            b->descr_dirty = true;
+        }
+    }
+    int rc = run_launch(b, nsteps, diag_every > 0 ? 1 : 0);
+    if (rc) return rc;
+    rc = check_launch_status(b);
+    if (rc) return rc;
+    std::vector<int> col(2 * (size_t)b->ncases);
+    batch_collect_kernel<<<(b->ncases + 127) / 128, 128, 0, b->stream>>>(b->d_cases, b->ncases, b->d_collect);
+    QB_CK(cudaGetLastError());
+    QB_CK(cudaMemcpyAsync(col.data(), b->d_collect, col.size() * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    int bad = -1;
+    for (int c = 0; c < b->ncases; ++c) {
+        if (diag_every > 0) {
+            const int n = std::min(col[2 * c + 1], max_diag);
+            ndiag[c] = n;
+            if (n > 0)
+                QB_CK(cudaMemcpy(diag_out + (size_t)c * max_diag * 15, b->cs[c].diag, sizeof(double) * 15 * (size_t)n,
+                                 cudaMemcpyDeviceToHost));
+        }
+        if (bad < 0 && (col[2 * c] & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE | QLGPU_STATUS_DIAG_FULL)))
+            bad = c;
+    }
+    if (bad >= 0) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "case %d: device status 0x%x (non-finite, unstable or records dropped)", bad,
+                      col[2 * bad]);
+        return bfail(b, QLGPU_ERR_STATUS, buf);
+    }
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_step_timed(qlgpu_batch_t* b, int nsteps, float* ms) {
+    if (!b || !ms || nsteps < 1) return QLGPU_ERR_ARG;
+    QB_CK(cudaSetDevice(b->device));
+    for (int c = 0; c < b->ncases; ++c)
+        if (b->tv_set[c] != 0.0) {
+            b->tv_set[c] = 0.0;
+            b->descr_dirty = true;
+        }
+    if (b->descr_dirty) {
+        int rc = upload_descriptors(b);
+        if (rc) return rc;
+    }
+    QB_CK(cudaEventRecord(b->ev[0], b->stream));
+    int rc = run_launch(b, nsteps, 0);
+    if (rc) return rc;
+    QB_CK(cudaEventRecord(b->ev[1], b->stream));
+    QB_CK(cudaEventSynchronize(b->ev[1]));
+    QB_CK(cudaEventElapsedTime(ms, b->ev[0], b->ev[1]));
+    return check_launch_status(b);
+}
+
+int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms) {
+    if (!b || probe_steps < 1) return QLGPU_ERR_ARG;
+    QB_CK(cudaSetDevice(b->device));
+    // probes run on the batch's own buffers; a copy of the whole arena is restored afterwards
+    unsigned char* backup = nullptr;
+    QB_CK(cudaMalloc(&backup, b->arena_bytes));
+    struct Restore {
+        qlgpu_batch_t* b;
+        unsigned char* p;
+        int cur;
+        ~Restore() {
+            cudaMemcpyAsync(b->arena, p, b->arena_bytes, cudaMemcpyDeviceToDevice, b->stream);
+            cudaStreamSynchronize(b->stream);
+            cudaFree(p);
+            b->cur = cur;
+        }
+    } restore{b, backup, b->cur};
+    QB_CK(cudaMemcpyAsync(backup, b->arena, b->arena_bytes, cudaMemcpyDeviceToDevice, b->stream));
+    for (int c = 0; c < b->ncases; ++c)
+        if (b->tv_set[c] != 0.0) {
+            b->tv_set[c] = 0.0;
+            b->descr_dirty = true;
+        }
+    if (b->descr_dirty) {
+        int rc = upload_descriptors(b);
+        if (rc) return rc;
+    }
+    struct Best {
+        double ms = 1e300;
+        int warps = 0, per_sm = 0;
+        size_t smem = 0;
+        std::vector<int> k;
+        std::vector<std::vector<Item>> bins;
+        CostModel cm;
+    } best;
+    std::vector<unsigned long long> ends(b->ncases);
+    // one probe of the current mapping: launch time and per-case stage times (us per stage)
+    auto probe = [&](double* ms, std::vector<double>* ystage) -> int {
+        QB_CK(cudaFuncSetAttribute(b->bk.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        QB_CK(cudaEventRecord(b->ev[0], b->stream));
+        QB_CK(enqueue_launch(b, probe_steps, 0));
+        QB_CK(cudaEventRecord(b->ev[1], b->stream));
+        QB_CK(cudaEventSynchronize(b->ev[1]));
+        float f = 0;
+        QB_CK(cudaEventElapsedTime(&f, b->ev[0], b->ev[1]));
+        b->cur = (b->cur + probe_steps) & 1;
+        int rc = check_launch_status(b);
+        if (rc) return rc;
+        BatchCtl ctl;
+        QB_CK(cudaMemcpy(&ctl, b->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+        QB_CK(cudaMemcpy(ends.data(), b->d_case_end, sizeof(unsigned long long) * b->ncases, cudaMemcpyDeviceToHost));
+        *ms = f;
+        if (ystage) {
+            ystage->resize(b->ncases);
+            for (int c = 0; c < b->ncases; ++c)
+                (*ystage)[c] = (double)(long long)(ends[c] - ctl.t_start) * 1e-3 / (3.0 * probe_steps);
+        }
+        return QLGPU_OK;
+    };
+    // least-squares fit of alpha, beta, r[NZ] to the per-case stage times, ridge towards the prior
+    auto fit = [&](const std::vector<double>& y, CostModel& cm) {
+        const int nu = 2 + NCLASS;
+        // the CTA that finished a case last is modelled as the most loaded CTA holding one of its items
+        std::vector<double> load(b->ctas.size(), 0.0);
+        for (size_t j = 0; j < b->ctas.size(); ++j)
+            for (int i = 0; i < b->ctas[j].nslots; ++i) {
+                const BatchSlot& s = b->ctas[j].slot[i];
+                load[j] += cm.beta + rounds_of(b->cs[s.c], s.ncta, b->warps) * cm.r[nz_class(s.NZ)];
+            }
+        std::vector<int> crit(b->ncases, -1);
+        for (size_t j = 0; j < b->ctas.size(); ++j)
+            for (int i = 0; i < b->ctas[j].nslots; ++i) {
+                const int c = b->ctas[j].slot[i].c;
+                if (crit[c] < 0 || load[j] > load[crit[c]]) crit[c] = (int)j;
+            }
+        std::vector<std::vector<double>> rows(b->ncases, std::vector<double>(nu, 0.0));
+        for (int c = 0; c < b->ncases; ++c) {
+            std::vector<double>& r = rows[c];
+            r[0] = 1.0;
+            if (crit[c] < 0) continue;
+            const BatchCta& m = b->ctas[crit[c]];
+            for (int i = 0; i < m.nslots; ++i) {
+                const BatchSlot& s = m.slot[i];
+                r[1] += 1.0;
+                r[2 + nz_class(s.NZ)] += rounds_of(b->cs[s.c], s.ncta, b->warps);
+            }
+        }
+        double prior[2 + NCLASS];
+        prior[0] = cm.alpha;
+        prior[1] = cm.beta;
+        for (int j = 0; j < NCLASS; ++j) prior[2 + j] = cm.r[j];
+        std::vector<double> M((size_t)nu * nu, 0.0), v(nu, 0.0);
+        const double lam = 1e-3;
+        for (int c = 0; c < b->ncases; ++c)
+            for (int i = 0; i < nu; ++i) {
+                v[i] += rows[c][i] * y[c];
+                for (int j = 0; j < nu; ++j) M[i * nu + j] += rows[c][i] * rows[c][j];
+            }
+        for (int i = 0; i < nu; ++i) {
+            const double w = lam * (1.0 + M[i * nu + i]);
+            M[i * nu + i] += w;
+            v[i] += w * prior[i];
+        }
+        // Gaussian elimination with partial pivoting
+        std::vector<double> x(nu, 0.0);
+        for (int col = 0; col < nu; ++col) {
+            int piv = col;
+            for (int r = col + 1; r < nu; ++r)
+                if (std::fabs(M[r * nu + col]) > std::fabs(M[piv * nu + col])) piv = r;
+            for (int j = 0; j < nu; ++j) std::swap(M[col * nu + j], M[piv * nu + j]);
+            std::swap(v[col], v[piv]);
+            const double d = M[col * nu + col];
+            if (std::fabs(d) < 1e-300) return;
+            for (int r = col + 1; r < nu; ++r) {
+                const double f = M[r * nu + col] / d;
+                for (int j = col; j < nu; ++j) M[r * nu + j] -= f * M[col * nu + j];
+                v[r] -= f * v[col];
+            }
+        }
+        for (int i = nu - 1; i >= 0; --i) {
+            double s = v[i];
+            for (int j = i + 1; j < nu; ++j) s -= M[i * nu + j] * x[j];
+            x[i] = s / M[i * nu + i];
+        }
+        cm.alpha = std::max(0.0, x[0]);
+        cm.beta = std::max(0.0, x[1]);
+        for (int j = 0; j < NCLASS; ++j)
+            if (x[2 + j] > 0) cm.r[j] = x[2 + j];
+    };
+    int rc = QLGPU_OK;
+    for (int warps : {8, 4}) {
+        int per_sm = 0;
+        size_t smem = 0;
+        if (!width_limits(b, warps, &per_sm, &smem)) continue;
+        const int G = std::min(b->sms * per_sm, b->sms * 2);
+        CostModel cm = b->cost;
+        for (int pass = 0; pass < 3; ++pass) {
+            std::vector<int> k;
+            std::vector<std::vector<Item>> bins;
+            if (!plan(b, warps, G, cm, nullptr, k, bins, nullptr)) break;
+            rc = apply_mapping(b, warps, per_sm, smem, k, bins);
+            if (rc) return rc;
+            double ms = 0;
+            std::vector<double> y;
+            rc = probe(&ms, nullptr);  // warm-up of this mapping
+            if (rc) return rc;
+            rc = probe(&ms, &y);
+            if (rc) return rc;
+            if (ms < best.ms) {
+                best.ms = ms;
+                best.warps = warps;
+                best.per_sm = per_sm;
+                best.smem = smem;
+                best.k = k;
+                best.bins = bins;
+                best.cm = cm;
+            }
+            fit(y, cm);
+        }
+    }
+    if (best.warps == 0) return bfail(b, QLGPU_ERR_UNSUPPORTED, "batch tune: no CTA width fits");
+    b->cost = best.cm;
+    rc = apply_mapping(b, best.warps, best.per_sm, best.smem, best.k, best.bins);
+    if (rc) return rc;
+    if (best_ms) *best_ms = best.ms;
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_mapping(const qlgpu_batch_t* b, int* info4, int* ncta) {
+    if (!b) return QLGPU_ERR_ARG;
+    if (info4) {
+        info4[0] = b->warps;
+        info4[1] = b->grid;
+        info4[2] = b->per_sm;
+        info4[3] = (int)b->smem;
+    }
+    if (ncta)
+        for (int c = 0; c < b->ncases; ++c) ncta[c] = b->ncta[c];
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_set_mapping(qlgpu_batch_t* b, int warps, const int* ncta) {
+    if (!b || !ncta) return QLGPU_ERR_ARG;
+    if (warps != 4 && warps != 8) return bfail(b, QLGPU_ERR_ARG, "warps per CTA must be 4 or 8");
+    QB_CK(cudaSetDevice(b->device));
+    return plan_and_apply(b, warps, ncta);
+}
+
+int qlgpu_batch_status(qlgpu_batch_t* b, int* case_status, int* launch_status) {
+    if (!b) return QLGPU_ERR_ARG;
+    QB_CK(cudaSetDevice(b->device));
+    if (case_status) {
+        std::vector<int> col(2 * (size_t)b->ncases);
+        batch_collect_kernel<<<(b->ncases + 127) / 128, 128, 0, b->stream>>>(b->d_cases, b->ncases, b->d_collect);
+        QB_CK(cudaGetLastError());
+        QB_CK(cudaMemcpyAsync(col.data(), b->d_collect, col.size() * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+        QB_CK(cudaStreamSynchronize(b->stream));
+        for (int c = 0; c < b->ncases; ++c) case_status[c] = col[2 * c];
+    }
+    if (launch_status) {
+        BatchCtl ctl;
+        QB_CK(cudaMemcpyAsync(&ctl, b->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, b->stream));
+        QB_CK(cudaStreamSynchronize(b->stream));
+        *launch_status = ctl.status;
+    }
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_set_wait(qlgpu_batch_t* b, double seconds) {
+    if (!b || !(seconds > 0) || seconds > 60) return QLGPU_ERR_ARG;
+    b->wait_ns = (long long)(seconds * 1e9);
+    drop_graphs(b);
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_debug_drop_item(qlgpu_batch_t* b, int c) {
+    if (!b) return QLGPU_ERR_ARG;
+    if (c < 0 || c >= b->ncases || b->ncta[c] < 2)
+        return bfail(b, QLGPU_ERR_ARG, "drop item: the case needs two or more CTAs");
+    QB_CK(cudaSetDevice(b->device));
+    std::vector<BatchCta> ctas = b->ctas;
+    bool done = false;
+    for (size_t j = 0; j < ctas.size() && !done; ++j)
+        for (int i = 0; i < ctas[j].nslots; ++i)
+            if (ctas[j].slot[i].c == c && ctas[j].slot[i].cta == b->ncta[c] - 1) {
+                for (int m = i + 1; m < ctas[j].nslots; ++m) ctas[j].slot[m - 1] = ctas[j].slot[m];
+                ctas[j].nslots -= 1;
+                done = true;
+                break;
+            }
+    if (!done) return bfail(b, QLGPU_ERR_ARG, "drop item: item not found");
+    QB_CK(cudaMemcpyAsync(b->d_ctas, ctas.data(), sizeof(BatchCta) * ctas.size(), cudaMemcpyHostToDevice, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    b->ctas = ctas;
+    drop_graphs(b);
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_stream(qlgpu_batch_t* b, void** stream) {
+    if (!b || !stream) return QLGPU_ERR_ARG;
+    *stream = (void*)b->stream;
+    return QLGPU_OK;
+}
+
+}  // extern "C"

@@ -253,19 +253,41 @@ struct Smem {
     }
 };
 
-template <int NZ, int MODEL, int INTEG, bool USE_TMEM>
-__global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
+// Static shared words of a stage: the TMEM base address, the last-arriver flag
+// and a flag the persistent batch kernel uses to leave its step loop.
+struct StageShared {
+    uint32_t tmem;
+    int last;
+    int ok;
+    int pad;
+};
+
+// Types of one stage variant.
+template <int NZ, int MODEL, bool USE_TMEM>
+struct StageKind {
     using G = Geom<NZ>;
-    constexpr int NB = MODEL == MODEL_BQLIN ? (int)PB_COUNT : (int)PF_COUNT;
+    static constexpr int NB = MODEL == MODEL_BQLIN ? (int)PB_COUNT : (int)PF_COUNT;
     using Priv = typename std::conditional<USE_TMEM, PrivTmem<G, NB>, PrivSmem<G, NB>>::type;
     using SM = Smem<G, MODEL, Priv>;
+};
+
+// One stage over the modes of one case, executed by one CTA that is number
+// `cta` of the `ncta` CTAs working on that case.  The CTA's TMEM columns (if
+// any) are allocated by the caller and passed in ss.tmem.  Returns true in the
+// one CTA that arrived last and ran the mean-field stage; every other CTA
+// returns as soon as its partial sums are published.
+template <int NZ, int MODEL, int INTEG, bool USE_TMEM>
+__device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& P, const int cta, const int ncta,
+                                           unsigned char* smem_raw, StageShared& ss) {
+    using K = StageKind<NZ, MODEL, USE_TMEM>;
+    using G = typename K::G;
+    constexpr int NB = K::NB;
+    using Priv = typename K::Priv;
+    using SM = typename K::SM;
     constexpr int SW = SM::SW;
     static_assert(SW % 2 == 0, "a warp holds whole pairs of groups");
     constexpr int NEMF = SM::NEMF;
     constexpr int PL = SM::PL;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ uint32_t s_tmem;
-    __shared__ int s_last;
     const int warps = blockDim.x >> 5;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int slot = lane / G::T, t = lane % G::T;
@@ -285,19 +307,14 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
     // optional trace (CTA 0 thread 0 and the top CTA): [0] start, [1] prologue done,
     // [2] mode loop done, [3] partials written, [4] top CTA start, [5] top done,
     // [8] first mode staged, [9..18] start of pipeline steps 0..9
-    const bool tr = A.trace && blockIdx.x == 0 && tid == 0;
-    const bool tr2 = A.trace && blockIdx.x == gridDim.x - 1 && tid == 0;
+    const bool tr = A.trace && cta == 0 && tid == 0;
+    const bool tr2 = A.trace && cta == ncta - 1 && tid == 0;
     if (tr) A.trace[0] = gtimer();
     if (tr2) A.trace[20] = gtimer();
     // ---- private store: TMEM allocation (one warp) or a shared-memory region
     Priv pv;
-    const int tcols = SM::tmem_cols(warps);
     if constexpr (USE_TMEM) {
-        if (warp == 0) tmem_alloc(&s_tmem, (uint32_t)tcols);
-        tmem_fence_before_sync();
-        __syncthreads();
-        tmem_fence_after_sync();
-        pv.init(s_tmem, warp);
+        pv.init(ss.tmem, warp);
     } else {
         pv.init(reinterpret_cast<cplx*>(work + SM::work_bytes(warps)) + (size_t)warp * NB * G::P * 32, lane);
     }
@@ -372,8 +389,8 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
     // ---- mode loop: one mode per pair of groups, warp-uniform trip count (TMEM access is warp-wide)
     constexpr int PW = SW / 2;  // pairs per warp
     if (tr) A.trace[6] = gtimer();
-    const int wglobal = blockIdx.x * warps + warp;
-    const int WG = gridDim.x * warps;
+    const int wglobal = cta * warps + warp;
+    const int WG = ncta * warps;
     for (int base = wglobal * PW; base < P.nxy; base += WG * PW) {
         const int mode_raw = base + pi;
         const bool valid = mode_raw < P.nxy;
@@ -386,7 +403,7 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
                                           tclock, cn);
         if (last && valid && role == 0) {
             // ShearingBox_Remap(q t) after t += dt (main.cpp:122-123, MHD_BQlin.cpp:319-329)
-            double kx0 = A.kx0[mode];
+            double kx0 = __ldcg(A.kx0 + mode);
             const double ky = __ldg(A.ky + mode);
             bool zeroed = false;
             if (P.remap) {
@@ -447,11 +464,8 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
     for (int c = 0; c < 6; ++c) dred[tid * 6 + c] = dacc[c];
     if constexpr (USE_TMEM) tmem_fence_before_sync();
     __syncthreads();
-    if constexpr (USE_TMEM) {
-        tmem_fence_after_sync();
-        if (warp == 0) tmem_dealloc(s_tmem, (uint32_t)tcols);
-    }
-    double* part = A.partials + (size_t)blockIdx.x * PL;
+    if constexpr (USE_TMEM) tmem_fence_after_sync();
+    double* part = A.partials + (size_t)cta * PL;
     for (int idx = tid; idx < NEMF * G::NZ; idx += blockDim.x) {
         double s = 0.0;
         for (int w = 0; w < warps; ++w) s += red[w * NEMF * G::NZ + idx];
@@ -467,16 +481,16 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
     __threadfence();
     __syncthreads();
     if (tr) A.trace[3] = gtimer();
-    const int ngroups = (gridDim.x + RED_GROUP - 1) / RED_GROUP;
-    const int grp = blockIdx.x / RED_GROUP;
+    const int ngroups = (ncta + RED_GROUP - 1) / RED_GROUP;
+    const int grp = cta / RED_GROUP;
     const int c0 = grp * RED_GROUP;
-    const int cn_in = min(RED_GROUP, (int)gridDim.x - c0);
+    const int cn_in = min(RED_GROUP, ncta - c0);
     if (tid == 0) {
         unsigned tk = atomicAdd(&A.clk->cnt_group[grp], 1u);
-        s_last = (tk == (unsigned)(cn_in - 1));
+        ss.last = (tk == (unsigned)(cn_in - 1));
     }
     __syncthreads();
-    if (!s_last) return;
+    if (!ss.last) return false;
     __threadfence();
     double* gpart = A.gpartials + (size_t)grp * PL;
     for (int idx = tid; idx < PL; idx += blockDim.x) {
@@ -484,22 +498,22 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
         for (int c = 0; c < cn_in; ++c) s += __ldcg(A.partials + (size_t)(c0 + c) * PL + idx);
         gpart[idx] = s;
     }
-    if (tid == 0) A.clk->cnt_group[grp] = 0u;
+    if (tid == 0) atomicExch(&A.clk->cnt_group[grp], 0u);
     __threadfence();
     __syncthreads();
     if (tid == 0) {
         unsigned tk = atomicAdd(&A.clk->cnt_top, 1u);
-        s_last = (tk == (unsigned)(ngroups - 1));
+        ss.last = (tk == (unsigned)(ngroups - 1));
     }
     __syncthreads();
-    if (!s_last) return;
+    if (!ss.last) return false;
     __threadfence();
     for (int idx = tid; idx < PL; idx += blockDim.x) {
         double s = 0.0;
         for (int g = 0; g < ngroups; ++g) s += __ldcg(A.gpartials + (size_t)g * PL + idx);
         tot[idx] = s;
     }
-    if (tid == 0) A.clk->cnt_top = 0u;
+    if (tid == 0) atomicExch(&A.clk->cnt_top, 0u);
     if (A.trace && tid == 0) A.trace[4] = gtimer();
     __syncthreads();
     mean_field_stage<G, MODEL, INTEG, NEMF>(A, P, tot, spec, xch, tw_s, gidx, ngc, t, gmask, tclock, t_new, last,
@@ -515,6 +529,31 @@ __global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
         if (tid == 0) A.clk->mfr_valid = 1;
     }
     if (A.trace && tid == 0) A.trace[5] = gtimer();
+    return true;
+}
+
+// One stage launch of a single case: one CTA per SM at most, TMEM allocated
+// for the duration of the launch.
+template <int NZ, int MODEL, int INTEG, bool USE_TMEM>
+__global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
+    using SM = typename StageKind<NZ, MODEL, USE_TMEM>::SM;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ StageShared ss;
+    const int warp = threadIdx.x >> 5;
+    const int tcols = SM::tmem_cols(blockDim.x >> 5);
+    if constexpr (USE_TMEM) {
+        if (warp == 0) tmem_alloc(&ss.tmem, (uint32_t)tcols);
+        tmem_fence_before_sync();
+        __syncthreads();
+        tmem_fence_after_sync();
+    }
+    stage_body<NZ, MODEL, INTEG, USE_TMEM>(A, P, (int)blockIdx.x, (int)gridDim.x, smem_raw, ss);
+    if constexpr (USE_TMEM) {
+        tmem_fence_before_sync();
+        __syncthreads();
+        tmem_fence_after_sync();
+        if (warp == 0) tmem_dealloc(ss.tmem, (uint32_t)tcols);
+    }
 }
 
 // Diagnostics of the current state without stepping (the initial record,

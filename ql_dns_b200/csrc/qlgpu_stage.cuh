@@ -25,8 +25,11 @@ namespace qlgpu {
 // ---------------------------------------------------------------------------
 // Small helpers
 // ---------------------------------------------------------------------------
+// State loads (fields, previous right-hand sides) go through L2 (ld.global.cg):
+// the persistent batch kernel rewrites these buffers while it runs, so the
+// non-coherent read-only path must not cache them.
 __device__ __forceinline__ cplx ldc(const cplx* p) {
-    double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    double2 v = __ldcg(reinterpret_cast<const double2*>(p));
     return mk(v.x, v.y);
 }
 __device__ __forceinline__ cplx ldc_cg(const cplx* p) {
@@ -185,7 +188,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
     const double fac = P.fac;
     if (A.trace && blockIdx.x == 0 && threadIdx.x == 0) A.trace[7] = gtimer();
     const double ky = __ldg(A.ky + mode);
-    const double kx0 = A.kx0[mode];
+    const double kx0 = __ldcg(A.kx0 + mode);
     const int kyi = __ldg(A.kyi + mode), kxi = __ldg(A.kxi + mode);
     const double ts = S.abs_time ? S.t_off : __dadd_rn(tclock, S.t_off);
     const double a = kx_at(kx0, P.q, ts, ky);  // kx(t_s), MHD_BQlin.cpp:498
@@ -504,7 +507,7 @@ __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParam
     const StageConst& S = A.sc;
     const double fac = P.fac;
     const double ky = __ldg(A.ky + mode);
-    const double kx0 = A.kx0[mode];
+    const double kx0 = __ldcg(A.kx0 + mode);
     const int kyi = __ldg(A.kyi + mode), kxi = __ldg(A.kxi + mode);
     const double ts = S.abs_time ? S.t_off : __dadd_rn(tclock, S.t_off);
     const double a = kx_at(kx0, P.q, ts, ky);  // kx(t_s), MHD_FullQlin.cpp:727

@@ -88,8 +88,56 @@ struct StageArgs {
     StageConst sc;
 };
 
+// ---------------------------------------------------------------------------
+// Batched ensemble (persistent kernel, qlgpu_batch.cuh)
+// ---------------------------------------------------------------------------
+constexpr int BATCH_MAX_SLOTS = 8;      // work items (case, CTA index) per CTA
+constexpr int BATCH_EPOCH_STRIDE = 32;  // words between the per-case stage counters (one 128-byte line each)
+
+// One case of a batch in device memory: its run constants and the arguments of
+// its three stages for a step that starts from lin buffer 0 (the kernel swaps
+// lin_in / lin_out on steps that start from buffer 1).
+struct BatchCase {
+    DevParams P;
+    StageArgs A[3];
+};
+
+// One work item: CTA number `cta` of the `ncta` CTAs that step case `c`.
+struct BatchSlot {
+    int c, cta, ncta, NZ;
+};
+
+// The work list of one CTA of the persistent launch.
+struct BatchCta {
+    int nslots;
+    int tcols;  // TMEM columns the CTA allocates (the largest of its slots' needs)
+    int pad[2];
+    BatchSlot slot[BATCH_MAX_SLOTS];
+};
+
+// Launch-wide control words (zeroed before every launch).
+struct BatchCtl {
+    int status;      // QLGPU_STATUS_TIMEOUT when a wait gave up
+    int abort;       // set with the timeout: every waiting CTA leaves
+    int fail_case;   // case and stage of the first wait that gave up
+    int fail_stage;
+    unsigned long long t_start;  // %globaltimer at the start of CTA 0
+};
+
+struct BatchLaunch {
+    const BatchCase* cases;
+    const BatchCta* ctas;
+    unsigned* epoch;               // [ncases * BATCH_EPOCH_STRIDE] stages completed in this launch
+    BatchCtl* ctl;
+    unsigned long long* case_end;  // [ncases] %globaltimer when the case finished its last stage
+    int nsteps;
+    int parity;                    // 1: the first step starts from lin buffer 1
+    long long wait_ns;             // bound on one wait for the other CTAs of a case
+};
+
 }  // namespace qlgpu
 
 #define QLGPU_STATUS_NONFINITE 1   // solution::Check_Solution NaN/Inf (solution.cpp:194)
 #define QLGPU_STATUS_UNSTABLE 2    // |mean field| > 1e20 (solution.cpp:184)
 #define QLGPU_STATUS_DIAG_FULL 4   // diagnostic ring overflowed (records dropped)
+#define QLGPU_STATUS_TIMEOUT 8     // batch: a CTA gave up waiting for the other CTAs of its case

@@ -1,0 +1,188 @@
+"""Batched ensemble (one persistent cooperative launch for many cases) against
+the CPU oracle, case by case, through the C ABI (qlgpu_batch_*).
+
+Tolerance: relative L2 error <= 1e-10 for every case's state after N steps and
+for its energy / stress / dissipation series, as for the single-case step.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import rel, require_gpu
+from oracle import oracle as O
+from ql_dns_b200.batch import QLBatch, mri_ensemble
+from ql_dns_b200.initial import initial_state
+from ql_dns_b200.params import QLParams
+from ql_dns_b200.solver import QLSolver
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def series_rel(dg, do):
+    errs = []
+    for c in range(1, 13):
+        scale = np.abs(do[:, c]).max()
+        if scale > 0:
+            errs.append(np.abs(dg[:, c] - do[:, c]).max() / scale)
+    return max(errs)
+
+
+def mixed_cases(model=0, integ=0):
+    """Uneven mode counts, every NZ, different nu / eta / mean fields."""
+    specs = [(8, 6, 16, 1 / 700), (16, 16, 32, 1 / 2000), (8, 8, 64, 1 / 3000), (12, 10, 32, 1 / 1500),
+             (6, 8, 128, 1 / 5000), (10, 4, 256, 1 / 9000), (20, 20, 64, 1 / 4000)]
+    cases = []
+    for i, (nx, ny, NZ, eta) in enumerate(specs):
+        cases.append(QLParams(model=model, integrator=integ, nx=nx, ny=ny, NZ=NZ, nu=eta * (1 + i % 3), eta=eta,
+                              dt=0.01, B0z=0.02 if model else 0.0, omega=0.9))
+    return cases
+
+
+def states(cases, sigma=0.2):
+    out = []
+    for i, p in enumerate(cases):
+        out.append(initial_state(p, 100 + i, sigma=sigma, B0=0.03 + 0.01 * i, mean_u=0.01 if p.model else 0.0))
+    return out
+
+
+def run_batch(cases, sts, n, diag_every=1, mapping=None, tune=0):
+    require_gpu()
+    res = []
+    with QLBatch(cases) as b:
+        if mapping is not None:
+            b.set_mapping(*mapping)
+        for c, (lin, mf, kx0) in enumerate(sts):
+            b.set_state(c, 0.0, lin, mf, kx0)
+        if tune:
+            b.tune(tune)
+        d0 = [b.diagnostics(c) for c in range(len(cases))]
+        d = b.step(n, diag_every=diag_every)
+        for c in range(len(cases)):
+            t, lo, mo, ko = b.get_state(c)
+            res.append((t, lo, mo, ko, np.vstack([d0[c][None], d[c]]) if diag_every else None))
+        st, ls = b.status()
+        assert ls == 0 and all(s == 0 for s in st)
+        m = b.mapping()
+    return res, m
+
+
+@pytest.mark.parametrize("model", [0, 1])
+@pytest.mark.parametrize("integ", [0, 1])
+def test_batch_matches_oracle(model, integ):
+    cases = mixed_cases(model, integ)
+    sts = states(cases)
+    n = 30
+    res, m = run_batch(cases, sts, n)
+    for p, (lin, mf, kx0), (t, lo, mo, ko, d) in zip(cases, sts, res):
+        t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, n, diag_every=1)
+        assert t == t2 and np.array_equal(ko, ko2)
+        assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL, (p, rel(lo, lo2), rel(mo, mo2))
+        assert d.shape == d2.shape and series_rel(d, d2) < TOL
+
+
+def test_batch_equals_single_case_path_bitwise():
+    # With the same CTA count and width as the single-case handle, a case's sums
+    # run in the same order: the batch reproduces the single-case step exactly.
+    cases = mixed_cases()[:4]
+    sts = states(cases)
+    ref = []
+    ncta = []
+    for p, (lin, mf, kx0) in zip(cases, sts):
+        with QLSolver(p) as s:
+            info = s.launch_info()
+            assert info["warps"] == 8
+            ncta.append(info["grid"])
+            s.set_state(0.0, lin, mf, kx0)
+            s.step(12)
+            ref.append(s.get_state())
+    res, m = run_batch(cases, sts, 12, diag_every=0, mapping=(8, ncta))
+    assert m["ncta"] == ncta
+    for (t, lo, mo, ko, _), (t2, lo2, mo2, ko2) in zip(res, ref):
+        assert t == t2
+        assert np.array_equal(lo, lo2) and np.array_equal(mo, mo2) and np.array_equal(ko, ko2)
+
+
+def test_batch_mapping_and_width_independent():
+    # different CTA counts / widths / packing change only the order of sums over CTAs
+    cases = mixed_cases()
+    sts = states(cases)
+    a, _ = run_batch(cases, sts, 20, diag_every=0, mapping=(8, [1] * len(cases)))
+    b, mb = run_batch(cases, sts, 20, diag_every=0, mapping=(4, [2, 3, 2, 4, 1, 2, 5]))
+    assert mb["warps"] == 4
+    for x, y in zip(a, b):
+        assert rel(x[1], y[1]) < 1e-12 and rel(x[2], y[2]) < 1e-12
+
+
+def test_batch_tune_keeps_state_and_parity():
+    cases = mixed_cases()
+    sts = states(cases)
+    require_gpu()
+    with QLBatch(cases) as b:
+        for c, (lin, mf, kx0) in enumerate(sts):
+            b.set_state(c, 0.0, lin, mf, kx0)
+        ms = b.tune(2)
+        assert ms > 0
+        for c, (lin, mf, kx0) in enumerate(sts):
+            t, lo, mo, ko = b.get_state(c)
+            assert t == 0.0 and np.array_equal(lo, lin) and np.array_equal(mo, mf) and np.array_equal(ko, kx0)
+        b.step(7)
+        b.step(6)  # two launches: the lin buffer parity carries over
+        for p, (lin, mf, kx0), c in zip(cases, sts, range(len(cases))):
+            t, lo, mo, ko = b.get_state(c)
+            t2, lo2, mo2, ko2, _ = O.run(p, 0.0, lin, mf, kx0, 13)
+            assert abs(t - t2) < 1e-15 and rel(lo, lo2) < TOL and rel(mo, mo2) < TOL
+
+
+def test_batch_without_graph(monkeypatch):
+    monkeypatch.setenv("QLGPU_BATCH_GRAPH", "0")
+    cases = mixed_cases()[:3]
+    sts = states(cases)
+    res, _ = run_batch(cases, sts, 9)
+    for p, (lin, mf, kx0), (t, lo, mo, ko, d) in zip(cases, sts, res):
+        t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, 9, diag_every=1)
+        assert rel(lo, lo2) < TOL and series_rel(d, d2) < TOL
+
+
+def test_batch_ensemble_law_short():
+    # the 48-case MRI ensemble (mode grids 16..64 squared, NZ 32..128) for a few steps
+    cases, b0s, seeds = mri_ensemble()
+    sts = [initial_state(p, s, sigma=1e-3, B0=b0) for p, b0, s in zip(cases, b0s, seeds)]
+    res, m = run_batch(cases, sts, 3, diag_every=1, tune=2)
+    assert 1 <= m["grid"] <= 2 * 148
+    for c in (0, 17, 47):
+        p = cases[c]
+        lin, mf, kx0 = sts[c]
+        t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, 3, diag_every=1)
+        assert rel(res[c][1], lo2) < TOL and rel(res[c][2], mo2) < TOL
+        assert series_rel(res[c][4], d2) < TOL
+
+
+def test_batch_wait_bound_reports_timeout():
+    # A case loses one of its work items, so its other CTAs wait for a stage that
+    # never completes: the bounded wait ends the launch with a status, and the
+    # batch is usable again after a new mapping and state.
+    from ql_dns_b200._capi import QLGPUError
+    cases = mixed_cases()[:3]
+    sts = states(cases)
+    require_gpu()
+    with QLBatch(cases) as b:
+        b.set_mapping(8, [2, 2, 1])
+        for c, (lin, mf, kx0) in enumerate(sts):
+            b.set_state(c, 0.0, lin, mf, kx0)
+        b.set_wait(0.2)
+        b.debug_drop_item(0)
+        with pytest.raises(QLGPUError) as ei:
+            b.step(2)
+        assert ei.value.code == 4 and "waiting" in str(ei.value)
+        st, ls = b.status()
+        assert ls & 8
+        b.set_mapping(8, [2, 2, 1])
+        for c, (lin, mf, kx0) in enumerate(sts):
+            b.set_state(c, 0.0, lin, mf, kx0)
+        b.step(4)
+        st, ls = b.status()
+        assert ls == 0
+        for p, (lin, mf, kx0), c in zip(cases, sts, range(3)):
+            t, lo, mo, ko = b.get_state(c)
+            t2, lo2, mo2, ko2, _ = O.run(p, 0.0, lin, mf, kx0, 4)
+            assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL
