@@ -2,25 +2,32 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (one "step" = one full RK3 step, three fused stage kernels, of every
-(kx,ky) mode): QL MRI plain FP64 at production size, MHD_BQlin with
-RK3CN_Elin, 64x64 (kx,ky) modes (2016 mode columns) x NZ=128 (85 dealiased kz),
-Lx=1, Ly=pi, Lz=1, q=1.5, Re=Rm=8000, dt=0.005, seeded initial condition
-(seed 1, sigma=1e-3 |k|^-2, By = 0.05 sin(2 pi z)).  The data are synthetic
-(the reference ships no data sets).
+Headline workload: the batched QL MRI ensemble.  48 independent MHD_BQlin
+cases stepped with RK3CN_Elin at dt = 0.01, drawn with numpy seed 12345: per
+case a square (kx,ky) mode grid from {16, 32, 48, 64}^2, NZ from {32, 64,
+128}, Rm log-uniform in [500, 16000], Pm from {1, 2, 4} (eta = 1/Rm,
+nu = Pm/Rm) and a mean-field amplitude B0 uniform in [0.01, 0.1]; case c
+starts from the seeded initial condition with seed c (sigma = 1e-3 |k|^-2,
+By = B0 sin(2 pi z)).  The data are synthetic (the reference ships no data
+sets).  One "step" = one full RK3 step of every mode of every case.  All 48
+cases run in ONE persistent cooperative launch per call (K steps), with the
+CTA mapping chosen by the autotuner before the warm-up.
 
 Metric: mode-steps/s = (mode columns advanced by one full step) / second,
-whole job over all ranks.  N > 1 runs independent replicas of the workload,
-one per GPU (the step has no cross-GPU exchange at this size), so scaling is
-weak.  The timed region is bracketed by a barrier and device synchronisation;
-the time per rank is the sum of CUDA-event durations on the solver's stream,
-and the job time is the max over ranks.  L2 is flushed (a 512 MiB write)
-before every timed step because the 2016-mode working set (~45 MB) would
-otherwise stay resident in the 126 MB L2.
+whole job over all ranks.  The same ensemble run case after case through the
+plain single-case path is reported beside it ("plain_per_case"), and so is
+the single-case production workload (64x64 modes x NZ=128, Re=Rm=8000,
+dt=0.005, seed 1; "single_case").  N > 1 runs independent replicas of the
+ensemble, one per GPU (rank r uses initial-condition seeds 48 r + c), so
+scaling is weak.  The timed region is bracketed by a barrier and device
+synchronisation and timed with CUDA events on the batch's stream; the job
+time is the max over ranks.  The ensemble's state (about 0.5 GB with its RK
+buffers) is larger than the 126 MB L2, so no flush is needed between steps;
+the single-case workload (45 MB) is timed with an L2 flush before every step.
 
 --impl reference times the CPU restatement of the reference's step (the
 oracle, OpenMP over modes, -O3 -ffast-math -march=native like the reference's
-SConstruct) on the host cores on a bounded sample of the same workload.
+SConstruct) on the host cores on a bounded sample of the same ensemble.
 """
 from __future__ import annotations
 
@@ -40,14 +47,30 @@ sys.path.insert(0, ROOT)
 
 METRIC = "mode-steps/s on 1 B200, batched vs plain per-case, rel err ≤1e-10 vs FP64 CPU"
 UNIT = "mode-steps/s"
-WORKLOAD = ("QL MRI plain FP64 MHD_BQlin + RK3CN_Elin, 64x64 (kx,ky) modes (2016 columns) x NZ=128 "
-            "(nz=85), Re=Rm=8000, dt=0.005, seed 1")
+WORKLOAD = ("batched QL MRI ensemble: 48 MHD_BQlin cases (RK3CN_Elin, dt=0.01), mode grids {16,32,48,64}^2, "
+            "NZ {32,64,128}, Rm log-uniform [500,16000], Pm {1,2,4}, B0 U[0.01,0.1], draw seed 12345, "
+            "IC seeds 0..47, one persistent launch")
+SINGLE_WORKLOAD = ("QL MRI plain FP64 MHD_BQlin + RK3CN_Elin, 64x64 (kx,ky) modes (2016 columns) x NZ=128 "
+                   "(nz=85), Re=Rm=8000, dt=0.005, seed 1")
+NCASES = 48
 FALLBACK_HBM_GBS = 6650.0
 
 
-def workload_params():
-    from ql_dns_b200.params import config1
-    return config1()
+def single_params():
+    from ql_dns_b200.params import mri_64x64_nz128
+    return mri_64x64_nz128()
+
+
+def ensemble(rank: int = 0):
+    """Cases, mean-field amplitudes and initial-condition seeds of one replica."""
+    from ql_dns_b200.batch import mri_ensemble
+    cases, b0s, seeds = mri_ensemble(NCASES)
+    return cases, b0s, [NCASES * rank + s for s in seeds]
+
+
+def ensemble_states(cases, b0s, seeds):
+    from ql_dns_b200.initial import initial_state
+    return [initial_state(p, s, sigma=1e-3, B0=b0) for p, b0, s in zip(cases, b0s, seeds)]
 
 
 def algorithmic_bytes_per_step(p) -> float:
@@ -70,12 +93,12 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def read_traffic():
-    """DRAM bytes per stage-kernel launch from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "stage_kernel_cfg1.md")
+def read_traffic(name: str):
+    """DRAM bytes per launch (per step for the batch kernel) from a committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith("traffic_bytes_per_launch:") or line.startswith("traffic_bytes_per_step:"):
                 return float(line.split(":")[1].split()[0])
     except Exception:
         pass
@@ -167,69 +190,76 @@ def max_over_ranks(ws, x: float) -> float:
     return float(t.item())
 
 
-def replica_plan(ws: int, rank: int, p):
-    """Weak scaling: every rank advances its own replica of the workload (no
-    data-path collective); returns (seed, mode columns of this rank, job total)."""
-    return 1 + rank, p.nxy, p.nxy * ws
+def replica_plan(ws: int, rank: int, modes: int):
+    """Weak scaling: every rank advances its own replica of the ensemble (no
+    data-path collective); returns (first initial-condition seed of this rank,
+    mode columns of this rank, job total)."""
+    return NCASES * rank, modes, modes * ws
 
 
 # ---------------------------------------------------------------------------
 # CPU reference arm: the oracle restatement of the reference step
 # ---------------------------------------------------------------------------
-def cpu_oracle_time(p, steps: int, threads: int):
-    """Time `steps` RK3 steps of the workload on the host with the fast oracle."""
+def _oracle_kind():
     from oracle import oracle as O
-    from ql_dns_b200.initial import initial_state
-    kind = "native"
     try:
         O.build(native=True)
+        return "native"
     except Exception:
-        kind = "fast"
-    lin, mf, kx0 = initial_state(p, 1, sigma=1e-3)
-    O.run(p, 0.0, lin, mf, kx0, 1, kind=kind, nthreads=threads)  # warm-up (page-in, OpenMP pool)
+        return "fast"
+
+
+def cpu_ensemble_time(cases, sts, steps: int, threads: int, kind: str):
+    """`steps` RK3 steps of every case of the ensemble with the oracle; (mode-steps/s, seconds)."""
+    from oracle import oracle as O
     t0 = time.perf_counter()
-    O.run(p, 0.0, lin, mf, kx0, steps, kind=kind, nthreads=threads)
+    for p, (lin, mf, kx0) in zip(cases, sts):
+        O.run(p, 0.0, lin, mf, kx0, steps, kind=kind, nthreads=threads)
     dt = time.perf_counter() - t0
-    return p.nxy * steps / dt, dt, kind
+    return sum(p.nxy for p in cases) * steps / dt, dt
 
 
-def cpu_baseline(p, budget_s: float = 15.0, threads: int | None = None):
+def cpu_baseline(budget_s: float = 15.0, threads: int | None = None):
     threads = threads or os.cpu_count() or 1
-    # size the sample: one timed step first, then as many as fit the budget
-    rate1, dt1, kind = cpu_oracle_time(p, 1, threads)
+    cases, b0s, seeds = ensemble(0)
+    sts = ensemble_states(cases, b0s, seeds)
+    kind = _oracle_kind()
+    cpu_ensemble_time(cases, sts, 1, threads, kind)  # warm-up (page-in, OpenMP pool)
+    r1, dt1 = cpu_ensemble_time(cases, sts, 1, threads, kind)
     steps = max(1, min(200, int(budget_s / max(dt1, 1e-6))))
-    rate, dt, kind = cpu_oracle_time(p, steps, threads)
+    rate, dt = cpu_ensemble_time(cases, sts, steps, threads, kind)
     return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{steps} RK3 steps of the full 2016-mode x NZ=128 workload ({dt:.1f} s), "
-                      f"oracle build '{kind}', OpenMP over modes"}
+            "sample": f"{steps} RK3 steps of all 48 ensemble cases ({dt:.1f} s), oracle build '{kind}', "
+                      f"OpenMP over modes"}
 
 
 def run_reference(args):
-    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    ws, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    p = workload_params()
     threads = os.cpu_count() or 1
-    vals = []
-    # each "step" of this arm is a bounded sample (a few RK3 steps on all cores),
-    # sized so the whole run stays near 60 s of CPU work
-    rate1, dt1, kind = cpu_oracle_time(p, 1, threads)
+    cases, b0s, seeds = ensemble(0)
+    sts = ensemble_states(cases, b0s, seeds)
+    kind = _oracle_kind()
+    # each "step" of this arm is a bounded sample (RK3 steps of all cases on all
+    # cores), sized so the whole run stays near 60 s of CPU work
+    r1, dt1 = cpu_ensemble_time(cases, sts, 1, threads, kind)
     per = max(1, min(50, int(60.0 / (max(args.steps, 1) * max(dt1, 1e-6)))))
     for _ in range(args.warmup):
-        cpu_oracle_time(p, 1, threads)
+        cpu_ensemble_time(cases, sts, 1, threads, kind)
     total_t = 0.0
     for _ in range(args.steps):
-        r, dt, kind = cpu_oracle_time(p, per, threads)
-        vals.append(r)
+        r, dt = cpu_ensemble_time(cases, sts, per, threads, kind)
         total_t += dt
-    value = p.nxy * per * args.steps / total_t
+    modes = sum(p.nxy for p in cases)
+    value = modes * per * args.steps / total_t
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_t / (args.steps * per),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "parallelism": "host cores (OpenMP over modes)"},
+        "config": {"workload": WORKLOAD, "parallelism": "host cores (OpenMP over modes)", "mode_columns": modes},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{per} RK3 steps per timed step, oracle build '{kind}'"},
+                         "sample": f"{per} RK3 steps of all 48 cases per timed step, oracle build '{kind}'"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -239,82 +269,128 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def run_single(args, ext_stream_of, local):
+    """The single-case production workload through the plain path (L2 flushed before each step)."""
+    import torch
+    from ql_dns_b200.initial import initial_state
+    from ql_dns_b200.solver import QLSolver
+    p = single_params()
+    lin, mf, kx0 = initial_state(p, 1, sigma=1e-3)
+    steps = max(1, min(args.steps, 500))
+    with QLSolver(p, device=local) as solver:
+        solver.set_state(0.0, lin, mf, kx0)
+        ext = ext_stream_of(solver.stream())
+        flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        for _ in range(args.warmup):
+            solver.step_timed()
+        stage_ms = np.zeros(3)
+        for _ in range(steps):
+            with torch.cuda.stream(ext):
+                flush.fill_(1.0)
+            stage_ms += solver.step_timed()
+        del flush
+    peak, _ = hbm_peak()
+    sb = stage_bytes(p)
+    achieved = sum(sb) * steps / (stage_ms.sum() / 1e3) / 1e9
+    return {"workload": SINGLE_WORKLOAD, "value": p.nxy * steps / (stage_ms.sum() / 1e3), "unit": UNIT,
+            "steps": steps, "ms_per_step": float(stage_ms.sum() / steps),
+            "l2": "flushed (512 MiB write) before every timed step",
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "kernel": "stage_kernel<128,MHD_BQlin,RK3CN_Elin>",
+                         "traffic": read_traffic("stage_kernel_mri_64x64_nz128.md"),
+                         "algorithmic_bytes_per_launch": sum(sb) / 3,
+                         "avg_launch_ms": float(stage_ms.sum() / (3 * steps))}}
+
+
+def run_plain_per_case(cases, sts, local, steps_per_case: int = 10):
+    """The ensemble case after case through the plain single-case path (device time)."""
+    from ql_dns_b200.solver import QLSolver
+    tot = 0.0
+    for p, (lin, mf, kx0) in zip(cases, sts):
+        with QLSolver(p, device=local) as s:
+            s.set_state(0.0, lin, mf, kx0)
+            for _ in range(3):
+                s.step_timed()
+            t = 0.0
+            for _ in range(steps_per_case):
+                t += float(s.step_timed().sum())
+            tot += t / steps_per_case
+    modes = sum(p.nxy for p in cases)
+    return {"value": modes / (tot / 1e3), "unit": UNIT, "ms_per_step": tot,
+            "sample": f"{steps_per_case} steps of each case, one case after another, 3 stage launches per step"}
+
+
 def run_gpu(args):
     import torch
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    from ql_dns_b200.initial import initial_state
-    from ql_dns_b200.solver import QLSolver
-    p = workload_params()
-    seed, my_modes, job_modes = replica_plan(ws, rank, p)
-    lin, mf, kx0 = initial_state(p, seed, sigma=1e-3)
-    solver = QLSolver(p, device=local)
-    solver.set_state(0.0, lin, mf, kx0)
-    ext = torch.cuda.ExternalStream(solver.stream())
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-
-    def flush_l2():
-        with torch.cuda.stream(ext):
-            flush.fill_(1.0)
-
-    for _ in range(args.warmup):
-        solver.step_timed()
+    from ql_dns_b200.batch import QLBatch
+    cases, b0s, _ = ensemble(0)
+    modes = sum(p.nxy for p in cases)
+    seed0, my_modes, job_modes = replica_plan(ws, rank, modes)
+    seeds = [seed0 + c for c in range(NCASES)]
+    sts = ensemble_states(cases, b0s, seeds)
+    batch = QLBatch(cases, device=local)
+    for c, (lin, mf, kx0) in enumerate(sts):
+        batch.set_state(c, 0.0, lin, mf, kx0)
+    tune_ms = batch.tune(3)
+    batch.step_timed(args.warmup)
     torch.cuda.synchronize()
     barrier(ws)
     torch.cuda.synchronize()
-    stage_ms = np.zeros(3)
-    step_ms = []
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush_l2()
-            with torch.cuda.stream(ext):
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(ext)
-            st = solver.step_timed()  # synchronises on its last event
-            e1.record(ext)
-            e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
-            stage_ms += st
+        ms = batch.step_timed(args.steps)  # one persistent launch of K steps, CUDA events on the batch stream
     torch.cuda.synchronize()
     barrier(ws)
     torch.cuda.synchronize()
-    my_total_ms = float(sum(step_ms))
-    job_ms = max_over_ranks(ws, my_total_ms)
+    job_ms = max_over_ranks(ws, ms)
     value = job_modes * args.steps / (job_ms / 1e3)
-    launches = 3 * args.steps
+    st, ls = batch.status()
+    assert ls == 0 and not any(st), (st, ls)
+    mapping = batch.mapping()
 
-    # roofline of the stage kernel: algorithmic bytes / event-timed duration
     peak, peak_kind = hbm_peak()
-    sb = stage_bytes(p)
-    achieved = sum(sb) * args.steps / (stage_ms.sum() / 1e3) / 1e9
-    traffic = read_traffic()
+    alg_step = sum(algorithmic_bytes_per_step(p) for p in cases)
+    achieved = alg_step * args.steps / (ms / 1e3) / 1e9
 
-    # end to end through the C ABI with pinned host buffers: set_state (H2D),
-    # K steps with a diagnostic record per step (D2H of the step's metrics),
-    # get_state (D2H)
-    lin_h = torch.empty(lin.shape, dtype=torch.complex128, pin_memory=True).numpy()
-    mf_h = torch.empty(mf.shape, dtype=torch.complex128, pin_memory=True).numpy()
-    lin_h[...] = lin
-    mf_h[...] = mf
+    # end to end through the batch C ABI: H2D of every case's state from pinned
+    # host memory, then per step one call that advances all cases and reads the
+    # 48 diagnostic records (energy / stress / dissipation) back to the host,
+    # then D2H of every case's state
+    pinned = []
+    for lin, mf, kx0 in sts:
+        lh = torch.empty(lin.shape, dtype=torch.complex128, pin_memory=True).numpy()
+        mh = torch.empty(mf.shape, dtype=torch.complex128, pin_memory=True).numpy()
+        lh[...] = lin
+        mh[...] = mf
+        pinned.append((lh, mh, kx0))
+    ext = torch.cuda.ExternalStream(batch.stream())
     torch.cuda.synchronize()
     barrier(ws)
-    flush_l2()
-    torch.cuda.synchronize()
     ee0 = torch.cuda.Event(enable_timing=True)
     ee1 = torch.cuda.Event(enable_timing=True)
     ee0.record(ext)
-    solver.set_state(0.0, lin_h, mf_h, kx0)
-    solver.step(args.steps, diag_every=1)
-    t_out, lo, mo, ko = solver.get_state()
+    for c, (lh, mh, kx0) in enumerate(pinned):
+        batch.set_state(c, 0.0, lh, mh, kx0)
+    ndiag = 0
+    for _ in range(args.steps):
+        recs = batch.step(1, diag_every=1)
+        ndiag += sum(len(r) for r in recs)
+    outs = [batch.get_state(c) for c in range(NCASES)]
     ee1.record(ext)
     ee1.synchronize()
     e2e_ms = max_over_ranks(ws, ee0.elapsed_time(ee1))
-    state_bytes = lin.nbytes + mf.nbytes + kx0.nbytes
+    assert ndiag == NCASES * args.steps
+    assert all(np.isfinite(o[1]).all() and np.isfinite(o[2]).all() for o in outs)
+    state_bytes = sum(lin.nbytes + mf.nbytes + kx0.nbytes for lin, mf, kx0 in sts)
     e2e = {"value": job_modes * args.steps / (e2e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": state_bytes / args.steps,
-           "d2h_bytes_per_step": 15 * 8 + state_bytes / args.steps}
-    assert np.isfinite(lo).all() and np.isfinite(mo).all()
+           "d2h_bytes_per_step": NCASES * 15 * 8 + state_bytes / args.steps,
+           "path": "QLBatch.set_state (pinned) x48, K x QLBatch.step(1, diag_every=1), QLBatch.get_state x48"}
+    batch.close()
+
+    plain = run_plain_per_case(cases, sts, local) if rank == 0 else None
+    single = run_single(args, torch.cuda.ExternalStream, local) if rank == 0 else None
 
     out = None
     if rank == 0:
@@ -323,25 +399,27 @@ def run_gpu(args):
             "warmup": args.warmup, "ms_per_step": job_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "flushed (512 MiB write) before every timed step",
-                       "mode_columns": p.nxy, "NZ": p.NZ, "nz": p.nz},
+                       "l2": "not flushed: the ensemble state (~0.5 GB with RK buffers) exceeds the 126 MB L2",
+                       "cases": NCASES, "mode_columns": modes, "mapping": mapping, "tune_probe_ms": tune_ms},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "stage_kernel<128,MHD_BQlin,RK3CN_Elin>",
-                         "algorithmic_bytes_per_launch": sum(sb) / 3,
-                         "avg_launch_ms": float(stage_ms.sum() / launches)},
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": read_traffic("batch_kernel_mri_ensemble48.md"),
+                         "kernel": "batch_kernel<MHD_BQlin,RK3CN_Elin> (one launch of K steps)",
+                         "algorithmic_bytes_per_step": alg_step, "avg_launch_ms": ms},
+            "plain_per_case": plain,
+            "speedup_vs_plain_per_case": value / plain["value"],
+            "single_case": single,
             "e2e": e2e,
-            "gpu_launches": launches,
+            "gpu_launches": 2,
         }
         out["clocks"] = clk.summary()
-    solver.close()
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         if not args.no_cpu_baseline and ws == 1:
-            out["cpu_baseline"] = cpu_baseline(p, budget_s=args.cpu_budget)
+            out["cpu_baseline"] = cpu_baseline(budget_s=args.cpu_budget)
         print(json.dumps(out), flush=True)
     return 0
 
@@ -349,7 +427,7 @@ def run_gpu(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

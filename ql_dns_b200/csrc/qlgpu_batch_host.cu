@@ -104,12 +104,18 @@ __global__ void batch_reset_kernel(const BatchCase* cases, int ncases, unsigned*
     }
 }
 
-// Gathers every case's status word and diagnostic record count.
-__global__ void batch_collect_kernel(const BatchCase* cases, int ncases, int* out /* [ncases][2] */) {
+// Gathers every case's status word and diagnostic record count, then the
+// launch status and the case of a wait that gave up.
+__global__ void batch_collect_kernel(const BatchCase* cases, int ncases, const BatchCtl* ctl,
+                                     int* out /* [ncases][2], status, fail_case */) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncases; c += gridDim.x * blockDim.x) {
         const DevClock* clk = cases[c].A[0].clk;
         out[2 * c] = clk->status;
         out[2 * c + 1] = clk->ndiag;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        out[2 * ncases] = ctl->status;
+        out[2 * ncases + 1] = ctl->fail_case;
     }
 }
 
@@ -128,6 +134,8 @@ struct qlgpu_batch {
     unsigned long long* d_case_end = nullptr;
     int* d_collect = nullptr;
     double* d_out15 = nullptr;
+    double* d_diag = nullptr;  // [ncases][diag_cap][15] diagnostic records of every case
+    int diag_cap = 0;
     BatchKernel bk;
     int sms = 0;
     size_t smem_optin = 0;
@@ -473,9 +481,8 @@ int qlgpu_batch_destroy(qlgpu_batch_t* b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
-    for (CaseHost& c : b->cs)
-        if (c.diag) cudaFree(c.diag);
-    void* bufs[] = {b->arena, b->d_cases, b->d_ctas, b->d_epoch, b->d_ctl, b->d_case_end, b->d_collect, b->d_out15};
+    void* bufs[] = {b->arena,     b->d_cases,   b->d_ctas,  b->d_epoch, b->d_ctl,
+                    b->d_case_end, b->d_collect, b->d_out15, b->d_diag};
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : b->ev)
@@ -640,7 +647,7 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
     QB_ALLOC(b->d_epoch, sizeof(unsigned) * BATCH_EPOCH_STRIDE * (size_t)ncases);
     QB_ALLOC(b->d_ctl, sizeof(BatchCtl));
     QB_ALLOC(b->d_case_end, sizeof(unsigned long long) * ncases);
-    QB_ALLOC(b->d_collect, sizeof(int) * 2 * ncases);
+    QB_ALLOC(b->d_collect, sizeof(int) * (2 * ncases + 2));
     QB_ALLOC(b->d_out15, sizeof(double) * 15);
 #undef QB_ALLOC
     if (cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess) {
@@ -722,40 +729,41 @@ int qlgpu_batch_step(qlgpu_batch_t* b, int nsteps, int diag_every, double* diag_
     if (diag_every > 0 && (!diag_out || !ndiag || max_diag < 1))
         return bfail(b, QLGPU_ERR_ARG, "diag_out, ndiag and max_diag >= 1 required");
     QB_CK(cudaSetDevice(b->device));
+    if (diag_every > 0 && b->diag_cap != max_diag) {
+        // one block for every case's records, laid out as diag_out: [case][max_diag][15]
+        if (b->d_diag) cudaFree(b->d_diag);
+        b->d_diag = nullptr;
+        b->diag_cap = 0;
+        QB_CK(cudaMalloc(&b->d_diag, sizeof(double) * 15 * (size_t)max_diag * b->ncases));
+        b->diag_cap = max_diag;
+        for (int c = 0; c < b->ncases; ++c) {
+            b->cs[c].diag = b->d_diag + (size_t)c * max_diag * 15;
+            b->cs[c].diag_cap = max_diag;
+        }
+        b->descr_dirty = true;
+    }
     for (int c = 0; c < b->ncases; ++c) {
-        CaseHost& h = b->cs[c];
-        const double tv = diag_every > 0 ? diag_every * h.p.dt : 0.0;
+        const double tv = diag_every > 0 ? diag_every * b->cs[c].p.dt : 0.0;
         if (tv != b->tv_set[c]) {
             b->tv_set[c] = tv;
-            b->descr_dirty = true;
-        }
-        if (diag_every > 0 && h.diag_cap < max_diag) {
-            if (h.diag) cudaFree(h.diag);
-            h.diag = nullptr;
-            h.diag_cap = 0;
-            QB_CK(cudaMalloc(&h.diag, sizeof(double) * 15 * (size_t)max_diag));
-            h.diag_cap = max_diag;
             b->descr_dirty = true;
         }
     }
     int rc = run_launch(b, nsteps, diag_every > 0 ? 1 : 0);
     if (rc) return rc;
-    rc = check_launch_status(b);
-    if (rc) return rc;
-    std::vector<int> col(2 * (size_t)b->ncases);
-    batch_collect_kernel<<<(b->ncases + 127) / 128, 128, 0, b->stream>>>(b->d_cases, b->ncases, b->d_collect);
+    const int nc = b->ncases;
+    std::vector<int> col(2 * (size_t)nc + 2);
+    batch_collect_kernel<<<(nc + 127) / 128, 128, 0, b->stream>>>(b->d_cases, nc, b->d_ctl, b->d_collect);
     QB_CK(cudaGetLastError());
     QB_CK(cudaMemcpyAsync(col.data(), b->d_collect, col.size() * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    if (diag_every > 0)
+        QB_CK(cudaMemcpyAsync(diag_out, b->d_diag, sizeof(double) * 15 * (size_t)max_diag * nc,
+                              cudaMemcpyDeviceToHost, b->stream));
     QB_CK(cudaStreamSynchronize(b->stream));
+    if (col[2 * nc] & QLGPU_STATUS_TIMEOUT) return check_launch_status(b);
     int bad = -1;
-    for (int c = 0; c < b->ncases; ++c) {
-        if (diag_every > 0) {
-            const int n = std::min(col[2 * c + 1], max_diag);
-            ndiag[c] = n;
-            if (n > 0)
-                QB_CK(cudaMemcpy(diag_out + (size_t)c * max_diag * 15, b->cs[c].diag, sizeof(double) * 15 * (size_t)n,
-                                 cudaMemcpyDeviceToHost));
-        }
+    for (int c = 0; c < nc; ++c) {
+        if (diag_every > 0) ndiag[c] = std::min(col[2 * c + 1], max_diag);
         if (bad < 0 && (col[2 * c] & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE | QLGPU_STATUS_DIAG_FULL)))
             bad = c;
     }
@@ -981,8 +989,9 @@ int qlgpu_batch_status(qlgpu_batch_t* b, int* case_status, int* launch_status) {
     if (!b) return QLGPU_ERR_ARG;
     QB_CK(cudaSetDevice(b->device));
     if (case_status) {
-        std::vector<int> col(2 * (size_t)b->ncases);
-        batch_collect_kernel<<<(b->ncases + 127) / 128, 128, 0, b->stream>>>(b->d_cases, b->ncases, b->d_collect);
+        std::vector<int> col(2 * (size_t)b->ncases + 2);
+        batch_collect_kernel<<<(b->ncases + 127) / 128, 128, 0, b->stream>>>(b->d_cases, b->ncases, b->d_ctl,
+                                                                              b->d_collect);
         QB_CK(cudaGetLastError());
         QB_CK(cudaMemcpyAsync(col.data(), b->d_collect, col.size() * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
         QB_CK(cudaStreamSynchronize(b->stream));

@@ -56,19 +56,19 @@ class QLParams:
         return dataclasses.replace(self, **kw)
 
 
-def config0(**kw) -> QLParams:
+def mri_16x16_nz32(**kw) -> QLParams:
     """QL MRI 16x16 modes x NZ=32, Re=Rm=2000, dt=0.01 (500 steps)."""
     p = QLParams(nx=16, ny=16, NZ=32, nu=1 / 2000, eta=1 / 2000, dt=0.01)
     return p.replace(**kw)
 
 
-def config1(**kw) -> QLParams:
+def mri_64x64_nz128(**kw) -> QLParams:
     """QL MRI production size: 64x64 modes x NZ=128, Re=Rm=8000, dt=0.005 (2000 steps)."""
     p = QLParams(nx=64, ny=64, NZ=128, nu=1 / 8000, eta=1 / 8000, dt=0.005)
     return p.replace(**kw)
 
 
-def config_adjoint(**kw) -> QLParams:
+def adjoint_32x32_nz64(**kw) -> QLParams:
     """Adjoint case: 32x32 modes x NZ=64, Re=Rm=4000, dt=0.01."""
     p = QLParams(nx=32, ny=32, NZ=64, nu=1 / 4000, eta=1 / 4000, dt=0.01)
     return p.replace(**kw)

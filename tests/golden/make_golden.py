@@ -19,7 +19,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 from numpy_ref import NumpyQL  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 from ql_dns_b200.initial import initial_state  # noqa: E402
-from ql_dns_b200.params import config0  # noqa: E402
+from ql_dns_b200.params import mri_16x16_nz32  # noqa: E402
 
 CASES = {
     # name: (params kwargs, seed, sigma, mean_u, nsteps)
@@ -29,13 +29,13 @@ CASES = {
     "fullqlin_cn_hyper": (dict(nx=8, ny=8, NZ=16, model=1, integrator=1, B0z=0.01, omega=0.9,
                                viscosity_order=4, nu=1e-5, eta=2e-5), 14, 0.3, 0.03, 20),
     "bqlin_remap": (dict(nx=8, ny=8, NZ=32, dt=0.05), 15, 0.1, 0.0, 30),
-    "config0_sigma0p1": (dict(), 0, 0.1, 0.0, 60),
+    "mri16_sigma0p1": (dict(), 0, 0.1, 0.0, 60),
 }
 
 
 def make(name):
     kw, seed, sigma, mean_u, n = CASES[name]
-    p = config0(**kw)
+    p = mri_16x16_nz32(**kw)
     lin, mf, kx0 = initial_state(p, seed, sigma=sigma, mean_u=mean_u)
     R = NumpyQL(p)
     l1, m1, _ = R.step(0.0, lin, mf, kx0)

@@ -55,10 +55,10 @@ def test_create_without_device_fails_cleanly():
     import torch
     if torch.cuda.is_available():
         pytest.skip("a GPU is present")
-    from ql_dns_b200.params import config0
+    from ql_dns_b200.params import mri_16x16_nz32
     L = _capi.load()
     h = ctypes.c_void_p()
-    cp = _capi.to_c(config0())
+    cp = _capi.to_c(mri_16x16_nz32())
     rc = L.qlgpu_create(ctypes.byref(cp), 0, ctypes.byref(h))
     assert rc == 5 and not h.value
     buf = ctypes.create_string_buffer(256)
@@ -67,9 +67,9 @@ def test_create_without_device_fails_cleanly():
 
 
 def test_invalid_parameters_rejected_before_device():
-    from ql_dns_b200.params import config0
+    from ql_dns_b200.params import mri_16x16_nz32
     L = _capi.load()
     h = ctypes.c_void_p()
     for bad, code in ((dict(NZ=48), 2), (dict(nx=7), 1), (dict(dt=-0.1), 2), (dict(nu=0.0), 1)):
-        cp = _capi.to_c(config0(**bad))
+        cp = _capi.to_c(mri_16x16_nz32(**bad))
         assert L.qlgpu_create(ctypes.byref(cp), 0, ctypes.byref(h)) == code, bad

@@ -11,7 +11,7 @@ from gpu_util import rel, require_gpu
 from oracle import oracle as O
 from ql_dns_b200.build import MAIN, build
 from ql_dns_b200.initial import initial_state
-from ql_dns_b200.params import config0
+from ql_dns_b200.params import mri_16x16_nz32
 
 pytestmark = pytest.mark.gpu
 
@@ -44,7 +44,7 @@ integrator_ = {integ}
 def test_cpp_driver_matches_oracle(tmp_path, integ):
     require_gpu()
     build()
-    p = config0(integrator=integ)
+    p = mri_16x16_nz32(integrator=integ)
     lin, mf, kx0 = initial_state(p, 9, sigma=0.1)
     inp = tmp_path / "case.DSSinput"
     write_input(inp, p, integ, 1)

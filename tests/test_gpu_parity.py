@@ -11,7 +11,7 @@ from gpu_util import rel, require_gpu
 from golden_cases import load, names
 from oracle import oracle as O
 from ql_dns_b200.initial import initial_state
-from ql_dns_b200.params import config0, config1
+from ql_dns_b200.params import mri_16x16_nz32, mri_64x64_nz128
 from ql_dns_b200.solver import QLSolver
 
 pytestmark = pytest.mark.gpu
@@ -56,7 +56,7 @@ def test_golden_fixture(name):
 @pytest.mark.parametrize("integ", [0, 1])
 def test_rhs_matches_oracle(model, integ):
     require_gpu()
-    p = config0(nx=8, ny=8, NZ=32, integrator=integ, model=model, B0z=0.03 if model else 0.0, omega=0.8)
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=32, integrator=integ, model=model, B0z=0.03 if model else 0.0, omega=0.8)
     lin, mf, kx0 = initial_state(p, 21, sigma=0.5, mean_u=0.02)
     with QLSolver(p) as s:
         s.set_state(0.0, lin, mf, kx0)
@@ -70,7 +70,7 @@ def test_rhs_matches_oracle(model, integ):
 @pytest.mark.parametrize("model", [0, 1])
 @pytest.mark.parametrize("NZ", [16, 32, 64, 128, 256])
 def test_each_nz_three_steps(NZ, model):
-    p = config0(nx=8, ny=6, NZ=NZ, model=model, B0z=0.02 if model else 0.0)
+    p = mri_16x16_nz32(nx=8, ny=6, NZ=NZ, model=model, B0z=0.02 if model else 0.0)
     lin, mf, kx0 = initial_state(p, NZ, sigma=0.3, mean_u=0.02)
     _, lo, mo, ko, d = run_gpu(p, lin, mf, kx0, 3)
     _, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, 3, diag_every=1)
@@ -79,9 +79,9 @@ def test_each_nz_three_steps(NZ, model):
 
 
 @pytest.mark.parametrize("integ", [0, 1])
-def test_config0_full_500_steps(integ):
+def test_mri_16x16_500_steps(integ):
     # 16x16 modes x NZ=32, Re=Rm=2000, dt=0.01, 500 steps, diagnostics every step
-    p = config0(integrator=integ)
+    p = mri_16x16_nz32(integrator=integ)
     lin, mf, kx0 = initial_state(p, 0, sigma=1e-3)
     t, lo, mo, ko, d = run_gpu(p, lin, mf, kx0, 500)
     t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, 500, diag_every=1)
@@ -90,9 +90,9 @@ def test_config0_full_500_steps(integ):
     assert series_rel(d, d2) < TOL
 
 
-def test_config0_strong_coupling_500_steps():
+def test_mri_16x16_strong_coupling_500_steps():
     # sigma = 0.1: the quasi-linear feedback changes the mean field by O(1)
-    p = config0()
+    p = mri_16x16_nz32()
     lin, mf, kx0 = initial_state(p, 0, sigma=0.1)
     t, lo, mo, ko, d = run_gpu(p, lin, mf, kx0, 500)
     t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, 500, diag_every=1)
@@ -100,9 +100,9 @@ def test_config0_strong_coupling_500_steps():
     assert series_rel(d, d2) < TOL
 
 
-def test_config1_short():
+def test_mri_64x64_nz128_short():
     # production size 64x64 modes x NZ=128: 10 steps against the oracle
-    p = config1()
+    p = mri_64x64_nz128()
     lin, mf, kx0 = initial_state(p, 1, sigma=1e-3)
     t, lo, mo, ko, d = run_gpu(p, lin, mf, kx0, 10)
     t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, 10, diag_every=1)
@@ -111,7 +111,7 @@ def test_config1_short():
 
 
 def test_deterministic_bitwise():
-    p = config0(nx=16, ny=16, NZ=64)
+    p = mri_16x16_nz32(nx=16, ny=16, NZ=64)
     lin, mf, kx0 = initial_state(p, 4, sigma=0.2)
     a = run_gpu(p, lin, mf, kx0, 20)
     b = run_gpu(p, lin, mf, kx0, 20)
@@ -120,7 +120,7 @@ def test_deterministic_bitwise():
 
 def test_nonfinite_state_reports_status():
     from ql_dns_b200._capi import QLGPUError
-    p = config0(nx=8, ny=8, NZ=32)
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=32)
     lin, mf, kx0 = initial_state(p, 5, sigma=0.3)
     mf[1, 1] = np.nan
     require_gpu()
@@ -141,7 +141,7 @@ def test_nonfinite_state_reports_status():
 @pytest.mark.parametrize("order", [2, 4])
 def test_fullqlin_200_steps(integ, order):
     # MHD_FullQlin with a vertical field, rotation, mean U and (order 4) hyper-dissipation
-    p = config0(model=1, integrator=integ, B0z=0.05, omega=1.0, viscosity_order=order,
+    p = mri_16x16_nz32(model=1, integrator=integ, B0z=0.05, omega=1.0, viscosity_order=order,
                 nu=1e-4 if order == 4 else 1 / 2000, eta=2e-4 if order == 4 else 1 / 2000)
     lin, mf, kx0 = initial_state(p, 3, sigma=0.05, mean_u=0.02)
     t, lo, mo, ko, d = run_gpu(p, lin, mf, kx0, 200)

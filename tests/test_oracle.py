@@ -7,7 +7,7 @@ from oracle import oracle as O
 from numpy_ref import NumpyQL
 from ql_dns_b200.initial import initial_state
 from ql_dns_b200.ktables import ktables
-from ql_dns_b200.params import QLParams, config0
+from ql_dns_b200.params import QLParams, mri_16x16_nz32
 
 
 def rel(a, b):
@@ -27,7 +27,7 @@ def small(model, integ, **kw):
     base = dict(nx=8, ny=8, NZ=16, model=model, integrator=integ,
                 B0z=0.02 if model == 1 else 0.0, omega=1.0)
     base.update(kw)
-    return config0(**base)
+    return mri_16x16_nz32(**base)
 
 
 @pytest.mark.parametrize("model", [0, 1])
@@ -59,7 +59,7 @@ def test_alfven_wave_exact_solution(integ, nu):
     # between second and third.  The oracle reproduces both behaviours.
     B0 = 0.7
     nuv = nu if nu > 0 else 1e-300
-    p = config0(nx=8, ny=8, NZ=16, q=0.0, nu=nuv, eta=nuv, quasilinear=0, remap=0, integrator=integ)
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=16, q=0.0, nu=nuv, eta=nuv, quasilinear=0, remap=0, integrator=integ)
     lin, mf, kx0 = initial_state(p, 5, sigma=1.0)
     mf[:] = 0
     mf[1, 0] = B0 * p.NZ
@@ -98,7 +98,7 @@ def test_channel_mri_growth_rate_fullqlin():
     # Mean fields of MHD_FullQlin with a vertical field B0z and no fluctuations
     # obey the ideal axisymmetric MRI (MHD_FullQlin.cpp:411-417).
     vA = 0.15
-    p = config0(nx=4, ny=4, NZ=16, model=1, B0z=vA, nu=0.0, eta=0.0, dt=0.005, omega=1.0, remap=0)
+    p = mri_16x16_nz32(nx=4, ny=4, NZ=16, model=1, B0z=vA, nu=0.0, eta=0.0, dt=0.005, omega=1.0, remap=0)
     lin = np.zeros((p.nxy, 4, p.nz), complex)
     mf = np.zeros((4, p.nz), complex)
     mf[0, 1] = 1e-6 * p.NZ
@@ -114,7 +114,7 @@ def test_channel_mri_growth_rate_fullqlin():
 def test_remap_zeroes_mode_at_predicted_step():
     # MHD_BQlin.cpp:314-331: a mode is zeroed (and its kx shifted by -(Nx-1)kxL)
     # right after the step at which kx0 + q t ky first exceeds (Nx-1)/2 kxL.
-    p = config0(nx=8, ny=8, NZ=16, dt=0.05)
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=16, dt=0.05)
     lin, mf, kx0 = initial_state(p, 2, sigma=0.1)
     kxL = 2 * np.pi / p.L[0]
     ky = NumpyQL(p).ky
@@ -135,7 +135,7 @@ def test_remap_zeroes_mode_at_predicted_step():
 def test_energy_conservation_ideal():
     # nu=eta=0, q=0, static uniform field, QuasiLinear off: fluctuation energy is
     # conserved up to the RK3 truncation error, which falls ~8x per halving of dt.
-    p = config0(nx=8, ny=8, NZ=16, q=0.0, nu=1e-300, eta=1e-300, quasilinear=0, remap=0)
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=16, q=0.0, nu=1e-300, eta=1e-300, quasilinear=0, remap=0)
     lin, mf, kx0 = initial_state(p, 7, sigma=1.0)
     mf[:] = 0
     mf[1, 0] = 0.5 * p.NZ

@@ -16,7 +16,7 @@ import pytest
 from gpu_util import rel, require_gpu
 from ql_dns_b200 import _capi
 from ql_dns_b200.initial import initial_state
-from ql_dns_b200.params import config0
+from ql_dns_b200.params import mri_16x16_nz32
 from ql_dns_b200.solver import QLSolver
 
 pytestmark = pytest.mark.gpu
@@ -31,7 +31,7 @@ def _dev(a):
 def test_rhs_noalloc_matches_rhs_twice(model, NZ):
     require_gpu()
     import torch
-    p = config0(nx=16, ny=16, NZ=NZ, model=model, B0z=0.03 if model else 0.0, omega=0.9)
+    p = mri_16x16_nz32(nx=16, ny=16, NZ=NZ, model=model, B0z=0.03 if model else 0.0, omega=0.9)
     L = _capi.load()
     cp = _capi.to_c(p)
     with QLSolver(p) as s:
@@ -58,7 +58,7 @@ def test_rhs_noalloc_matches_rhs_twice(model, NZ):
 def test_rhs_noalloc_rejects_oversized_case():
     require_gpu()
     import torch
-    p = config0(nx=256, ny=256, NZ=32)  # 255*128 modes > 8192: rejected before any device work
+    p = mri_16x16_nz32(nx=256, ny=256, NZ=32)  # 255*128 modes > 8192: rejected before any device work
     L = _capi.load()
     cp = _capi.to_c(p)
     small = torch.zeros(16, dtype=torch.float64, device="cuda")
