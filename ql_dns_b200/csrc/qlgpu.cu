@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -213,13 +214,13 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
         h->err = "cudaGetDeviceProperties failed";
         return bail(QLGPU_ERR_CUDA);
     }
-    // CTA width: the number of warps (8, 4, 2 or 1) that maximises resident warps per SM,
-    // given shared memory, registers and (for the TMEM store) 512 TMEM columns per SM.
+    // CTA width: the number of warps (16 or 8 down to 1, as compiled) that maximises resident
+    // warps per SM, given shared memory, registers and (for the TMEM store) 512 TMEM columns per SM.
     int best_w = 1, best_res = -1, best_per_sm = 1;
-    for (int w = 8; w >= 1; w >>= 1) {
+    for (int w = var.max_warps; w >= 1; w >>= 1) {
         const size_t sm_bytes = var.smem(w);
         if (sm_bytes > (size_t)prop.sharedMemPerBlockOptin) continue;
-        if (cudaFuncSetAttribute(var.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_bytes) !=
+        if (ensure_smem_attr(var.kernel(), sm_bytes) !=
             cudaSuccess)
             continue;
         const int tc = var.tmem(w);
@@ -234,12 +235,14 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, var.kernel(), 32 * w, sm_bytes);
         if (tc > 0 && occ > 512 / tc) occ = 512 / tc;
         if (occ < 1) continue;
+        // warps that hold work at once: the CTAs the modes need (one mode per pair of
+        // groups), capped by what the GPU holds.  Narrower CTAs win ties: the same
+        // warps spread over more SMs.
         const int modes_per_cta = w * (32 / var.T) / 2;
-        // resident modes per SM, capped by the work available
-        int res = occ * modes_per_cta;
-        const int per_sm_need = (h->nxy + prop.multiProcessorCount - 1) / prop.multiProcessorCount;
-        if (res > per_sm_need) res = per_sm_need + (occ * w);  // prefer wider CTAs once the work fits
-        if (res > best_res) {
+        const long need = (h->nxy + modes_per_cta - 1) / modes_per_cta;
+        const long cap = (long)prop.multiProcessorCount * occ;
+        const int res = (int)((need < cap ? need : cap) * w);
+        if (best_res < 0 || res >= best_res * 0.98) {
             best_res = res;
             best_w = w;
             best_per_sm = occ;
@@ -248,7 +251,7 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
     h->warps = best_w;
     h->block = 32 * h->warps;
     h->smem = var.smem(h->warps);
-    if (cudaFuncSetAttribute(var.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem) != cudaSuccess) {
+    if (ensure_smem_attr(var.kernel(), h->smem) != cudaSuccess) {
         h->err = "shared memory request too large";
         return bail(QLGPU_ERR_CUDA);
     }
@@ -687,6 +690,12 @@ extern "C" int qlgpu_rhs_noalloc(const qlgpu_params* pp, double t, double dt_lin
     if (!(p.L[0] > 0 && p.L[1] > 0 && p.L[2] > 0)) return fail(nullptr, QLGPU_ERR_ARG, "box lengths must be > 0");
     if (p.model == QLGPU_MODEL_MHD_BQLIN && p.nu == 0.0)
         return fail(nullptr, QLGPU_ERR_ARG, "MHD_BQlin divides by nu (MHD_BQlin.cpp:251); nu must be nonzero");
+    {
+        // the kernel moves complex values as 16-byte vectors and requests whole modes into L2
+        const uintptr_t bits = (uintptr_t)lin_in | (uintptr_t)mf_in | (uintptr_t)kx0 | (uintptr_t)lin_rhs |
+                               (uintptr_t)mf_rhs | (uintptr_t)linop;
+        if (bits & 15) return fail(nullptr, QLGPU_ERR_ARG, "device pointers must be 16-byte aligned");
+    }
     Variant var;
     if (!pick_variant(p.NZ, p.model, QLGPU_INTEG_RK3CN_ELIN, true, &var))
         return fail(nullptr, QLGPU_ERR_UNSUPPORTED, "unsupported NZ: must be a power of two in [16, 256]");
@@ -717,7 +726,7 @@ extern "C" int qlgpu_rhs_noalloc(const qlgpu_params* pp, double t, double dt_lin
     int warps = 8;
     while (warps > 1 && var.smem(warps) > (size_t)prop.sharedMemPerBlockOptin) warps >>= 1;
     const size_t smem = var.smem(warps);
-    if (cudaFuncSetAttribute(var.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (ensure_smem_attr(var.kernel(), smem) != cudaSuccess)
         return fail(nullptr, QLGPU_ERR_CUDA, "shared memory request too large");
     const int modes_per_cta = warps * (32 / var.T) / 2;
     int grid = (nxy + modes_per_cta - 1) / modes_per_cta;

@@ -65,7 +65,7 @@ __device__ __forceinline__ void cta_copy8(void* dst, const void* src, int n) {
 // keeps the compile time of the kernel linear in the number of classes.  The
 // shared-memory objects are declared here so that every access stays a
 // shared-space access.
-template <int NZ, int MODEL, int INTEG>
+template <int NZ, int MODEL, int INTEG, int MAXNZ>
 __device__ __noinline__ bool batch_item_stage(const BatchCase* cs, int s, int swap, int cta, int ncta, uint32_t tmem) {
     static_assert(sizeof(StageArgs) % 8 == 0 && sizeof(DevParams) % 8 == 0, "8-byte copies");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -88,8 +88,16 @@ __device__ __noinline__ bool batch_item_stage(const BatchCase* cs, int s, int sw
     return stage_body<NZ, MODEL, INTEG, true>(sA, sP, cta, ncta, smem_raw, ss);
 }
 
-template <int MODEL, int INTEG>
-__global__ void __maxnreg__(224) batch_kernel(BatchLaunch L) {
+// MAXNZ: the largest NZ class the kernel steps.  With TMEM one CTA runs per
+// SM; classes up to NZ = 64 hold 8 points per thread, fit 128 registers and
+// run 16-warp CTAs, the NZ = 128 / 256 classes (16 points per thread) 8-warp CTAs.
+template <int MAXNZ>
+struct BatchOcc {
+    static constexpr int MAX_THREADS = MAXNZ <= 64 ? 512 : 256;
+};
+
+template <int MODEL, int INTEG, int MAXNZ>
+__global__ void __launch_bounds__(BatchOcc<MAXNZ>::MAX_THREADS, 1) batch_kernel(BatchLaunch L) {
     __shared__ uint32_t s_tmem;
     __shared__ int s_ok;
     __shared__ BatchSlot s_items[BATCH_MAX_SLOTS];
@@ -115,13 +123,17 @@ __global__ void __maxnreg__(224) batch_kernel(BatchLaunch L) {
                 const BatchSlot it = s_items[i];
                 const BatchCase* cs = L.cases + it.c;
                 bool top = false;
-                switch (it.NZ) {
-                    case 16: top = batch_item_stage<16, MODEL, INTEG>(cs, s, swap, it.cta, it.ncta, tmem); break;
-                    case 32: top = batch_item_stage<32, MODEL, INTEG>(cs, s, swap, it.cta, it.ncta, tmem); break;
-                    case 64: top = batch_item_stage<64, MODEL, INTEG>(cs, s, swap, it.cta, it.ncta, tmem); break;
-                    case 128: top = batch_item_stage<128, MODEL, INTEG>(cs, s, swap, it.cta, it.ncta, tmem); break;
-                    case 256: top = batch_item_stage<256, MODEL, INTEG>(cs, s, swap, it.cta, it.ncta, tmem); break;
-                    default: break;
+                if (it.NZ == 16) {
+                    top = batch_item_stage<16, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem);
+                } else if (it.NZ == 32) {
+                    top = batch_item_stage<32, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem);
+                } else if (it.NZ == 64) {
+                    top = batch_item_stage<64, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem);
+                } else if constexpr (MAXNZ >= 128) {
+                    if (it.NZ == 128)
+                        top = batch_item_stage<128, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem);
+                    else if (it.NZ == 256)
+                        top = batch_item_stage<256, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem);
                 }
                 if (tid == 0) s_top[i] = top ? 1 : 0;
                 if (top) {

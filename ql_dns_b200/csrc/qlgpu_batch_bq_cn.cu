@@ -2,5 +2,5 @@
 #include "qlgpu_batch_inst.cuh"
 
 namespace qlgpu {
-bool batch_kernel_bq_cn(BatchKernel* out) { return make_batch_kernel<MODEL_BQLIN, INTEG_CN>(out); }
+bool batch_kernel_bq_cn(bool wide, BatchKernel* out) { return make_batch_kernel<MODEL_BQLIN, INTEG_CN>(wide, out); }
 }  // namespace qlgpu

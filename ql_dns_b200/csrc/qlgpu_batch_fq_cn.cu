@@ -2,5 +2,5 @@
 #include "qlgpu_batch_inst.cuh"
 
 namespace qlgpu {
-bool batch_kernel_fq_cn(BatchKernel* out) { return make_batch_kernel<MODEL_FULLQLIN, INTEG_CN>(out); }
+bool batch_kernel_fq_cn(bool wide, BatchKernel* out) { return make_batch_kernel<MODEL_FULLQLIN, INTEG_CN>(wide, out); }
 }  // namespace qlgpu

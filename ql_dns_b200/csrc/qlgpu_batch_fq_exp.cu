@@ -2,5 +2,5 @@
 #include "qlgpu_batch_inst.cuh"
 
 namespace qlgpu {
-bool batch_kernel_fq_exp(BatchKernel* out) { return make_batch_kernel<MODEL_FULLQLIN, INTEG_EXP>(out); }
+bool batch_kernel_fq_exp(bool wide, BatchKernel* out) { return make_batch_kernel<MODEL_FULLQLIN, INTEG_EXP>(wide, out); }
 }  // namespace qlgpu

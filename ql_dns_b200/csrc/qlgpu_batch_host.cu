@@ -194,7 +194,7 @@ bool width_limits(qlgpu_batch_t* b, int warps, int* per_sm, size_t* smem) {
         tc = std::max(tc, b->bk.tmem(c.NZ, warps));
     }
     if (sm > b->smem_optin || tc > 512) return false;
-    if (cudaFuncSetAttribute(b->bk.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    if (ensure_smem_attr(b->bk.kernel(), sm) != cudaSuccess)
         return false;
     cudaFuncSetAttribute(b->bk.kernel(), cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     int occ = 0;
@@ -351,7 +351,7 @@ int apply_mapping(qlgpu_batch_t* b, int warps, int per_sm, size_t smem, const st
         }
         m.tcols = tc;
     }
-    if (cudaFuncSetAttribute(b->bk.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (ensure_smem_attr(b->bk.kernel(), smem) != cudaSuccess)
         return bfail(b, QLGPU_ERR_CUDA, "batch kernel: shared memory request too large");
     QB_CK(cudaMemcpyAsync(b->d_ctas, ctas.data(), sizeof(BatchCta) * ctas.size(), cudaMemcpyHostToDevice, b->stream));
     QB_CK(cudaStreamSynchronize(b->stream));
@@ -412,7 +412,7 @@ int run_launch(qlgpu_batch_t* b, int nsteps, int reset_ndiag) {
     }
     if (nsteps == 0) return QLGPU_OK;
     // the dynamic shared memory attribute belongs to the kernel, not to this batch
-    QB_CK(cudaFuncSetAttribute(b->bk.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+    QB_CK(ensure_smem_attr(b->bk.kernel(), b->smem));
     if (b->use_graph) {
         const auto key = std::make_tuple(nsteps, b->cur, reset_ndiag);
         auto itg = b->graphs.find(key);
@@ -521,7 +521,9 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
         b->err = "cudaSetDevice failed";
         return bail(QLGPU_ERR_NODEVICE);
     }
-    if (!pick_batch_kernel(b->model, b->integ, &b->bk)) {
+    int max_nz = 0;
+    for (int c = 0; c < ncases; ++c) max_nz = std::max(max_nz, cases[c].NZ);
+    if (!pick_batch_kernel(b->model, b->integ, max_nz > 64, &b->bk)) {
         b->err = "no batch kernel for this model / integrator";
         return bail(QLGPU_ERR_UNSUPPORTED);
     }
@@ -547,7 +549,7 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
     // Per-case sizes and the arena layout
     b->cs.resize(ncases);
     b->tv_set.assign(ncases, 0.0);
-    const int max_grid = 2 * b->sms;  // widest launch: 4-warp CTAs, two per SM
+    const int max_grid = 2 * b->sms;  // widest launch: two CTAs per SM
     std::vector<size_t> off(ncases);
     size_t o = 0;
     for (int c = 0; c < ncases; ++c) {
@@ -655,8 +657,8 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
         return bail(QLGPU_ERR_CUDA);
     }
     // initial mapping from the cost model: the widest CTA that fits
-    int rc = plan_and_apply(b, 8, nullptr);
-    if (rc) rc = plan_and_apply(b, 4, nullptr);
+    int rc = plan_and_apply(b, b->bk.max_warps, nullptr);
+    if (rc) rc = plan_and_apply(b, b->bk.max_warps / 2, nullptr);
     if (rc) return bail(rc);
     rc = upload_descriptors(b);
     if (rc) return bail(rc);
@@ -835,7 +837,7 @@ int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms) {
     std::vector<unsigned long long> ends(b->ncases);
     // one probe of the current mapping: launch time and per-case stage times (us per stage)
     auto probe = [&](double* ms, std::vector<double>* ystage) -> int {
-        QB_CK(cudaFuncSetAttribute(b->bk.kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+        QB_CK(ensure_smem_attr(b->bk.kernel(), b->smem));
         QB_CK(cudaEventRecord(b->ev[0], b->stream));
         QB_CK(enqueue_launch(b, probe_steps, 0));
         QB_CK(cudaEventRecord(b->ev[1], b->stream));
@@ -927,7 +929,7 @@ int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms) {
             if (x[2 + j] > 0) cm.r[j] = x[2 + j];
     };
     int rc = QLGPU_OK;
-    for (int warps : {8, 4}) {
+    for (int warps : {b->bk.max_warps, b->bk.max_warps / 2}) {
         int per_sm = 0;
         size_t smem = 0;
         if (!width_limits(b, warps, &per_sm, &smem)) continue;
@@ -980,7 +982,10 @@ int qlgpu_batch_mapping(const qlgpu_batch_t* b, int* info4, int* ncta) {
 
 int qlgpu_batch_set_mapping(qlgpu_batch_t* b, int warps, const int* ncta) {
     if (!b || !ncta) return QLGPU_ERR_ARG;
-    if (warps != 4 && warps != 8) return bfail(b, QLGPU_ERR_ARG, "warps per CTA must be 4 or 8");
+    if (warps != b->bk.max_warps && warps != b->bk.max_warps / 2)
+        return bfail(b, QLGPU_ERR_ARG,
+                     "warps per CTA must be " + std::to_string(b->bk.max_warps) + " or " +
+                         std::to_string(b->bk.max_warps / 2) + " for this batch");
     QB_CK(cudaSetDevice(b->device));
     return plan_and_apply(b, warps, ncta);
 }

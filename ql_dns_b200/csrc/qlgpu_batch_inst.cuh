@@ -6,7 +6,7 @@
 
 namespace qlgpu {
 
-template <int MODEL, int INTEG>
+template <int MODEL, int INTEG, int MAXNZ>
 cudaError_t batch_launch(const BatchLaunch& L, int grid, int block, size_t smem, cudaStream_t st) {
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
@@ -19,11 +19,11 @@ cudaError_t batch_launch(const BatchLaunch& L, int grid, int block, size_t smem,
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, batch_kernel<MODEL, INTEG>, L);
+    return cudaLaunchKernelEx(&cfg, batch_kernel<MODEL, INTEG, MAXNZ>, L);
 }
-template <int MODEL, int INTEG>
+template <int MODEL, int INTEG, int MAXNZ>
 const void* batch_ptr() {
-    return reinterpret_cast<const void*>(&batch_kernel<MODEL, INTEG>);
+    return reinterpret_cast<const void*>(&batch_kernel<MODEL, INTEG, MAXNZ>);
 }
 template <int MODEL>
 size_t batch_smem(int NZ, int warps) {
@@ -48,11 +48,13 @@ int batch_tmem(int NZ, int warps) {
     }
 }
 template <int MODEL, int INTEG>
-bool make_batch_kernel(BatchKernel* out) {
-    out->launch = &batch_launch<MODEL, INTEG>;
-    out->kernel = &batch_ptr<MODEL, INTEG>;
+bool make_batch_kernel(bool wide, BatchKernel* out) {
+    out->launch = wide ? &batch_launch<MODEL, INTEG, 256> : &batch_launch<MODEL, INTEG, 64>;
+    out->kernel = wide ? &batch_ptr<MODEL, INTEG, 256> : &batch_ptr<MODEL, INTEG, 64>;
     out->smem = &batch_smem<MODEL>;
     out->tmem = &batch_tmem<MODEL>;
+    out->max_nz = wide ? 256 : 64;
+    out->max_warps = (wide ? BatchOcc<256>::MAX_THREADS : BatchOcc<64>::MAX_THREADS) / 32;
     return true;
 }
 

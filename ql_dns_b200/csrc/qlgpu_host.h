@@ -7,7 +7,10 @@
 
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/qlgpu.h"
@@ -37,8 +40,9 @@ struct Variant {
     smem_fn smem;
     tmem_fn tmem;
     diag_launch_fn diag;
-    int T;   // threads per transform group
-    int PL;  // partial vector length (doubles)
+    int T;          // threads per transform group
+    int PL;         // partial vector length (doubles)
+    int max_warps;  // widest CTA the kernel is compiled for
 };
 
 // Defined in qlgpu_nz<NZ>.cu, one translation unit per NZ.
@@ -59,21 +63,43 @@ inline bool pick_variant(int NZ, int model, int integ, bool tm, Variant* out) {
     }
 }
 
-// The persistent batch kernel of one model x integrator (qlgpu_batch_<model>_<integ>.cu).
+// The persistent batch kernel of one model x integrator (qlgpu_batch_<model>_<integ>.cu),
+// in two builds: NZ <= 64 only (128 registers, two 8-warp CTAs per SM) and all NZ.
 struct BatchKernel {
     cudaError_t (*launch)(const BatchLaunch& L, int grid, int block, size_t smem, cudaStream_t st);
     const void* (*kernel)();
     size_t (*smem)(int NZ, int warps);  // dynamic shared memory of one NZ class
     int (*tmem)(int NZ, int warps);     // TMEM columns of one NZ class
+    int max_nz;                         // largest NZ class the build steps
+    int max_warps;                      // widest CTA the build is compiled for
 };
-bool batch_kernel_bq_exp(BatchKernel* out);
-bool batch_kernel_bq_cn(BatchKernel* out);
-bool batch_kernel_fq_exp(BatchKernel* out);
-bool batch_kernel_fq_cn(BatchKernel* out);
+bool batch_kernel_bq_exp(bool wide, BatchKernel* out);
+bool batch_kernel_bq_cn(bool wide, BatchKernel* out);
+bool batch_kernel_fq_exp(bool wide, BatchKernel* out);
+bool batch_kernel_fq_cn(bool wide, BatchKernel* out);
 
-inline bool pick_batch_kernel(int model, int integ, BatchKernel* out) {
-    if (model == MODEL_BQLIN) return integ == INTEG_EXP ? batch_kernel_bq_exp(out) : batch_kernel_bq_cn(out);
-    return integ == INTEG_EXP ? batch_kernel_fq_exp(out) : batch_kernel_fq_cn(out);
+inline bool pick_batch_kernel(int model, int integ, bool wide, BatchKernel* out) {
+    if (model == MODEL_BQLIN)
+        return integ == INTEG_EXP ? batch_kernel_bq_exp(wide, out) : batch_kernel_bq_cn(wide, out);
+    return integ == INTEG_EXP ? batch_kernel_fq_exp(wide, out) : batch_kernel_fq_cn(wide, out);
+}
+
+// The dynamic shared memory limit is an attribute of the kernel function, shared
+// by every handle, batch and no-allocation call of the process on a device: it
+// is only ever raised, so a launch prepared by one of them is never invalidated
+// by another that needs less.
+inline cudaError_t ensure_smem_attr(const void* kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> set;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = set[std::make_pair(dev, kernel)];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
 }
 
 // Threads per transform group for a supported NZ (qlgpu_fft.cuh Geom), 0 if unsupported.

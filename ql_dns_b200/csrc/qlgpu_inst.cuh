@@ -41,6 +41,7 @@ Variant make_variant() {
     v.diag = &launch_diag<NZ>;
     v.T = Geom<NZ>::T;
     v.PL = StageKind<NZ, MODEL, TM>::SM::PL;
+    v.max_warps = StageOcc<NZ>::MAX_THREADS / 32;
     return v;
 }
 

@@ -391,10 +391,24 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     if (tr) A.trace[6] = gtimer();
     const int wglobal = cta * warps + warp;
     const int WG = ncta * warps;
+    // The fields (and previous right-hand side) of a mode are contiguous, 64 nz
+    // bytes each: one lane per pair requests the pair's next mode into L2 while
+    // the current one is transformed, so the stage's loads wait on L2, not DRAM.
+    const bool pf_lane = (role == 0 && t == 0);
+    const cplx* pf_prev = (A.Fprev && A.sc.has_prev) ? A.Fprev : nullptr;
+    const unsigned pf_bytes = 64u * (unsigned)P.nz;
+    if (pf_lane && wglobal * PW + pi < P.nxy) {
+        l2_prefetch(A.lin_in + (size_t)(wglobal * PW + pi) * 4 * P.nz, pf_bytes);
+        if (pf_prev) l2_prefetch(pf_prev + (size_t)(wglobal * PW + pi) * 4 * P.nz, pf_bytes);
+    }
     for (int base = wglobal * PW; base < P.nxy; base += WG * PW) {
         const int mode_raw = base + pi;
         const bool valid = mode_raw < P.nxy;
         const int mode = valid ? mode_raw : P.nxy - 1;
+        if (pf_lane && mode_raw + WG * PW < P.nxy) {
+            l2_prefetch(A.lin_in + (size_t)(mode_raw + WG * PW) * 4 * P.nz, pf_bytes);
+            if (pf_prev) l2_prefetch(pf_prev + (size_t)(mode_raw + WG * PW) * 4 * P.nz, pf_bytes);
+        }
         if constexpr (MODEL == MODEL_BQLIN)
             bqlin_pair<G, INTEG, Priv>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps, pv, tw_s, mfr, tclock,
                                        cn);
@@ -534,8 +548,17 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
 
 // One stage launch of a single case: one CTA per SM at most, TMEM allocated
 // for the duration of the launch.
+// CTA size bound.  A kernel that allocates TMEM runs one CTA per SM, so the
+// resident warps of an SM are the warps of one CTA.  Transform groups of P = 8
+// points per thread fit 128 registers and run 16-warp CTAs; P = 16 keeps
+// 8-warp CTAs with up to 255 registers.
+template <int NZ>
+struct StageOcc {
+    static constexpr int MAX_THREADS = Geom<NZ>::P <= 8 ? 512 : 256;
+};
+
 template <int NZ, int MODEL, int INTEG, bool USE_TMEM>
-__global__ void __maxnreg__(224) stage_kernel(StageArgs A, DevParams P) {
+__global__ void __launch_bounds__(StageOcc<NZ>::MAX_THREADS, 1) stage_kernel(StageArgs A, DevParams P) {
     using SM = typename StageKind<NZ, MODEL, USE_TMEM>::SM;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ StageShared ss;

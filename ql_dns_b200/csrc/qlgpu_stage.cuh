@@ -42,6 +42,12 @@ __device__ __forceinline__ void stc(cplx* p, cplx v) {
 // i*s*a for real s
 __device__ __forceinline__ cplx imul(cplx a, double s) { return mk(-a.y * s, a.x * s); }
 
+// Asynchronous prefetch of a contiguous range into L2 (one bulk request, no
+// registers or shared memory held; bytes a multiple of 16, address 16-aligned).
+__device__ __forceinline__ void l2_prefetch(const void* p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long v;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(v)::"memory");
