@@ -28,7 +28,10 @@ EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "ql
            "qlgpu_batch_get_state", "qlgpu_batch_diagnostics", "qlgpu_batch_step", "qlgpu_batch_step_timed",
            "qlgpu_batch_tune", "qlgpu_batch_mapping", "qlgpu_batch_set_mapping", "qlgpu_batch_status",
            "qlgpu_batch_set_wait", "qlgpu_batch_debug_drop_item", "qlgpu_batch_stream",
-           "qlgpu_batch_last_error"]
+           "qlgpu_batch_last_error",
+           "qlgpu_timevars_open", "qlgpu_timevars_save_data", "qlgpu_timevars_save_mean_fields",
+           "qlgpu_timevars_close", "qlgpu_fullsave_write", "qlgpu_fullsave_read_latest", "qlgpu_fullsave_times",
+           "qlgpu_io_last_error"]
 
 
 class qlgpu_params(ctypes.Structure):
@@ -101,6 +104,15 @@ def load(path: str = LIB_PATH):
     L.qlgpu_batch_debug_drop_item.argtypes = [vp, ctypes.c_int]
     L.qlgpu_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.qlgpu_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    L.qlgpu_timevars_open.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(vp)]
+    L.qlgpu_timevars_save_data.argtypes = [vp, dp]
+    L.qlgpu_timevars_save_mean_fields.argtypes = [vp, dp, ctypes.c_int]
+    L.qlgpu_timevars_close.argtypes = [vp]
+    L.qlgpu_fullsave_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(qlgpu_params), ctypes.c_double, dp, dp, dp]
+    L.qlgpu_fullsave_read_latest.argtypes = [ctypes.c_char_p, ctypes.POINTER(qlgpu_params), dp, dp, dp, dp]
+    L.qlgpu_fullsave_times.argtypes = [ctypes.c_char_p, dp, ctypes.c_int, ip]
+    L.qlgpu_io_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int]
     for name in EXPORTS:
         if name not in ("qlgpu_version",):
             getattr(L, name).restype = ctypes.c_int
@@ -131,4 +143,13 @@ def check_batch(rc: int, b=None):
         L = load()
         buf = ctypes.create_string_buffer(512)
         L.qlgpu_batch_last_error(b, buf, 512)
+        raise QLGPUError(rc, buf.value.decode(errors="replace"))
+
+
+def check_io(rc: int):
+    """As check() for the file entry points of include/qlgpu_io.h."""
+    if rc != QLGPU_OK:
+        L = load()
+        buf = ctypes.create_string_buffer(512)
+        L.qlgpu_io_last_error(buf, 512)
         raise QLGPUError(rc, buf.value.decode(errors="replace"))

@@ -29,7 +29,7 @@ OBJ_DIR = os.path.join(OUT_DIR, "obj")
 
 def sources():
     """Translation units of libqlgpu.so: the host code and one file per kernel family, compiled in parallel."""
-    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
 
 
 def deps():
@@ -45,7 +45,7 @@ def stale() -> bool:
 
 
 def _headers_mtime() -> float:
-    hs = [d for d in deps() if not d.endswith(".cu") and os.path.isfile(d)]
+    hs = [d for d in deps() if not d.endswith((".cu", ".cpp")) and os.path.isfile(d)]
     return max(os.path.getmtime(h) for h in hs) if hs else 0.0
 
 
@@ -58,7 +58,7 @@ def build(force: bool = False, verbose: bool = False, extra=None, jobs: int | No
     inc = ["-I" + os.path.join(ROOT, "include")]
 
     def compile_one(src):
-        obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
+        obj = os.path.join(OBJ_DIR, os.path.splitext(os.path.basename(src))[0] + ".o")
         if (not force and extra is None and os.path.exists(obj) and os.path.getmtime(obj) > os.path.getmtime(src)
                 and os.path.getmtime(obj) > hdr_t):
             return obj
@@ -74,7 +74,8 @@ def build(force: bool = False, verbose: bool = False, extra=None, jobs: int | No
         return obj
 
     # the kernel translation units are the slow ones: start them first
-    srcs = sorted(sources(), key=lambda f: -os.path.getsize(f) if os.path.basename(f) != "qlgpu.cu" else 0)
+    srcs = sorted(sources(), key=lambda f: -os.path.getsize(f) if f.endswith(".cu") and
+                  os.path.basename(f) != "qlgpu.cu" else 0)
     n = jobs or max(1, min(len(srcs), os.cpu_count() or 1))
     with concurrent.futures.ThreadPoolExecutor(max_workers=n) as ex:
         objs = list(ex.map(compile_one, srcs))

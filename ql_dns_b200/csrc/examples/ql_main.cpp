@@ -1,6 +1,6 @@
 // ql_main.cpp -- a QL_DNS/main.cpp-shaped driver on the B200 step.
 //
-//   ql_main <input.DSSinput> <state_in.bin> <nsteps> <state_out.bin> <diag_out.bin>
+//   ql_main <input.DSSinput> <state_in.bin> <nsteps> <state_out.bin> <diag_out.bin> [output_dir]
 //
 // Reads the reference's .DSSinput keys (QL_DNS/Auxiliary/Input_parameters.cpp:68-138,
 // found by substring then '=' like Read_From_Input_File_, :178-209), an initial
@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "qlgpu.hpp"
+#include "qlgpu_io.h"
 
 template <class T>
 static T read_key(const std::string& file, const std::string& key, T dflt) {
@@ -28,8 +29,9 @@ static T read_key(const std::string& file, const std::string& key, T dflt) {
 }
 
 int main(int argc, char** argv) {
-    if (argc != 6) {
-        std::fprintf(stderr, "usage: %s input.DSSinput state_in.bin nsteps state_out.bin diag_out.bin\n", argv[0]);
+    if (argc != 6 && argc != 7) {
+        std::fprintf(stderr, "usage: %s input.DSSinput state_in.bin nsteps state_out.bin diag_out.bin [output_dir]\n",
+                     argv[0]);
         return 2;
     }
     std::ifstream fin(argv[1]);
@@ -74,6 +76,7 @@ int main(int argc, char** argv) {
             std::cerr << "state file too short" << std::endl;
             return 1;
         }
+        const std::vector<qlgpu::dcmplx> mf0 = sol.mf;
         qlgpu::Integrator* integrator = integ == 1 ? static_cast<qlgpu::Integrator*>(new qlgpu::RK3CN(t, SP, model))
                                                    : static_cast<qlgpu::Integrator*>(new qlgpu::RK3CN_Elin(t, SP, model));
         const int every = (int)(tv_save / SP.dt + 0.5);
@@ -88,6 +91,33 @@ int main(int argc, char** argv) {
         std::ofstream sd(argv[5], std::ios::binary);
         sd.write(reinterpret_cast<const char*>(diag.data()), diag.size() * sizeof(double));
         std::printf("ql_main: %d steps, t = %.10g, %zu diagnostic records\n", nsteps, tout, diag.size() / 15);
+        if (argc > 6) {
+            // Output directory (SP.simulation_dir): the TimeVariables files (main.cpp:98-130) with a
+            // record per diagnostic save and the mean fields at the start and the end, and a full
+            // save of the final state when full_save_ > 0 (main.cpp:135-140).
+            const std::string dir = std::string(argv[6]) + "/";
+            const qlgpu_params gp = model->params();
+            qlgpu_timevars_t* tv = nullptr;
+            const int nrey = SP.equations_to_use == "MHD_BQlin" ? 5 : 4;
+            char msg[256];
+            if (qlgpu_timevars_open(dir.c_str(), model->num_MFs(), model->NZfull(), nrey, 0, &tv) != QLGPU_OK) {
+                qlgpu_io_last_error(msg, sizeof(msg));
+                std::cerr << "time variables: " << msg << std::endl;
+                return 1;
+            }
+            qlgpu_timevars_save_mean_fields(tv, reinterpret_cast<const double*>(mf0.data()), model->NZ());
+            for (size_t r = 0; r < diag.size() / 15; ++r) qlgpu_timevars_save_data(tv, diag.data() + 15 * r);
+            qlgpu_timevars_save_mean_fields(tv, reinterpret_cast<const double*>(sol.mf.data()), model->NZ());
+            qlgpu_timevars_close(tv);
+            if (read_key<double>(full, "full_save_", 0.0) > 0.0 &&
+                qlgpu_fullsave_write((dir + "FullSave.bin").c_str(), &gp, tout,
+                                     reinterpret_cast<const double*>(sol.lin.data()),
+                                     reinterpret_cast<const double*>(sol.mf.data()), sol.kx0.data()) != QLGPU_OK) {
+                qlgpu_io_last_error(msg, sizeof(msg));
+                std::cerr << "full save: " << msg << std::endl;
+                return 1;
+            }
+        }
         delete integrator;
         delete model;
     } catch (const qlgpu::Error& e) {

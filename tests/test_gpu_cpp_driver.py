@@ -36,6 +36,7 @@ B0z_ = {p.B0z!r}
 Remap? = {p.remap}
 QuasiLinear? = {p.quasilinear}
 integrator_ = {integ}
+full_save_ = 1.0
 """
     open(path, "w").write(txt)
 
@@ -55,7 +56,9 @@ def test_cpp_driver_matches_oracle(tmp_path, integ):
         mf.tofile(f)
         kx0.tofile(f)
     out, dg = tmp_path / "out.bin", tmp_path / "diag.bin"
-    r = subprocess.run([MAIN, str(inp), str(st), "100", str(out), str(dg)], capture_output=True, text=True)
+    odir = tmp_path / "sim"
+    odir.mkdir()
+    r = subprocess.run([MAIN, str(inp), str(st), "100", str(out), str(dg), str(odir)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     raw = np.fromfile(out, dtype=np.float64)
     n_lin, n_mf = lin.size * 2, mf.size * 2
@@ -68,3 +71,11 @@ def test_cpp_driver_matches_oracle(tmp_path, integ):
     assert t == t2 and np.array_equal(ko, ko2)
     assert rel(lo, lo2) < 1e-10 and rel(mo, mo2) < 1e-10
     assert d.shape == d2.shape and rel(d[:, 1:13], d2[:, 1:13]) < 1e-10
+    # the reference's output files from the same run
+    from ql_dns_b200 import io
+    e = np.fromfile(odir / "energy.dat").reshape(-1, 4)
+    assert np.array_equal(e, d[:, 1:5]) and np.array_equal(np.fromfile(odir / "time_vec.dat"), d[:, 0])
+    assert np.fromfile(odir / "mean_fields.dat").size == 2 * p.nmf * p.NZ
+    tl, ll, ml, kl = io.load_solution(str(odir / "FullSave.bin"), p)
+    assert tl == t and np.array_equal(ll, lo.astype(np.complex64).astype(np.complex128))
+    assert np.array_equal(ml, mo.astype(np.complex64).astype(np.complex128))
