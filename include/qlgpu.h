@@ -160,6 +160,19 @@ int qlgpu_last_error(const qlgpu_t* h, char* buf, int buflen);
 /* Library version string. */
 const char* qlgpu_version(void);
 
+/* Discrete adjoint (no counterpart in the reference).  For MHD_BQlin with
+ * RK3CN_Elin: J = (1/N) sum_{n=1..N} AM_b(t0 + n dt), the fluctuation Maxwell
+ * stress of the diagnostic records (MHD_BQlin.cpp:392,424, column 8 of a
+ * record) averaged over N = nsteps steps.  Runs the N steps from (t0, lin0,
+ * mf0, kx0) (kx0 may be NULL) keeping a checkpoint every checkpoint_every
+ * steps, then the adjoint of every stage in reverse, recomputing the stages of
+ * one checkpoint window at a time.  Returns J, grad_lin = dJ/d lin0 (complex
+ * [nxy][4][nz]: dJ = Re sum conj(grad_lin) d lin0, i.e. the derivatives with
+ * respect to the real and imaginary parts) and, when grad_mf is not NULL,
+ * dJ/d mf0 likewise.  The handle is left at the end of the forward run. */
+int qlgpu_adjoint_maxwell(qlgpu_t* h, double t0, const double* lin0, const double* mf0, const double* kx0,
+                          int nsteps, int checkpoint_every, double* J, double* grad_lin, double* grad_mf);
+
 /* ------------------------------------------------------------------------
  * Batched ensemble.  No counterpart in the reference, which runs one case per
  * MPI job (QL_DNS/main.cpp:23-180): here many independent cases, each with

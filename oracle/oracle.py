@@ -55,6 +55,8 @@ def lib(kind: str = "strict"):
                              dp, dp, dp, dp, dp, dp]
     L.oracle_diagnostics.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_double, dp, dp, dp, dp]
     L.oracle_fft.argtypes = [ctypes.c_int, ctypes.c_int, dp]
+    L.oracle_tlm_maxwell.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_double, dp, dp, dp, dp, dp,
+                                     ctypes.c_int, dp, dp]
     _LIBS[kind] = L
     return L
 
@@ -110,3 +112,21 @@ def run(p, t0, lin, mf, kx0, nsteps, diag_every=0, kind: str = "strict", nthread
     n = lib(kind).oracle_run(ctypes.byref(pp), _dp(t), _dp(lin), _dp(mf), _dp(kx0), nsteps,
                              diag_every, _dp(diag), maxd)
     return float(t[0]), lin, mf, kx0, diag[:n]
+
+
+def tlm_maxwell(p, t0, lin, mf, kx0, dlin, dmf=None, nsteps: int = 1, kind: str = "strict"):
+    """Tangent-linear run (MHD_BQlin / RK3CN_Elin): (J, dJ) with J the mean over the
+    steps of the fluctuation Maxwell stress and dJ its derivative along (dlin, dmf)."""
+    lin = np.ascontiguousarray(lin, dtype=np.complex128)
+    mf = np.ascontiguousarray(mf, dtype=np.complex128)
+    dlin = np.ascontiguousarray(dlin, dtype=np.complex128)
+    k = None if kx0 is None else _dp(np.ascontiguousarray(kx0, dtype=np.float64))
+    dm = None if dmf is None else _dp(np.ascontiguousarray(dmf, dtype=np.complex128))
+    J = np.zeros(1)
+    dJ = np.zeros(1)
+    pp = _params(p)
+    rc = lib(kind).oracle_tlm_maxwell(ctypes.byref(pp), t0, _dp(lin), _dp(mf), k, _dp(dlin), dm, nsteps,
+                                      _dp(J), _dp(dJ))
+    if rc:
+        raise ValueError("the tangent-linear oracle covers MHD_BQlin with RK3CN_Elin")
+    return float(J[0]), float(dJ[0])

@@ -946,4 +946,94 @@ int oracle_run(const OracleParams* p, double* t_io, double* lin_io, double* mf_i
     return nrec;
 }
 
+// Tangent-linear run for MHD_BQlin / RK3CN_Elin (the checker of the adjoint).
+// J = (1/N) sum_{n=1..N} AM_b after each step (main.cpp:108-133, AM_b of
+// MHD_BQlin.cpp:392,424) and its derivative dJ in the direction (dlin, dmf)
+// of the initial state.  The state is propagated with the tangent alongside:
+// the stage update is linear (RK3CN_Elin.cpp:102-104) and is applied to both;
+// the remap zeroes the same modes in both; the derivative of the rhs and of
+// AM_b, both polynomials of degree two in the state, is taken exactly by the
+// polarization identity D f(x) d = (f(x + h d) - f(x - h d)) / (2 h).
+int oracle_tlm_maxwell(const OracleParams* p, double t0, const double* lin_in, const double* mf_in,
+                       const double* kx0_in, const double* dlin_in, const double* dmf_in, int nsteps, double* J,
+                       double* dJ) {
+    if (p->model != 0 || p->integrator != 0) return 1;
+    Model M(*p);
+    State s, ds;
+    s.init(M.d);
+    ds.init(M.d);
+    std::memcpy(s.lin.data(), lin_in, s.lin.size() * sizeof(cd));
+    std::memcpy(s.mf.data(), mf_in, s.mf.size() * sizeof(cd));
+    std::memcpy(ds.lin.data(), dlin_in, ds.lin.size() * sizeof(cd));
+    if (dmf_in) std::memcpy(ds.mf.data(), dmf_in, ds.mf.size() * sizeof(cd));
+    std::vector<double> kx0(M.K.kx);
+    if (kx0_in) kx0.assign(kx0_in, kx0_in + M.d.nxy);
+    double t = t0;
+    Integrator I(M, t, kx0);
+    auto norm = [](const State& x) {
+        double a = 0;
+        for (const cd& v : x.lin) a += std::norm(v);
+        for (const cd& v : x.mf) a += std::norm(v);
+        return std::sqrt(a);
+    };
+    auto axpy = [&](State& out, const State& x, double h, const State& d) {
+        for (size_t i = 0; i < x.lin.size(); ++i) out.lin[i] = x.lin[i] + h * d.lin[i];
+        for (size_t i = 0; i < x.mf.size(); ++i) out.mf[i] = x.mf[i] + h * d.mf[i];
+    };
+    State F1, F2, dF1, dF2, xp, xm, Fp, Fm;
+    for (State* z : {&F1, &F2, &dF1, &dF2, &xp, &xm, &Fp, &Fm}) z->init(M.d);
+    dvec dummy((size_t)M.d.nxy * 4 * M.d.nz);
+    auto step_h = [&](const State& x, const State& d) {
+        const double nx = norm(x), nd = norm(d);
+        return (nd > 0 && nx > 0) ? nx / nd : 1.0;
+    };
+    // dF = D rhs(x) d
+    auto tangent_rhs = [&](double tt, double ldt, const State& x, const State& d, State& dF) {
+        const double h = step_h(x, d);
+        axpy(xp, x, h, d);
+        axpy(xm, x, -h, d);
+        M.rhs(tt, ldt, xp, Fp, kx0, dummy);
+        M.rhs(tt, ldt, xm, Fm, kx0, dummy);
+        for (size_t i = 0; i < dF.lin.size(); ++i) dF.lin[i] = (Fp.lin[i] - Fm.lin[i]) / (2 * h);
+        for (size_t i = 0; i < dF.mf.size(); ++i) dF.mf[i] = (Fp.mf[i] - Fm.mf[i]) / (2 * h);
+    };
+    double diag[14];
+    auto amb = [&](double tt, const State& x) {
+        M.diagnostics(tt, x, kx0, diag);
+        return diag[7];  // AM_b: energy[4], AM[4] -> index 7 of the 14 values
+    };
+    const double dt = p->dt;
+    const double a0 = I.a0, a1 = I.a1, a2 = I.a2, b1 = I.b1, b2 = I.b2, p1 = I.p1, p2 = I.p2;
+    double sJ = 0, sdJ = 0;
+    for (int n = 0; n < nsteps; ++n) {
+        // RK3CN_Elin::Step (RK3CN_Elin.cpp:86-177) on the state and the tangent
+        M.rhs(t, dt * p1, s, F1, kx0, I.linOp);
+        tangent_rhs(t, dt * p1, s, ds, dF1);
+        I.update_exp(s, F1, nullptr, dt * a0, a0 * dt, 0);
+        I.update_exp(ds, dF1, nullptr, dt * a0, a0 * dt, 0);
+        M.rhs(t + dt * p1, dt * (p2 - p1), s, F2, kx0, I.linOp);
+        tangent_rhs(t + dt * p1, dt * (p2 - p1), s, ds, dF2);
+        I.update_exp(s, F2, &F1, dt * (a1 + b1), a1 * dt, b1 * dt);
+        I.update_exp(ds, dF2, &dF1, dt * (a1 + b1), a1 * dt, b1 * dt);
+        M.rhs(t + dt * p2, dt * (1.0 - p2), s, F1, kx0, I.linOp);
+        tangent_rhs(t + dt * p2, dt * (1.0 - p2), s, ds, dF1);
+        I.update_exp(s, F1, &F2, dt * (a2 + b2), a2 * dt, b2 * dt);
+        I.update_exp(ds, dF1, &dF2, dt * (a2 + b2), a2 * dt, b2 * dt);
+        t += dt;
+        if (p->remap) {
+            std::vector<double> k2 = kx0;
+            M.remap(p->q * t, s, kx0);
+            M.remap(p->q * t, ds, k2);
+        }
+        sJ += amb(t, s);
+        const double h = step_h(s, ds);
+        axpy(xp, s, h, ds);
+        axpy(xm, s, -h, ds);
+        sdJ += (amb(t, xp) - amb(t, xm)) / (2 * h);
+    }
+    *J = sJ / nsteps;
+    *dJ = sdJ / nsteps;
+    return 0;
+}
+
 }  // extern "C"

@@ -24,6 +24,7 @@ EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "ql
            "qlgpu_stream",
            "qlgpu_last_error",
            "qlgpu_version",
+           "qlgpu_adjoint_maxwell",
            "qlgpu_batch_create", "qlgpu_batch_destroy", "qlgpu_batch_dims", "qlgpu_batch_set_state",
            "qlgpu_batch_get_state", "qlgpu_batch_diagnostics", "qlgpu_batch_step", "qlgpu_batch_step_timed",
            "qlgpu_batch_tune", "qlgpu_batch_mapping", "qlgpu_batch_set_mapping", "qlgpu_batch_status",
@@ -88,6 +89,7 @@ def load(path: str = LIB_PATH):
     L.qlgpu_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.qlgpu_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.qlgpu_version.restype = ctypes.c_char_p
+    L.qlgpu_adjoint_maxwell.argtypes = [vp, ctypes.c_double, dp, dp, dp, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.qlgpu_batch_create.argtypes = [ctypes.POINTER(qlgpu_params), ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
     L.qlgpu_batch_destroy.argtypes = [vp]
     L.qlgpu_batch_dims.argtypes = [vp, ctypes.c_int, ip, ip, ip]

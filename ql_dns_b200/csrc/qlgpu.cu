@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <functional>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -13,6 +14,7 @@
 #include <vector>
 
 #include "../../include/qlgpu.h"
+#include "qlgpu_handle.h"
 #include "qlgpu_host.h"
 #include "qlgpu_kernel.cuh"
 
@@ -23,48 +25,6 @@ namespace {
 thread_local std::string g_create_error;
 
 }  // namespace
-
-struct qlgpu_handle {
-    qlgpu_params p;
-    DevParams dp;
-    Variant var;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int nxy = 0, nz = 0, NZ = 0, nmf = 0;
-    cplx* d_lin[2] = {nullptr, nullptr};
-    int cur = 0;
-    cplx* d_F1 = nullptr;
-    cplx* d_F2 = nullptr;
-    cplx* d_mf = nullptr;
-    cplx* d_Fmf1 = nullptr;
-    cplx* d_Fmf2 = nullptr;
-    double* d_kx0 = nullptr;
-    double* d_ky = nullptr;
-    int* d_kxi = nullptr;
-    int* d_kyi = nullptr;
-    cplx* d_tw = nullptr;
-    double* d_partials = nullptr;
-    double* d_gpartials = nullptr;
-    DevClock* d_clk = nullptr;
-    double* d_diag = nullptr;
-    int diag_cap = 0;
-    double* d_out15 = nullptr;
-    double* d_linop = nullptr;
-    double* d_ilap2 = nullptr;
-    int tmem_cols = 0;
-    int per_sm = 0;
-    unsigned long long* d_trace = nullptr;
-    double* d_mfr = nullptr;  // [8][NZ] mean-field profile cache
-    double* d_ekz = nullptr;  // [3 stages][2][nz]  // QLGPU_TRACE=1: %globaltimer stamps of each stage
-    int grid = 0, warps = 4, block = 128;
-    size_t smem = 0;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    std::vector<double> kx_tab, ky_tab;
-    std::vector<int> kxi_tab, kyi_tab;
-    std::vector<double> il2_tab, ekz_tab;
-    StageConst sc[3];
-    std::string err;
-};
 
 namespace {
 
@@ -113,7 +73,13 @@ StageArgs base_args(qlgpu_t* h) {
 
 // One RK3 step = three stage launches (RK3CN_Elin::Step / RK3CN::Step).
 // ev (optional): 4 events recorded before stage 1 and after each stage.
-void enqueue_step(qlgpu_t* h, cudaEvent_t* ev = nullptr) {
+}  // namespace
+
+// One RK3 step = three stage launches (RK3CN_Elin::Step / RK3CN::Step).  ev
+// (optional): 4 events recorded before stage 1 and after each stage.  hook
+// (optional) is called before each stage launch with the stage index (the
+// adjoint records the stage inputs there).
+void qlgpu_enqueue_step(qlgpu_t* h, cudaEvent_t* ev, const std::function<void(int)>& hook) {
     cplx* Fbuf[3] = {h->d_F1, h->d_F2, nullptr};
     const cplx* Fprev[3] = {nullptr, h->d_F1, h->d_F2};
     cplx* Fmf[3] = {h->d_Fmf1, h->d_Fmf2, h->d_Fmf1};
@@ -130,11 +96,16 @@ void enqueue_step(qlgpu_t* h, cudaEvent_t* ev = nullptr) {
         A.sc = h->sc[s];
         if (A.trace) A.trace += 32 * s;
         A.ekz_tab = h->d_ekz + (size_t)s * 2 * h->nz;
+        if (hook) hook(s);
         h->var.launch(A, h->dp, h->grid, h->block, h->smem, h->stream);
         if (ev) cudaEventRecord(ev[s + 1], h->stream);
         h->cur ^= 1;
     }
 }
+
+namespace {
+
+void enqueue_step(qlgpu_t* h, cudaEvent_t* ev = nullptr) { qlgpu_enqueue_step(h, ev, nullptr); }
 
 int ensure_diag(qlgpu_t* h, int cap) {
     if (cap <= h->diag_cap) return QLGPU_OK;

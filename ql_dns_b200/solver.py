@@ -121,6 +121,24 @@ class QLSolver:
                     self.h)
         return F, Fm, Lop
 
+    def adjoint_maxwell(self, t0: float, lin0: np.ndarray, mf0: np.ndarray, kx0: np.ndarray | None, nsteps: int,
+                        checkpoint_every: int = 100):
+        """J = mean over nsteps steps of the fluctuation Maxwell stress, and dJ/d lin0, dJ/d mf0
+        (qlgpu_adjoint_maxwell).  Returns (J, grad_lin, grad_mf)."""
+        lin0 = np.ascontiguousarray(lin0, dtype=np.complex128)
+        mf0 = np.ascontiguousarray(mf0, dtype=np.complex128)
+        k = None
+        if kx0 is not None:
+            kx0 = np.ascontiguousarray(kx0, dtype=np.float64)
+            k = _capi.dptr(kx0)
+        J = ctypes.c_double()
+        gl = np.empty_like(lin0)
+        gm = np.empty_like(mf0)
+        _capi.check(self.L.qlgpu_adjoint_maxwell(self.h, float(t0), _capi.dptr(lin0), _capi.dptr(mf0), k, int(nsteps),
+                                                 int(checkpoint_every), ctypes.byref(J), _capi.dptr(gl),
+                                                 _capi.dptr(gm)), self.h)
+        return J.value, gl, gm
+
     def launch_info(self) -> dict:
         a = (ctypes.c_int * 8)()
         _capi.check(self.L.qlgpu_launch_info(self.h, a), self.h)
