@@ -219,8 +219,9 @@ int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms);
  * dynamic shared bytes}; ncta[c] = CTAs that step case c (may be NULL). */
 int qlgpu_batch_mapping(const qlgpu_batch_t* b, int* info4, int* ncta);
 
-/* Fixed mapping: ncta[c] CTAs for case c at `warps` warps per CTA (4 or 8);
- * cases are packed onto the launch's CTAs by the cost model. */
+/* Fixed mapping: ncta[c] CTAs for case c at `warps` warps per CTA (1 up to
+ * the widest CTA that fits the batch's NZ classes); cases are packed onto the
+ * launch's CTAs by the cost model. */
 int qlgpu_batch_set_mapping(qlgpu_batch_t* b, int warps, const int* ncta);
 
 /* Per-case device status words (bits as qlgpu_status) and the launch status

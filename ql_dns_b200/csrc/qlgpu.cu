@@ -185,10 +185,10 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
         h->err = "cudaGetDeviceProperties failed";
         return bail(QLGPU_ERR_CUDA);
     }
-    // CTA width: the number of warps (16 or 8 down to 1, as compiled) that maximises resident
+    // CTA width: the number of warps (up to 16 or 8, as compiled) that maximises resident
     // warps per SM, given shared memory, registers and (for the TMEM store) 512 TMEM columns per SM.
     int best_w = 1, best_res = -1, best_per_sm = 1;
-    for (int w = var.max_warps; w >= 1; w >>= 1) {
+    for (int w = var.max_warps; w >= 1; --w) {
         const size_t sm_bytes = var.smem(w);
         if (sm_bytes > (size_t)prop.sharedMemPerBlockOptin) continue;
         if (ensure_smem_attr(var.kernel(), sm_bytes) !=

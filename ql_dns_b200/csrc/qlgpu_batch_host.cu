@@ -15,8 +15,8 @@
 // count k_c(M) fits and first-fit-decreasing packs all items onto the launch's
 // CTAs.  The autotuner measures the per-case finishing times of probe launches
 // (%globaltimer stamps written by the kernel), fits alpha, beta and r[NZ] by
-// least squares, re-plans, and keeps the fastest measured mapping over the CTA
-// widths 8 and 4 warps.
+// least squares, re-plans, and keeps the fastest measured mapping over two CTA
+// widths: the widest that fits the batch and half of it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -141,6 +141,7 @@ struct qlgpu_batch {
     size_t smem_optin = 0;
     // current mapping
     int warps = 8, per_sm = 1, grid = 0;
+    int wide_warps = 0;  // widest CTA that fits every NZ class of the batch
     size_t smem = 0;
     std::vector<BatchCta> ctas;
     std::vector<int> ncta;
@@ -657,8 +658,17 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
         return bail(QLGPU_ERR_CUDA);
     }
     // initial mapping from the cost model: the widest CTA that fits
-    int rc = plan_and_apply(b, b->bk.max_warps, nullptr);
-    if (rc) rc = plan_and_apply(b, b->bk.max_warps / 2, nullptr);
+    b->wide_warps = 0;
+    for (int w = b->bk.max_warps; w >= 1 && !b->wide_warps; --w) {
+        int ps = 0;
+        size_t sm = 0;
+        if (width_limits(b, w, &ps, &sm)) b->wide_warps = w;
+    }
+    if (!b->wide_warps) {
+        b->err = "batch: no CTA width fits (shared memory / TMEM)";
+        return bail(QLGPU_ERR_UNSUPPORTED);
+    }
+    int rc = plan_and_apply(b, b->wide_warps, nullptr);
     if (rc) return bail(rc);
     rc = upload_descriptors(b);
     if (rc) return bail(rc);
@@ -929,7 +939,7 @@ int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms) {
             if (x[2 + j] > 0) cm.r[j] = x[2 + j];
     };
     int rc = QLGPU_OK;
-    for (int warps : {b->bk.max_warps, b->bk.max_warps / 2}) {
+    for (int warps : {b->wide_warps, std::max(1, b->wide_warps / 2)}) {
         int per_sm = 0;
         size_t smem = 0;
         if (!width_limits(b, warps, &per_sm, &smem)) continue;
@@ -982,10 +992,8 @@ int qlgpu_batch_mapping(const qlgpu_batch_t* b, int* info4, int* ncta) {
 
 int qlgpu_batch_set_mapping(qlgpu_batch_t* b, int warps, const int* ncta) {
     if (!b || !ncta) return QLGPU_ERR_ARG;
-    if (warps != b->bk.max_warps && warps != b->bk.max_warps / 2)
-        return bfail(b, QLGPU_ERR_ARG,
-                     "warps per CTA must be " + std::to_string(b->bk.max_warps) + " or " +
-                         std::to_string(b->bk.max_warps / 2) + " for this batch");
+    if (warps < 1 || warps > b->wide_warps)
+        return bfail(b, QLGPU_ERR_ARG, "warps per CTA must be 1 ... " + std::to_string(b->wide_warps) + " for this batch");
     QB_CK(cudaSetDevice(b->device));
     return plan_and_apply(b, warps, ncta);
 }

@@ -235,6 +235,8 @@ struct Smem {
     static constexpr size_t o_work = o_tot + sizeof(double) * ((PL + 1) & ~1);
     // per pair of groups: BQlin R_uz, R_bz (2 NZ cplx); FullQlin the six components (6 NZ cplx)
     static constexpr size_t GS_BYTES = sizeof(cplx) * G::NZ * (MODEL == MODEL_BQLIN ? 1 : 3);
+    // per pair of groups: the 4 nz fields of the mode being transformed, staged once per mode
+    static constexpr size_t STG_BYTES = sizeof(cplx) * 4 * G::nz;
     __host__ __device__ static size_t work_bytes(int warps) {
         const size_t xch = sizeof(cplx) * (size_t)warps * SW * G::XSIZE;
         const size_t red = sizeof(double) * ((size_t)warps * NEMF * G::NZ + (size_t)warps * 32 * 6);
@@ -242,7 +244,7 @@ struct Smem {
     }
     __host__ __device__ static size_t bytes(int warps) {
         return o_work + work_bytes(warps) + Priv::smem_bytes_per_warp() * (size_t)warps +
-               GS_BYTES * (size_t)warps * SW;
+               GS_BYTES * (size_t)warps * SW + STG_BYTES * (size_t)warps * (SW / 2);
     }
     __host__ __device__ static int tmem_cols(int warps) {
         int need = Priv::tmem_cols_per_warp() * ((warps + 3) / 4);
@@ -323,12 +325,15 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     const int pi = slot >> 1;
     const unsigned pmask = (2 * G::T == 32) ? 0xffffffffu : (((1u << (2 * G::T)) - 1u) << (pi * 2 * G::T));
     PairShared ps;
+    cplx* stg;  // this pair's staged mode fields
     {
         unsigned char* gbase = work + SM::work_bytes(warps) + Priv::smem_bytes_per_warp() * (size_t)warps;
         cplx* k_all = reinterpret_cast<cplx*>(gbase);
         cplx* kpair = k_all + (size_t)(warp * (SW / 2) + pi) * 2 * G::NZ * (MODEL == MODEL_BQLIN ? 1 : 3);
         ps.KU = kpair;
         ps.KB = kpair + G::NZ;
+        cplx* s_all = reinterpret_cast<cplx*>(gbase + SM::GS_BYTES * (size_t)warps * SW);
+        stg = s_all + (size_t)(warp * (SW / 2) + pi) * 4 * G::nz;
     }
     {   // zero the stress accumulators
         cplx z4[4] = {mk(0, 0), mk(0, 0), mk(0, 0), mk(0, 0)};
@@ -409,12 +414,23 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
             l2_prefetch(A.lin_in + (size_t)(mode_raw + WG * PW) * 4 * P.nz, pf_bytes);
             if (pf_prev) l2_prefetch(pf_prev + (size_t)(mode_raw + WG * PW) * 4 * P.nz, pf_bytes);
         }
+        {
+            // stage the mode's 4 nz fields (contiguous, 16-byte aligned) into the pair's buffer:
+            // one round trip per mode instead of one per transform and per update chunk
+            const cplx* src = A.lin_in + (size_t)mode * 4 * P.nz;
+            const int lp = role * G::T + t;  // lane within the pair
+            __syncwarp(pmask);               // the previous mode's readers are done
+            for (int i = lp; i < 4 * G::nz; i += 2 * G::T) cp_async16(stg + i, src + i);
+            cp_async_commit();
+            cp_async_wait_all();
+            __syncwarp(pmask);
+        }
         if constexpr (MODEL == MODEL_BQLIN)
             bqlin_pair<G, INTEG, Priv>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps, pv, tw_s, mfr, tclock,
-                                       cn);
+                                       cn, stg);
         else
             fullqlin_pair<G, INTEG, Priv>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps.KU, pv, tw_s, mfr,
-                                          tclock, cn);
+                                          tclock, cn, stg);
         if (last && valid && role == 0) {
             // ShearingBox_Remap(q t) after t += dt (main.cpp:122-123, MHD_BQlin.cpp:319-329)
             double kx0 = __ldcg(A.kx0 + mode);

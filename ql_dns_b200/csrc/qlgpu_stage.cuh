@@ -32,6 +32,8 @@ __device__ __forceinline__ cplx ldc(const cplx* p) {
     double2 v = __ldcg(reinterpret_cast<const double2*>(p));
     return mk(v.x, v.y);
 }
+// The fields of the mode being transformed, staged in shared memory by its pair.
+__device__ __forceinline__ cplx lds(const cplx* p) { return *p; }
 __device__ __forceinline__ cplx ldc_cg(const cplx* p) {
     double2 v = __ldcg(reinterpret_cast<const double2*>(p));
     return mk(v.x, v.y);
@@ -46,6 +48,13 @@ __device__ __forceinline__ cplx imul(cplx a, double s) { return mk(-a.y * s, a.x
 // registers or shared memory held; bytes a multiple of 16, address 16-aligned).
 __device__ __forceinline__ void l2_prefetch(const void* p, unsigned bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// SM cycle counter, ordered with the surrounding memory operations (trace only)
+__device__ __forceinline__ unsigned long long ctimer() {
+    unsigned long long v;
+    asm volatile("mov.u64 %0, %%clock64;" : "=l"(v)::"memory");
+    return v;
 }
 
 __device__ __forceinline__ unsigned long long gtimer() {
@@ -188,7 +197,7 @@ template <class G, int INTEG, class Priv>
 __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& P, const StageTables& TB, int mode,
                                            bool valid, int role, int t, unsigned gmask, unsigned pmask, cplx* xch,
                                            const PairShared& ps, const Priv& pv, const cplx* tw, const double* mfr,
-                                           double tclock, const CnOld& cn) {
+                                           double tclock, const CnOld& cn, const cplx* stg) {
     constexpr int Pn = G::P;
     const StageConst& S = A.sc;
     const double fac = P.fac;
@@ -202,7 +211,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
     const double ab = __dmul_rn(a, b);
     const double Om2 = __dmul_rn(2.0, P.Omega);
     const double mult = valid ? ((ky == 0.0) ? 1.0 : 2.0) : 0.0;
-    const cplx* __restrict__ u_in = A.lin_in + (size_t)mode * 4 * P.nz;
+    const cplx* __restrict__ u_in = stg;  // this mode's lin_in fields, staged in shared memory
     cplx* u_out = A.lin_out + (size_t)mode * 4 * P.nz;
     const cplx* Fp = (A.Fprev && S.has_prev) ? A.Fprev + (size_t)mode * 4 * P.nz : nullptr;
     cplx* Fo = A.Fout ? A.Fout + (size_t)mode * 4 * P.nz : nullptr;
@@ -236,6 +245,8 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
 #pragma unroll 1
     for (int step = 0; step < 5; ++step) {
         if (tr) A.trace[9 + step] = gtimer();
+        const bool trs = tr && step == 1;  // cycle stamps of the phases of step 1: [23..27]
+        if (trs) A.trace[23] = ctimer();
         // field updated by this group's forward transform at this step (-1: none)
         int fupd = -1;
         if (step == 1) fupd = role ? -2 : 2;  // B: S buffer
@@ -261,11 +272,11 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
                 const int s = stored_index<G>(k);
                 cplx v = mk(0.0, 0.0);
                 if (s >= 0 && kind != 4) {
-                    const cplx g0 = ldc(p0 + s);
+                    const cplx g0 = lds(p0 + s);
                     if (kind == 0) {
                         v = g0;
                     } else {
-                        const cplx g1 = ldc(p1 + s);
+                        const cplx g1 = lds(p1 + s);
                         const double c = kzval(kz_int<G>(k), P.kzL);
                         const double il2 = __ldg(il2row + s);
                         if (kind == 3) {
@@ -280,6 +291,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
             }
             inv_fft<G>(x, xch, tw, t, gmask);
         }
+        if (trs) A.trace[24] = ctimer();
         // ---- real-space products (role-dependent values are selected, not branched:
         // every TMEM access below is executed by the whole warp)
         __syncwarp();
@@ -368,7 +380,9 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
             break;
         }
         // ---- forward transform and the update of one field
+        if (trs) A.trace[25] = ctimer();
         fwd_fft<G>(x, xch, tw, t, gmask);
+        if (trs) A.trace[26] = ctimer();
         __syncwarp();
         if (step == 1) {
             // B keeps fwd(i ky By R_b) for F_u (the U lanes store into their own, unused, buffer)
@@ -376,6 +390,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
             for (int c4 = 0; c4 < Pn / 4; ++c4) pv.st4(PB_S, c4, x + 4 * c4);
             pv.st_fence();
         }
+        if (trs) A.trace[28] = ctimer();
         const int f = fupd;  // field this group updates now (-1/-2: none)
         const int fs = f < 0 ? 0 : f;
         const cplx* __restrict__ fin = u_in + fs * P.nz;
@@ -394,18 +409,20 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
 #pragma unroll
         for (int c4 = 0; c4 < Pn / 4; ++c4) {
             cplx sv[4];
-            __syncwarp();
-            if (step == 3) pv.ld4(PB_S, c4, sv);  // warp-uniform
+            if (step == 3) {  // the TMEM load is warp-wide: reconverge first
+                __syncwarp();
+                pv.ld4(PB_S, c4, sv);
+            }
             if (f < 0 || !valid) continue;
             cplx uin[4], fpv[4], l0[4], l1[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const int s = stored_index<G>(t + G::T * (4 * c4 + i));
                 const int sl = s < 0 ? 0 : s;
-                uin[i] = ldc(fin + sl);
+                uin[i] = lds(fin + sl);
                 fpv[i] = fpp ? ldc(fpp + sl) : mk(0.0, 0.0);
-                l0[i] = ldc(lin0 + sl);
-                l1[i] = ldc(zin + sl);
+                l0[i] = lds(lin0 + sl);
+                l1[i] = lds(zin + sl);
             }
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
@@ -447,6 +464,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
             }
         }
         __syncwarp();
+        if (trs) A.trace[27] = ctimer();
     }
 }
 
@@ -508,7 +526,7 @@ template <class G, int INTEG, class Priv>
 __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParams& P, const StageTables& TB, int mode,
                                               bool valid, int role, int t, unsigned gmask, unsigned pmask, cplx* xch,
                                               cplx* SH, const Priv& pv, const cplx* tw, const double* mfr,
-                                              double tclock, const CnOld& cn) {
+                                              double tclock, const CnOld& cn, const cplx* stg) {
     constexpr int Pn = G::P;
     const StageConst& S = A.sc;
     const double fac = P.fac;
@@ -521,7 +539,7 @@ __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParam
     const double ab = __dmul_rn(a, b);
     const double Om2 = __dmul_rn(2.0, P.Omega);
     const double mult = valid ? ((ky == 0.0) ? 1.0 : 2.0) : 0.0;
-    const cplx* __restrict__ u_in = A.lin_in + (size_t)mode * 4 * P.nz;
+    const cplx* __restrict__ u_in = stg;  // this mode's lin_in fields, staged in shared memory
     cplx* u_out = A.lin_out + (size_t)mode * 4 * P.nz;
     const cplx* Fp = (A.Fprev && S.has_prev) ? A.Fprev + (size_t)mode * 4 * P.nz : nullptr;
     cplx* Fo = A.Fout ? A.Fout + (size_t)mode * 4 * P.nz : nullptr;
@@ -566,12 +584,12 @@ __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParam
                 const int s = stored_index<G>(k);
                 cplx v = mk(0.0, 0.0);
                 if (s >= 0) {
-                    const cplx g0 = ldc(p0 + s);
+                    const cplx g0 = lds(p0 + s);
                     const double c = kzval(kz_int<G>(k), P.kzL);
                     if (kind == 0 || kind == 5) {
                         v = g0;
                     } else {
-                        const cplx g1 = ldc(p1 + s);
+                        const cplx g1 = lds(p1 + s);
                         const double il2 = __ldg(il2row + s);
                         if (kind == 1) v = cscale(csub(cscale(g0, __dmul_rn(a, c)), imul(g1, b)), il2);
                         else v = cscale(cadd(cscale(g0, ab), imul(g1, c)), il2);  // (MHD_FullQlin.cpp:220-221)
@@ -674,8 +692,8 @@ __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParam
                 if (s < 0) continue;
                 const double c = kzval(kz_int<G>(k), P.kzL);
                 const double kz2 = kz2val(c);
-                const cplx u0 = ldc(u_in + s), ze = ldc(u_in + P.nz + s), b0 = ldc(u_in + 2 * P.nz + s),
-                           et = ldc(u_in + 3 * P.nz + s);
+                const cplx u0 = lds(u_in + s), ze = lds(u_in + P.nz + s), b0 = lds(u_in + 2 * P.nz + s),
+                           et = lds(u_in + 3 * P.nz + s);
                 if (step == 3) {
                     // F_b = B0z kz u - s1 (MHD_FullQlin.cpp:303)
                     const cplx F = csub(imul(u0, P.B0z * c), x[k2]);

@@ -95,8 +95,6 @@ def test_batch_equals_single_case_path_bitwise():
             groups.setdefault(info["warps"], []).append((p, st, info["grid"], s.get_state()))
     compared = 0
     for w, items in groups.items():
-        if w not in (16, 8):  # widths a batch of NZ <= 64 cases can run
-            continue
         cs = [it[0] for it in items]
         res, m = run_batch(cs, [it[1] for it in items], 12, diag_every=0, mapping=(w, [it[2] for it in items]))
         assert m["warps"] == w
@@ -112,9 +110,9 @@ def test_batch_mapping_and_width_independent():
     # different CTA counts / widths / packing change only the order of sums over CTAs
     cases = mixed_cases()
     sts = states(cases)
-    a, _ = run_batch(cases, sts, 20, diag_every=0, mapping=(8, [1] * len(cases)))
-    b, mb = run_batch(cases, sts, 20, diag_every=0, mapping=(4, [2, 3, 2, 4, 1, 2, 5]))
-    assert mb["warps"] == 4
+    a, _ = run_batch(cases, sts, 20, diag_every=0, mapping=(6, [1] * len(cases)))
+    b, mb = run_batch(cases, sts, 20, diag_every=0, mapping=(3, [2, 3, 2, 4, 1, 2, 5]))
+    assert mb["warps"] == 3
     for x, y in zip(a, b):
         assert rel(x[1], y[1]) < 1e-12 and rel(x[2], y[2]) < 1e-12
 
@@ -172,7 +170,7 @@ def test_batch_wait_bound_reports_timeout():
     sts = states(cases)
     require_gpu()
     with QLBatch(cases) as b:
-        b.set_mapping(8, [2, 2, 1])
+        b.set_mapping(6, [2, 2, 1])
         for c, (lin, mf, kx0) in enumerate(sts):
             b.set_state(c, 0.0, lin, mf, kx0)
         b.set_wait(0.2)
@@ -182,7 +180,7 @@ def test_batch_wait_bound_reports_timeout():
         assert ei.value.code == 4 and "waiting" in str(ei.value)
         st, ls = b.status()
         assert ls & 8
-        b.set_mapping(8, [2, 2, 1])
+        b.set_mapping(6, [2, 2, 1])
         for c, (lin, mf, kx0) in enumerate(sts):
             b.set_state(c, 0.0, lin, mf, kx0)
         b.step(4)
