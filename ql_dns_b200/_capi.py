@@ -32,7 +32,10 @@ EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "ql
            "qlgpu_batch_last_error",
            "qlgpu_timevars_open", "qlgpu_timevars_save_data", "qlgpu_timevars_save_mean_fields",
            "qlgpu_timevars_close", "qlgpu_fullsave_write", "qlgpu_fullsave_read_latest", "qlgpu_fullsave_times",
-           "qlgpu_io_last_error"]
+           "qlgpu_io_last_error",
+           "qlgpu_dns_create", "qlgpu_dns_destroy", "qlgpu_dns_dims", "qlgpu_dns_set_state", "qlgpu_dns_get_state",
+           "qlgpu_dns_step", "qlgpu_dns_diagnostics", "qlgpu_dns_rhs", "qlgpu_dns_status", "qlgpu_dns_last_error",
+           "qlgpu_dns_step_timed", "qlgpu_dns_stream"]
 
 
 class qlgpu_params(ctypes.Structure):
@@ -45,6 +48,18 @@ class qlgpu_params(ctypes.Structure):
         ("viscosity_order", ctypes.c_int),
         ("dt", ctypes.c_double),
         ("remap", ctypes.c_int), ("quasilinear", ctypes.c_int),
+    ]
+
+
+class qlgpu_dns_params(ctypes.Structure):
+    _fields_ = [
+        ("integrator", ctypes.c_int), ("Mx", ctypes.c_int), ("My", ctypes.c_int), ("NZ", ctypes.c_int),
+        ("L", ctypes.c_double * 3),
+        ("q", ctypes.c_double), ("omega", ctypes.c_double),
+        ("nu", ctypes.c_double), ("eta", ctypes.c_double), ("B0z", ctypes.c_double),
+        ("viscosity_order", ctypes.c_int),
+        ("dt", ctypes.c_double),
+        ("remap", ctypes.c_int), ("dealias_xy", ctypes.c_int),
     ]
 
 
@@ -115,8 +130,21 @@ def load(path: str = LIB_PATH):
     L.qlgpu_fullsave_read_latest.argtypes = [ctypes.c_char_p, ctypes.POINTER(qlgpu_params), dp, dp, dp, dp]
     L.qlgpu_fullsave_times.argtypes = [ctypes.c_char_p, dp, ctypes.c_int, ip]
     L.qlgpu_io_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int]
+    L.qlgpu_dns_create.argtypes = [ctypes.POINTER(qlgpu_dns_params), ctypes.c_int, ctypes.POINTER(vp)]
+    L.qlgpu_dns_destroy.argtypes = [vp]
+    L.qlgpu_dns_dims.argtypes = [vp, ip, ip, ip, ip]
+    L.qlgpu_dns_set_state.argtypes = [vp, ctypes.c_double, dp, dp]
+    L.qlgpu_dns_get_state.argtypes = [vp, dp, dp, dp]
+    L.qlgpu_dns_step.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ip]
+    L.qlgpu_dns_diagnostics.argtypes = [vp, dp]
+    L.qlgpu_dns_rhs.argtypes = [vp, ctypes.c_double, dp]
+    L.qlgpu_dns_status.argtypes = [vp, ip]
+    L.qlgpu_dns_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    L.qlgpu_dns_step_timed.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.qlgpu_dns_stream.argtypes = [vp]
+    L.qlgpu_dns_stream.restype = vp
     for name in EXPORTS:
-        if name not in ("qlgpu_version",):
+        if name not in ("qlgpu_version", "qlgpu_dns_stream"):
             getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -145,6 +173,20 @@ def check_batch(rc: int, b=None):
         L = load()
         buf = ctypes.create_string_buffer(512)
         L.qlgpu_batch_last_error(b, buf, 512)
+        raise QLGPUError(rc, buf.value.decode(errors="replace"))
+
+
+def to_c_dns(p) -> qlgpu_dns_params:
+    return qlgpu_dns_params(p.integrator, p.Mx, p.My, p.NZ, (ctypes.c_double * 3)(*p.L), p.q, p.omega, p.nu, p.eta,
+                            p.B0z, p.viscosity_order, p.dt, p.remap, p.dealias_xy)
+
+
+def check_dns(rc: int, h=None):
+    """As check() for the qlgpu_dns_* entry points (include/qlgpu_dns.h)."""
+    if rc != QLGPU_OK:
+        L = load()
+        buf = ctypes.create_string_buffer(512)
+        L.qlgpu_dns_last_error(h, buf, 512)
         raise QLGPUError(rc, buf.value.decode(errors="replace"))
 
 

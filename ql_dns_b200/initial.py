@@ -92,3 +92,49 @@ def initial_state(p: QLParams, seed: int, sigma: float = 1e-3, B0: float = 0.05,
         mf[2] = hermitian(np.fft.fft(prof.astype(np.complex128))[idx])
         mf[3] = mf[2]
     return np.ascontiguousarray(lin), np.ascontiguousarray(mf), kt["kx"].copy()
+
+
+def dns_initial_state(p, seed: int, sigma: float = 1e-2, B0: float = 0.05):
+    """Seeded initial state of the 3-D DNS (``DNSParams`` p).
+
+    Returns (lin[nxy, 6, nz] c128 = (u_x, u_y, u_z, b_x, b_y, b_z) per mode
+    column, kx0[nxy] f64).  Every (kx, ky, kz) entry of each Cartesian
+    component is a complex Gaussian of physical standard deviation
+    ``sigma |k|^-2`` (PCG64 with the given seed, (mode, component, kz) order),
+    then projected onto the plane normal to k (divergence-free); k = 0 entries
+    and the kx=ky=0 column are zero; ky=0 columns are Hermitian,
+    f(-kx, 0, -kz) = conj f(kx, 0, kz).  The kx=ky=0 column carries the mean
+    field By(z) = B0 sin(2 pi z / Lz), Bx = Ux = Uy = 0.  Stored values are the
+    physical ones times Mx*My*NZ (unnormalised forward transform)."""
+    q = p.ql()
+    kt = ktables(q)
+    nxy, nz = q.nxy, q.nz
+    kx = kt["kx"][:, None]
+    ky = kt["ky"][:, None]
+    kz = kt["kz"][None, :]
+    k2 = kx * kx + ky * ky + kz * kz
+    norm = float(p.Mx * p.My * p.NZ)
+    with np.errstate(divide="ignore"):
+        amp = np.where(k2 > 0, sigma / k2, 0.0) * norm
+    rng = np.random.Generator(np.random.PCG64(seed))
+    g = rng.standard_normal((nxy, 6, nz, 2))
+    lin = (g[..., 0] + 1j * g[..., 1]) * (amp[:, None, :] / np.sqrt(2.0))
+    kv = [np.broadcast_to(kx, k2.shape), np.broadcast_to(ky, k2.shape), np.broadcast_to(kz, k2.shape)]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ik2 = np.where(k2 > 0, 1.0 / k2, 0.0)
+    for base in (0, 3):
+        kdot = sum(kv[c] * lin[:, base + c] for c in range(3))
+        for c in range(3):
+            lin[:, base + c] -= kv[c] * kdot * ik2
+    kxi, kyi = kt["kx_index"], kt["ky_index"]
+    lin[(kxi == 0) & (kyi == 0)] = 0.0
+    flip = (nz - np.arange(nz)) % nz
+    pos = {int(kxi[i]): i for i in range(nxy) if kyi[i] == 0}
+    for i in range(nxy):
+        if kyi[i] == 0 and kxi[i] < 0:
+            lin[i] = np.conj(lin[pos[-int(kxi[i])]][:, flip])
+    zg = np.arange(p.NZ) * (p.L[2] / p.NZ)
+    by = B0 * np.sin(2 * np.pi * zg / p.L[2])
+    idx = dealias_indices(p.NZ, nz)
+    lin[0, 4] = hermitian(np.fft.fft(by.astype(np.complex128))[idx]) * float(p.Mx * p.My)
+    return np.ascontiguousarray(lin), kt["kx"].copy()
