@@ -320,6 +320,68 @@ def run_plain_per_case(cases, sts, local, steps_per_case: int = 10):
             "sample": f"{steps_per_case} steps of each case, one case after another, 3 stage launches per step"}
 
 
+DNS_WORKLOAD = ("full 3-D DNS MRI, MHD shearing box 64x128x64 grid (2/3 dealiased in x, y, z; 1849 (kx,ky) columns x "
+                "nz=43), Re=Rm=4000, dt=0.005, RK3CN_Elin, mean By = 0.05 sin(2 pi z), sigma=1e-2 k^-2 "
+                "divergence-free fluctuations, seed 2")
+
+
+def dns_flops_per_step(p, nxy, Kyn) -> float:
+    """FP64 flops of the transforms of one DNS step, 5 N log2 N per complex transform
+    (6 inverse and 9 forward fields per stage; two real y lines per complex transform)."""
+    import math
+    fz = 5 * p.NZ * math.log2(p.NZ)
+    fx = 5 * p.Mx * math.log2(p.Mx)
+    fy = 5 * p.My * math.log2(p.My)
+    per_rhs = 15 * nxy * fz + 15 * Kyn * p.NZ * fx + 8 * p.Mx * p.NZ * fy
+    return 3 * per_rhs
+
+
+def run_dns(args, local):
+    """The 64x128x64 DNS through QLDns: K steps timed with CUDA events on the handle's stream."""
+    from ql_dns_b200 import _capi
+    from ql_dns_b200.dns import QLDns
+    from ql_dns_b200.initial import dns_initial_state
+    from ql_dns_b200.params import dns_64x128x64
+    import ctypes
+    p = dns_64x128x64()
+    lin, kx0 = dns_initial_state(p, 2, sigma=1e-2, B0=0.05)
+    steps = max(1, min(args.steps, 1000))
+    with QLDns(p, device=local) as d:
+        d.set_state(0.0, lin, kx0)
+        d.step(args.warmup)
+        d.set_state(0.0, lin, kx0)
+        ms = d.step_timed(steps)
+        rec = d.diagnostics()
+        nxy = d.nxy
+        Kyn = d.ny // 2
+    peak = ctypes.c_double()
+    _capi.check(_capi.load().qlgpu_fp64_peak(local, ctypes.byref(peak)))
+    flops = dns_flops_per_step(p, nxy, Kyn)
+    achieved = flops * steps / (ms / 1e3) / 1e12
+    out = {"workload": DNS_WORKLOAD, "value": nxy * steps / (ms / 1e3), "unit": UNIT, "steps": steps,
+           "ms_per_step": ms / steps, "grid_points_per_s": p.Mx * p.My * p.NZ * steps / (ms / 1e3),
+           "l2": "not flushed: the DNS state and transform scratch (~75 MB) stay in L2 across steps, as in a run",
+           "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                        "frac": achieved / peak.value, "peak_source": "measured FP64 FMA loop (qlgpu_fp64_peak)",
+                        "flops_per_step": flops,
+                        "kernels": "dns_inv_zx<64,64>, dns_phys<128>, dns_fwd_xz<64,64>, dns_update (x3 per step)"},
+           "energy_at_end": {"t": rec[0], "E_u": rec[3], "E_b": rec[4], "E_By_mean": rec[2]},
+           "gpu_launches_per_step": 14}
+    if not args.no_cpu_baseline:
+        from oracle.dns_oracle import DNSOracle
+        D = DNSOracle(p)
+        D.step(0.0, lin, kx0)  # warm-up
+        n = 2
+        t0 = time.perf_counter()
+        t, l, k = 0.0, lin, kx0
+        for _ in range(n):
+            t, l, k, _ = D.step(t, l, k)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": nxy * n / dt, "unit": UNIT, "cores": 1, "kind": "port",
+                               "sample": f"{n} steps of the same DNS with the numpy oracle ({dt:.1f} s)"}
+    return out
+
+
 def run_gpu(args):
     import torch
     ws, rank, local = dist_setup()
@@ -391,6 +453,7 @@ def run_gpu(args):
 
     plain = run_plain_per_case(cases, sts, local) if rank == 0 else None
     single = run_single(args, torch.cuda.ExternalStream, local) if rank == 0 else None
+    dns = run_dns(args, local) if rank == 0 else None
 
     out = None
     if rank == 0:
@@ -409,6 +472,7 @@ def run_gpu(args):
             "plain_per_case": plain,
             "speedup_vs_plain_per_case": value / plain["value"],
             "single_case": single,
+            "dns": dns,
             "e2e": e2e,
             "gpu_launches": 2,
         }

@@ -160,6 +160,11 @@ int qlgpu_last_error(const qlgpu_t* h, char* buf, int buflen);
 /* Library version string. */
 const char* qlgpu_version(void);
 
+/* Measured FP64 FMA throughput of a device (TFLOP/s, best of 5 timed launches
+ * of independent FMA chains): the denominator of the FP64 roofline of the 3-D
+ * DNS transforms (include/qlgpu_dns.h).  device < 0: the current device. */
+int qlgpu_fp64_peak(int device, double* tflops);
+
 /* Discrete adjoint (no counterpart in the reference).  For MHD_BQlin with
  * RK3CN_Elin: J = (1/N) sum_{n=1..N} AM_b(t0 + n dt), the fluctuation Maxwell
  * stress of the diagnostic records (MHD_BQlin.cpp:392,424, column 8 of a

@@ -84,20 +84,17 @@ struct InvZX {
     static constexpr int XZ = (BLOCK / GZ::T) * GZ::XSIZE;
     static constexpr int XX = (BLOCK / GX::T) * GX::XSIZE;
     static constexpr int XCH = XZ > XX ? XZ : XX;
-    static size_t smem(int ncol) {
-        return sizeof(cplx) * ((size_t)ncol * SROW + (size_t)MX * SROW + XCH) + sizeof(int) * MX;
-    }
+    static size_t smem(int ncol) { return sizeof(cplx) * ((size_t)ncol * SROW + XCH) + sizeof(int) * MX; }
 };
 
 template <int NZ, int MX>
-__global__ void __launch_bounds__(BLOCK) dns_inv_zx(DnsArgs a) {
+__global__ void __launch_bounds__(BLOCK, 2) dns_inv_zx(DnsArgs a) {
     using K = InvZX<NZ, MX>;
     using GZ = typename K::GZ;
     using GX = typename K::GX;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx* S = reinterpret_cast<cplx*>(smraw);
-    cplx* O = S + (size_t)a.ncol * K::SROW;
-    cplx* xch = O + (size_t)MX * K::SROW;
+    cplx* xch = S + (size_t)a.ncol * K::SROW;
     int* bin2col = reinterpret_cast<int*>(xch + K::XCH);
     const int ky = blockIdx.x, f = blockIdx.y, tid = threadIdx.x;
     for (int b = tid; b < MX; b += BLOCK) bin2col[b] = -1;
@@ -123,11 +120,13 @@ __global__ void __launch_bounds__(BLOCK) dns_inv_zx(DnsArgs a) {
         }
     }
     __syncthreads();
-    {  // x inverse of every z row
+    {  // x inverse of every z row, stored to X[f][ky][x][z]: the groups of a warp take
+       // consecutive z, so each store instruction writes whole 32-byte sectors
         constexpr int T = GX::T, NG = BLOCK / T;
         const int g = tid / T, t = tid % T;
         const unsigned gm = group_mask(T);
         cplx* xg = xch + g * GX::XSIZE;
+        cplx* dst = a.X + ((size_t)f * a.Kyn + ky) * MX * NZ;
         for (int z = g; z < NZ; z += NG) {
             cplx x[GX::P];
 #pragma unroll
@@ -137,12 +136,9 @@ __global__ void __launch_bounds__(BLOCK) dns_inv_zx(DnsArgs a) {
             }
             inv_fft<GX>(x, xg, a.twx, t, gm);
 #pragma unroll
-            for (int j = 0; j < GX::P; ++j) O[zpos<GX>(t, j) * K::SROW + z] = x[j];
+            for (int j = 0; j < GX::P; ++j) dst[(size_t)zpos<GX>(t, j) * NZ + z] = x[j];
         }
     }
-    __syncthreads();
-    cplx* dst = a.X + ((size_t)f * a.Kyn + ky) * MX * NZ;
-    for (int i = tid; i < MX * NZ; i += BLOCK) dst[i] = O[(i / NZ) * K::SROW + (i % NZ)];
 }
 
 // ---------------------------------------------------------------------------
@@ -265,29 +261,26 @@ struct FwdXZ {
     static constexpr int XZ = (BLOCK / GZ::T) * GZ::XSIZE;
     static constexpr int XX = (BLOCK / GX::T) * GX::XSIZE;
     static constexpr int XCH = XZ > XX ? XZ : XX;
-    static size_t smem(int ncol) {
-        return sizeof(cplx) * ((size_t)ncol * SROW + (size_t)MX * SROW + XCH) + sizeof(int) * MX;
-    }
+    static size_t smem(int ncol) { return sizeof(cplx) * ((size_t)ncol * SROW + XCH) + sizeof(int) * MX; }
 };
 
 template <int MX, int NZ>
-__global__ void __launch_bounds__(BLOCK) dns_fwd_xz(DnsArgs a) {
+__global__ void __launch_bounds__(BLOCK, 2) dns_fwd_xz(DnsArgs a) {
     using K = FwdXZ<MX, NZ>;
     using GZ = typename K::GZ;
     using GX = typename K::GX;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx* S = reinterpret_cast<cplx*>(smraw);
-    cplx* Pt = S + (size_t)a.ncol * K::SROW;
-    cplx* xch = Pt + (size_t)MX * K::SROW;
+    cplx* xch = S + (size_t)a.ncol * K::SROW;
     int* bin2col = reinterpret_cast<int*>(xch + K::XCH);
     const int ky = blockIdx.x, p = blockIdx.y, tid = threadIdx.x;
     for (int b = tid; b < MX; b += BLOCK) bin2col[b] = -1;
     const cplx* src = a.P + ((size_t)p * a.Kyn + ky) * MX * NZ;
-    for (int i = tid; i < MX * NZ; i += BLOCK) Pt[(i / NZ) * K::SROW + (i % NZ)] = src[i];
     __syncthreads();
     for (int c = tid; c < a.ncol; c += BLOCK) bin2col[xbin(a.kx0[ky + a.Kyn * c], a.dkx, MX)] = c;
     __syncthreads();
-    {  // x forward of every z row, kept at the plane's column bins
+    {  // x forward of every z row (loads: consecutive z per warp, whole sectors), kept at
+       // the plane's column bins
         constexpr int T = GX::T, NG = BLOCK / T;
         const int g = tid / T, t = tid % T;
         const unsigned gm = group_mask(T);
@@ -295,7 +288,7 @@ __global__ void __launch_bounds__(BLOCK) dns_fwd_xz(DnsArgs a) {
         for (int z = g; z < NZ; z += NG) {
             cplx x[GX::P];
 #pragma unroll
-            for (int j = 0; j < GX::P; ++j) x[j] = Pt[zpos<GX>(t, j) * K::SROW + z];
+            for (int j = 0; j < GX::P; ++j) x[j] = src[(size_t)zpos<GX>(t, j) * NZ + z];
             fwd_fft<GX>(x, xg, a.twx, t, gm);
 #pragma unroll
             for (int k2 = 0; k2 < GX::P; ++k2) {
