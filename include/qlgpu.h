@@ -160,6 +160,26 @@ int qlgpu_last_error(const qlgpu_t* h, char* buf, int buflen);
 /* Library version string. */
 const char* qlgpu_version(void);
 
+/* Driving noise after every step (Model::DrivingNoise, QL_DNS/Models/
+ * MHD_BQlin.cpp:558-618, called by main.cpp:112-113 when f_noise != 0):
+ * modes with ky != 0 and k_low < |k| < k_high get complex normal increments
+ * of standard deviation f_noise/sqrt(2) per part, scaled as the reference.
+ * The reference's clock-seeded mt19937 (MHD_BQlin.cpp:22) is replaced by one
+ * Philox4x32-10 counter per (step since set_state, mode, kz, field) under
+ * `seed`.  f_noise = 0 turns it off.  MHD_BQlin only (QLGPU_ERR_UNSUPPORTED
+ * otherwise). */
+int qlgpu_set_noise(qlgpu_t* h, double f_noise, double k_low, double k_high, unsigned long long seed);
+
+/* Variable time step (RK3CN_Elin.cpp:76-80; RK3CN.cpp alike): cfl > 0 makes
+ * every step dt = cfl / Calculate_CFL (MHD_BQlin.cpp:540-552,
+ * MHD_FullQlin.cpp:769-780), capped at dt_max (the reference's -dt input).
+ * With noise or cfl set, qlgpu_step writes a record after every diag_every-th
+ * step.  cfl = 0 restores the fixed dt of the parameters. */
+int qlgpu_set_cfl(qlgpu_t* h, double cfl, double dt_max);
+
+/* Integrator::mean_time_step(): mean dt of the steps since set_state. */
+int qlgpu_mean_time_step(qlgpu_t* h, double* dt_mean);
+
 /* Measured FP64 FMA throughput of a device (TFLOP/s, best of 5 timed launches
  * of independent FMA chains): the denominator of the FP64 roofline of the 3-D
  * DNS transforms (include/qlgpu_dns.h).  device < 0: the current device. */

@@ -57,6 +57,11 @@ def lib(kind: str = "strict"):
     L.oracle_fft.argtypes = [ctypes.c_int, ctypes.c_int, dp]
     L.oracle_tlm_maxwell.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_double, dp, dp, dp, dp, dp,
                                      ctypes.c_int, dp, dp]
+    L.oracle_run_forced.argtypes = [ctypes.POINTER(OracleParams), dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, dp,
+                                    ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_ulonglong, dp]
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    L.oracle_philox.argtypes = [u32p, u32p, u32p]
     _LIBS[kind] = L
     return L
 
@@ -112,6 +117,33 @@ def run(p, t0, lin, mf, kx0, nsteps, diag_every=0, kind: str = "strict", nthread
     n = lib(kind).oracle_run(ctypes.byref(pp), _dp(t), _dp(lin), _dp(mf), _dp(kx0), nsteps,
                              diag_every, _dp(diag), maxd)
     return float(t[0]), lin, mf, kx0, diag[:n]
+
+
+def run_forced(p, t0, lin, mf, kx0, nsteps, diag_every=0, cfl=0.0, dt_max=0.0, f_noise=0.0, k_lo=0.0,
+               k_hi=0.0, seed=0, kind: str = "strict"):
+    """main.cpp loop with variable dt (cfl > 0) and driving noise (f_noise != 0); a
+    record after every diag_every-th step -> (t, lin, mf, kx0, diag[nrec, 15], dt_mean)."""
+    lin = np.ascontiguousarray(lin, dtype=np.complex128).copy()
+    mf = np.ascontiguousarray(mf, dtype=np.complex128).copy()
+    kx0 = np.ascontiguousarray(kx0, dtype=np.float64).copy()
+    t = np.array([t0], dtype=np.float64)
+    maxd = (nsteps + 2) if diag_every > 0 else 1
+    diag = np.zeros((maxd, 15))
+    dtm = np.zeros(1)
+    pp = _params(p)
+    n = lib(kind).oracle_run_forced(ctypes.byref(pp), _dp(t), _dp(lin), _dp(mf), _dp(kx0), nsteps, diag_every,
+                                    _dp(diag), maxd, cfl, dt_max, f_noise, k_lo, k_hi, seed, _dp(dtm))
+    return float(t[0]), lin, mf, kx0, diag[:n], float(dtm[0])
+
+
+def philox(ctr, key, kind: str = "strict"):
+    """Philox4x32-10 of one counter (4 x uint32) under a key (2 x uint32)."""
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    lib(kind).oracle_philox(c.ctypes.data_as(u32p), k.ctypes.data_as(u32p), out.ctypes.data_as(u32p))
+    return out
 
 
 def tlm_maxwell(p, t0, lin, mf, kx0, dlin, dmf=None, nsteps: int = 1, kind: str = "strict"):

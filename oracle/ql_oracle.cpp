@@ -24,7 +24,9 @@
 //                         (CPU baseline timing, mirrors SConstruct:6 flags and
 //                          stands in for the MPI mode split MPIdata.cpp:30-33)
 
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -265,6 +267,33 @@ static void assign_laplacians(const OracleParams& p, const Dims& d, const Kd& K,
 // ---------------------------------------------------------------------------
 // Model: right-hand sides
 // ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter (c0..c3), key (k0, k1).
+static void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    for (int r = 0; r < 10; ++r) {
+        if (r > 0) { k0 += W0; k1 += W1; }
+        const uint64_t p0 = (uint64_t)M0 * c[0], p1 = (uint64_t)M1 * c[2];
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+    }
+}
+
+// Two standard normals from the counter (a, b, step) under key seed: Box-Muller
+// on two 53-bit uniforms, u1 in (0, 1), u2 in [0, 1).
+static void philox_normal_pair(unsigned long long seed, unsigned long long step, uint32_t a, uint32_t b,
+                               double* z1, double* z2) {
+    uint32_t c[4] = {a, b, (uint32_t)step, (uint32_t)(step >> 32)};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint64_t x = ((uint64_t)c[0] << 32) | c[1], y = ((uint64_t)c[2] << 32) | c[3];
+    const double u1 = ((double)(x >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    const double u2 = (double)(y >> 11) * (1.0 / 9007199254740992.0);
+    const double r = std::sqrt(-2.0 * std::log(u1));
+    *z1 = r * std::cos(2.0 * PI_ * u2);
+    *z2 = r * std::sin(2.0 * PI_ * u2);
+}
+
 struct Model {
     OracleParams p;
     Dims d;
@@ -274,6 +303,10 @@ struct Model {
     long totalN2;
     int num_to_send;
     int nthreads;
+    // max |profile|^2 over the NZ grid of the real-space mean fields of the last
+    // rhs call's input (By_ / MBx_, MBy_, MUx_, MUy_ members, zero before the
+    // first call: MHD_BQlin.cpp:105, MHD_FullQlin.cpp:151); Calculate_CFL reads them
+    double mf_max2[4] = {0, 0, 0, 0};
     Model(const OracleParams& pp)
         : p(pp), d(make_dims(pp)), K(make_kdata(pp, d)), fft(pp.NZ, d.nz) {
         reynolds_stress_ft_fac = 1.0 / (d.Ny * d.Nx) / (d.Ny * d.Nx);  // MHD_BQlin.cpp:56
@@ -284,6 +317,59 @@ struct Model {
 #ifdef _OPENMP
         nthreads = p.nthreads > 0 ? p.nthreads : omp_get_max_threads();
 #endif
+    }
+
+    static double max_abs2(const cvec& v) {
+        double m = 0;
+        for (const cd& x : v) m = std::max(m, std::norm(x));
+        return m;
+    }
+
+    // Calculate_CFL: MHD_BQlin.cpp:540-552 (By from the last rhs, Bx from sol),
+    // MHD_FullQlin.cpp:769-780 (all four from the last rhs); kmax of
+    // MHD_BQlin.cpp:69-74 (dealias factors 2, 2, 3).
+    double calculate_cfl(const State& sol) const {
+        const double Ns[3] = {(double)d.Nx, (double)d.Ny, (double)d.NZ};
+        const double dealias[3] = {2.0, 2.0, 3.0};
+        double kmax = 0;
+        for (int i = 0; i < 3; ++i) kmax = std::max(kmax, 2 * PI_ / p.L[i] * (Ns[i] / dealias[i]));
+        if (p.model == 1)
+            return kmax * (std::sqrt(mf_max2[1]) + std::sqrt(mf_max2[0]) + std::sqrt(mf_max2[2]) +
+                           std::sqrt(mf_max2[3])) + p.q;
+        cvec tmp(d.nz), bx(d.NZ);
+        for (int k = 0; k < d.nz; ++k) tmp[k] = sol.pMF(0)[k] * fft.fac;
+        fft.inverse(tmp.data(), bx.data());
+        return kmax * std::sqrt(mf_max2[1]) + kmax * std::sqrt(max_abs2(bx)) + p.q;
+    }
+
+    // DrivingNoise of MHD_BQlin (MHD_BQlin.cpp:558-618; ky = 0 modes are not
+    // driven, dont_drive_ky0_modes_ = 1 at :18).  The reference draws from a
+    // clock-seeded mt19937 (:22-23); here every (step, mode, kz, field) has its
+    // own Philox4x32-10 counter and Box-Muller pair, so runs are reproducible
+    // and the GPU draws the same numbers.
+    void driving_noise(double t, double dt, State& sol, const std::vector<double>& kx0, double f_noise,
+                       double k_lo, double k_hi, unsigned long long seed, unsigned long long step) {
+        const double lo2 = k_lo * k_lo, hi2 = k_hi * k_hi;
+        const double mult_noise_fac = (1.0 / (16 * 32 * 32)) * (1.0 / (16 * 32 * 32));  // :35-36
+        const double multfac = dt * (double)totalN2 * mult_noise_fac;
+        const double sd = f_noise / std::sqrt(2.0);
+        for (int i = 0; i < d.nxy; ++i) {
+            if (K.ky_index[i] == 0) continue;
+            ModeK m;
+            assign_laplacians(p, d, K, kx0, i, t, false, m);
+            for (int k = 0; k < d.nz; ++k) {
+                const double lapF = m.lapF[k], lap2 = m.lap2[k];
+                if (!(lapF > -hi2 && lapF < -lo2)) continue;
+                const double mu = std::sqrt(multfac * lap2 / lapF);
+                const double mz = std::sqrt(-multfac * lap2);
+                for (int v = 0; v < 4; ++v) {
+                    double z1, z2;
+                    philox_normal_pair(seed, step, (unsigned)i, (unsigned)(4 * k + v), &z1, &z2);
+                    const double mult = (v == 0 || v == 2) ? mu : mz;
+                    sol.pLin(i, v)[k] += mult * cd(z1 * sd, z2 * sd);
+                }
+            }
+        }
     }
 
     // MHD_BQlin::rhs, MHD_BQlin.cpp:117-284.  kx0 holds the (possibly remapped)
@@ -301,6 +387,7 @@ struct Model {
         fft.inverse(tmp.data(), dzBy.data());
         for (int k = 0; k < nz; ++k) tmp[k] = fac * K.kz2[k] * in.pMF(1)[k];
         fft.inverse(tmp.data(), dzdzBy.data());
+        mf_max2[1] = max_abs2(By);
 
         std::vector<cvec> send_thr(nthreads, cvec(2 * num_to_send, 0.0));
 #ifdef _OPENMP
@@ -445,6 +532,7 @@ struct Model {
             fft.inverse(tmp.data(), MF[m].data());
             for (int k = 0; k < nz; ++k) tmp[k] = fac * K.kz[k] * in.pMF(m)[k];
             fft.inverse(tmp.data(), dzMF[m].data());
+            mf_max2[m] = max_abs2(MF[m]);
         }
         const cvec &MBx = MF[0], &MBy = MF[1], &MUx = MF[2], &MUy = MF[3];
         const cvec &dzMBx = dzMF[0], &dzMBy = dzMF[1], &dzMUx = dzMF[2], &dzMUy = dzMF[3];
@@ -944,6 +1032,61 @@ int oracle_run(const OracleParams* p, double* t_io, double* lin_io, double* mf_i
     std::memcpy(mf_io, s.mf.data(), s.mf.size() * sizeof(cd));
     std::memcpy(kx0_io, kx0.data(), kx0.size() * sizeof(double));
     return nrec;
+}
+
+// The main loop with forcing (main.cpp:108-133): optional variable dt
+// (RK3CN_Elin.cpp:76-80: dt = cfl / Calculate_CFL, capped at dt_max) and
+// driving noise after every step (main.cpp:112-113), then t += dt and the
+// remap.  A diagnostic record after every diag_every-th step (and the initial
+// one).  Returns the record count; *dt_mean_out = Integrator::mean_time_step.
+int oracle_run_forced(const OracleParams* p, double* t_io, double* lin_io, double* mf_io, double* kx0_io,
+                      int nsteps, int diag_every, double* diag_out, int max_diag, double cfl, double dt_max,
+                      double f_noise, double k_lo, double k_hi, unsigned long long seed, double* dt_mean_out) {
+    Model M(*p);
+    State s;
+    s.init(M.d);
+    std::memcpy(s.lin.data(), lin_io, s.lin.size() * sizeof(cd));
+    std::memcpy(s.mf.data(), mf_io, s.mf.size() * sizeof(cd));
+    std::vector<double> kx0(kx0_io, kx0_io + M.d.nxy);
+    double t = *t_io;
+    Integrator I(M, t, kx0);
+    int nrec = 0;
+    auto record = [&](double tt) {
+        if (diag_every > 0 && diag_out && nrec < max_diag) {
+            diag_out[nrec * 15] = tt;
+            M.diagnostics(tt, s, kx0, diag_out + nrec * 15 + 1);
+            ++nrec;
+        }
+    };
+    record(t);
+    double dt_sum = 0;
+    for (int n = 0; n < nsteps; ++n) {
+        double dt = p->dt;
+        if (cfl > 0) {
+            dt = cfl / M.calculate_cfl(s);
+            if (dt > dt_max) dt = dt_max;
+        }
+        I.step(t, dt, s, kx0);
+        dt_sum += dt;
+        if (f_noise != 0.0) M.driving_noise(t, dt, s, kx0, f_noise, k_lo, k_hi, seed, (unsigned long long)n);
+        t += dt;
+        if (p->remap) M.remap(p->q * t, s, kx0);
+        if (diag_every > 0 && (n + 1) % diag_every == 0) record(t);
+    }
+    *t_io = t;
+    if (dt_mean_out) *dt_mean_out = nsteps > 0 ? dt_sum / nsteps : 0.0;
+    std::memcpy(lin_io, s.lin.data(), s.lin.size() * sizeof(cd));
+    std::memcpy(mf_io, s.mf.data(), s.mf.size() * sizeof(cd));
+    std::memcpy(kx0_io, kx0.data(), kx0.size() * sizeof(double));
+    return nrec;
+}
+
+// Philox4x32-10 of one counter (known-answer tests of the generator).
+int oracle_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+    uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+    philox4x32_10(c, key[0], key[1]);
+    for (int i = 0; i < 4; ++i) out[i] = c[i];
+    return 0;
 }
 
 // Tangent-linear run for MHD_BQlin / RK3CN_Elin (the checker of the adjoint).

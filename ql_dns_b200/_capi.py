@@ -35,7 +35,8 @@ EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "ql
            "qlgpu_io_last_error",
            "qlgpu_dns_create", "qlgpu_dns_destroy", "qlgpu_dns_dims", "qlgpu_dns_set_state", "qlgpu_dns_get_state",
            "qlgpu_dns_step", "qlgpu_dns_diagnostics", "qlgpu_dns_rhs", "qlgpu_dns_status", "qlgpu_dns_last_error",
-           "qlgpu_dns_step_timed", "qlgpu_dns_stream", "qlgpu_fp64_peak"]
+           "qlgpu_dns_step_timed", "qlgpu_dns_stream", "qlgpu_fp64_peak",
+           "qlgpu_set_noise", "qlgpu_set_cfl", "qlgpu_mean_time_step"]
 
 
 class qlgpu_params(ctypes.Structure):
@@ -144,6 +145,9 @@ def load(path: str = LIB_PATH):
     L.qlgpu_dns_stream.argtypes = [vp]
     L.qlgpu_dns_stream.restype = vp
     L.qlgpu_fp64_peak.argtypes = [ctypes.c_int, dp]
+    L.qlgpu_set_noise.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong]
+    L.qlgpu_set_cfl.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+    L.qlgpu_mean_time_step.argtypes = [vp, dp]
     for name in EXPORTS:
         if name not in ("qlgpu_version", "qlgpu_dns_stream"):
             getattr(L, name).restype = ctypes.c_int

@@ -3,6 +3,7 @@
 // bookkeeping of QL_DNS/main.cpp:108-133.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <functional>
@@ -17,6 +18,7 @@
 #include "qlgpu_handle.h"
 #include "qlgpu_host.h"
 #include "qlgpu_kernel.cuh"
+#include "qlgpu_forcing.cuh"
 
 using namespace qlgpu;
 
@@ -95,7 +97,7 @@ void qlgpu_enqueue_step(qlgpu_t* h, cudaEvent_t* ev, const std::function<void(in
         A.Fmf_out = (s < 2) ? Fmf[s] : nullptr;
         A.sc = h->sc[s];
         if (A.trace) A.trace += 32 * s;
-        A.ekz_tab = h->d_ekz + (size_t)s * 2 * h->nz;
+        A.ekz_tab = h->ekz_dynamic ? nullptr : h->d_ekz + (size_t)s * 2 * h->nz;
         if (hook) hook(s);
         h->var.launch(A, h->dp, h->grid, h->block, h->smem, h->stream);
         if (ev) cudaEventRecord(ev[s + 1], h->stream);
@@ -312,7 +314,7 @@ int qlgpu_destroy(qlgpu_t* h) {
     void* bufs[] = {h->d_lin[0], h->d_lin[1], h->d_F1, h->d_F2, h->d_mf, h->d_Fmf1, h->d_Fmf2,
                     h->d_kx0, h->d_ky, h->d_kxi, h->d_kyi, h->d_tw, h->d_partials, h->d_gpartials,
                     h->d_clk, h->d_diag, h->d_out15, h->d_linop, h->d_ilap2, h->d_trace,
-                    h->d_mfr, h->d_ekz};
+                    h->d_mfr, h->d_ekz, h->d_forcing, h->d_kx0_prev};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : h->ev)
@@ -344,6 +346,10 @@ static int set_state_impl(qlgpu_t* h, double t, const void* lin, const void* mf,
                                  h->stream));
     int rc = reset_clock(h, t);
     if (rc) return rc;
+    // the integrator and model start afresh: no steps, zero mean-field profiles of a previous rhs
+    h->dt_sum = 0.0;
+    h->steps_taken = 0;
+    if (h->d_forcing) QLGPU_CK(cudaMemsetAsync(h->d_forcing, 0, 9 * sizeof(double), h->stream));
     QLGPU_CK(cudaStreamSynchronize(h->stream));
     return QLGPU_OK;
 }
@@ -375,11 +381,142 @@ int qlgpu_get_state_device(qlgpu_t* h, double* t, void* lin, void* mf, void* kx0
     return get_state_impl(h, t, lin, mf, kx0, cudaMemcpyDeviceToDevice);
 }
 
+// Steps with driving noise and / or the CFL time step (main.cpp:108-133 with
+// RK3CN_Elin.cpp:76-80): per step the host reads the mean-field maxima, sets dt
+// and the stage constants, enqueues the three stages (the stage-3 input's
+// maxima are taken before stage 3: the profiles the last rhs computed), then
+// the noise; a record after every diag_every-th step through diag_kernel.
+static int step_forced(qlgpu_t* h, int nsteps, int diag_every, double* diag_out, int max_diag, int* ndiag) {
+    if (!h->d_forcing) {
+        QLGPU_CK(cudaMalloc(&h->d_forcing, 9 * sizeof(double)));
+        QLGPU_CK(cudaMemsetAsync(h->d_forcing, 0, 9 * sizeof(double), h->stream));
+    }
+    if (h->noise_f != 0.0 && !h->d_kx0_prev) QLGPU_CK(cudaMalloc(&h->d_kx0_prev, h->nxy * sizeof(double)));
+    if (diag_every > 0) {
+        int rc = ensure_diag(h, max_diag > 0 ? max_diag : 1);
+        if (rc) return rc;
+    }
+    const double fac = 1.0 / h->NZ;  // fftwPlans.cpp:30
+    const double Ns[3] = {(double)h->p.nx, (double)((h->p.ny / 2) * 2), (double)h->NZ};
+    const double dealias[3] = {2.0, 2.0, 3.0};
+    double kmax = 0;  // MHD_BQlin.cpp:69-74
+    for (int i = 0; i < 3; ++i) kmax = std::max(kmax, 2 * kPI / h->p.L[i] * (Ns[i] / dealias[i]));
+    double t = 0;
+    QLGPU_CK(cudaMemcpyAsync(&t, &h->d_clk->t, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    const double tv_saved = h->dp.tv_interval;
+    h->dp.tv_interval = 0.0;  // records come from diag_kernel here
+    h->ekz_dynamic = h->cfl > 0;
+    const long tot = (long)h->p.nx * ((h->p.ny / 2) * 2) * h->NZ;
+    const double mult_noise_fac = (1.0 / (16 * 32 * 32)) * (1.0 / (16 * 32 * 32));  // MHD_BQlin.cpp:35-36
+    int nd = 0, rc = QLGPU_OK;
+    for (int n = 0; n < nsteps && rc == QLGPU_OK; ++n) {
+        double dt = h->p.dt;
+        if (h->cfl > 0) {
+            mf_absmax2_kernel<<<1, 256, 0, h->stream>>>(h->d_mf, 1, h->nz, h->NZ, fac, h->d_forcing + 4);
+            double m[8];
+            QLGPU_CK(cudaMemcpyAsync(m, h->d_forcing, sizeof(m), cudaMemcpyDeviceToHost, h->stream));
+            QLGPU_CK(cudaStreamSynchronize(h->stream));
+            const double c = h->p.model == QLGPU_MODEL_MHD_BQLIN
+                                 ? kmax * std::sqrt(m[1]) + kmax * std::sqrt(m[4]) + h->p.q
+                                 : kmax * (std::sqrt(m[1]) + std::sqrt(m[0]) + std::sqrt(m[2]) + std::sqrt(m[3])) +
+                                       h->p.q;
+            dt = h->cfl / c;  // RK3CN_Elin.cpp:77-79
+            if (dt > h->dt_max) dt = h->dt_max;
+        }
+        qlgpu_params pp = h->p;
+        pp.dt = dt;
+        h->dp.dt = dt;
+        for (int s = 0; s < 3; ++s) h->sc[s] = stage_const(pp, s);
+        if (h->noise_f != 0.0) {
+            QLGPU_CK(cudaMemcpyAsync(h->d_kx0_prev, h->d_kx0, h->nxy * sizeof(double), cudaMemcpyDeviceToDevice,
+                                     h->stream));
+        }
+        qlgpu_enqueue_step(h, nullptr, [&](int s) {
+            if (s == 2 && h->cfl > 0)
+                mf_absmax2_kernel<<<1, 256, 0, h->stream>>>(h->d_mf, h->nmf, h->nz, h->NZ, fac, h->d_forcing);
+        });
+        if (h->noise_f != 0.0) {
+            NoiseArgs a;
+            a.lin = h->d_lin[h->cur];
+            a.kx0_prev = h->d_kx0_prev;
+            a.kx0_now = h->d_kx0;
+            a.ky = h->d_ky;
+            a.kyi = h->d_kyi;
+            a.nxy = h->nxy;
+            a.nz = h->nz;
+            a.q = h->p.q;
+            a.t = t;
+            a.kzL = 2 * kPI / h->p.L[2];
+            a.lo2 = h->noise_klo * h->noise_klo;
+            a.hi2 = h->noise_khi * h->noise_khi;
+            a.multfac = dt * (double)tot * (double)tot * mult_noise_fac;
+            a.sd = h->noise_f / std::sqrt(2.0);
+            a.seed = h->noise_seed;
+            a.step = h->steps_taken;
+            const int n_el = h->nxy * h->nz;
+            noise_kernel<<<(n_el + 255) / 256, 256, 0, h->stream>>>(a);
+        }
+        t = t + dt;  // main.cpp:116, the device clock's sum
+        h->dt_sum += dt;
+        ++h->steps_taken;
+        if (diag_every > 0 && (n + 1) % diag_every == 0 && nd < max_diag) {
+            h->var.diag(h->d_lin[h->cur], h->d_mf, h->d_kx0, h->d_ky, h->d_kxi, h->d_kyi, h->dp, t,
+                        h->d_diag + 15 * (size_t)nd, h->stream);
+            ++nd;
+        }
+        rc = check_launch(h);
+    }
+    h->dp.tv_interval = tv_saved;
+    h->dp.dt = h->p.dt;
+    for (int s = 0; s < 3; ++s) h->sc[s] = stage_const(h->p, s);
+    h->ekz_dynamic = false;
+    if (rc) return rc;
+    DevClock c;
+    QLGPU_CK(cudaMemcpyAsync(&c, h->d_clk, sizeof(DevClock), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    if (nd > 0) QLGPU_CK(cudaMemcpy(diag_out, h->d_diag, sizeof(double) * 15 * (size_t)nd, cudaMemcpyDeviceToHost));
+    if (ndiag) *ndiag = nd;
+    if (c.status & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE))
+        return fail(h, QLGPU_ERR_STATUS, "device status set: non-finite or unstable solution");
+    return QLGPU_OK;
+}
+
+int qlgpu_set_noise(qlgpu_t* h, double f_noise, double k_low, double k_high, unsigned long long seed) {
+    if (!h) return QLGPU_ERR_ARG;
+    if (!std::isfinite(f_noise) || !(k_low >= 0) || !(k_high >= k_low))
+        return fail(h, QLGPU_ERR_ARG, "noise: finite f_noise, 0 <= k_low <= k_high");
+    if (f_noise != 0.0 && h->p.model != QLGPU_MODEL_MHD_BQLIN)
+        return fail(h, QLGPU_ERR_UNSUPPORTED, "driving noise is built for MHD_BQlin");
+    h->noise_f = f_noise;
+    h->noise_klo = k_low;
+    h->noise_khi = k_high;
+    h->noise_seed = seed;
+    return QLGPU_OK;
+}
+
+int qlgpu_set_cfl(qlgpu_t* h, double cfl, double dt_max) {
+    if (!h) return QLGPU_ERR_ARG;
+    if (!(cfl >= 0) || (cfl > 0 && !(dt_max > 0))) return fail(h, QLGPU_ERR_ARG, "cfl >= 0 and dt_max > 0");
+    h->cfl = cfl;
+    h->dt_max = dt_max;
+    return QLGPU_OK;
+}
+
+int qlgpu_mean_time_step(qlgpu_t* h, double* dt_mean) {
+    if (!h || !dt_mean) return QLGPU_ERR_ARG;
+    *dt_mean = h->steps_taken ? h->dt_sum / (double)h->steps_taken : h->p.dt;
+    return QLGPU_OK;
+}
+
 int qlgpu_step(qlgpu_t* h, int nsteps, int diag_every, double* diag_out, int max_diag, int* ndiag) {
     if (!h) return QLGPU_ERR_ARG;
     if (nsteps < 0) return fail(h, QLGPU_ERR_ARG, "nsteps < 0");
     if (diag_every > 0 && (!diag_out || max_diag < 0)) return fail(h, QLGPU_ERR_ARG, "diag_out required");
     QLGPU_CK(cudaSetDevice(h->device));
+    if (h->noise_f != 0.0 || h->cfl > 0) return step_forced(h, nsteps, diag_every, diag_out, max_diag, ndiag);
+    h->dt_sum += nsteps * h->p.dt;
+    h->steps_taken += (unsigned long long)nsteps;
     const double interval = diag_every > 0 ? diag_every * h->p.dt : 0.0;
     if (interval != h->dp.tv_interval) h->dp.tv_interval = interval;
     if (diag_every > 0) {

@@ -53,6 +53,15 @@ struct qlgpu_handle {
     std::vector<double> il2_tab, ekz_tab;
     StageConst sc[3];
     std::string err;
+    // forcing (include/qlgpu.h: qlgpu_set_noise, qlgpu_set_cfl)
+    double noise_f = 0.0, noise_klo = 0.0, noise_khi = 0.0;
+    unsigned long long noise_seed = 0;
+    double cfl = 0.0, dt_max = 0.0;
+    double dt_sum = 0.0;                 // Integrator::mean_time_step accumulators
+    unsigned long long steps_taken = 0;  // since set_state; the noise counter's step word
+    double* d_forcing = nullptr;         // [0..3] last rhs mean-field maxima, [4..7] current, [8] step start time
+    double* d_kx0_prev = nullptr;        // kx0 at the start of the step (noise)
+    bool ekz_dynamic = false;            // stage exp(kz) factors computed in the kernel (variable dt)
 };
 
 

@@ -67,7 +67,7 @@ def initial_state(p: QLParams, seed: int, sigma: float = 1e-3, B0: float = 0.05,
     ky = kt["ky"][:, None]
     kz = kt["kz"][None, :]
     k2 = kx * kx + ky * ky + kz * kz
-    with np.errstate(divide="ignore"):
+    with np.errstate(divide="ignore", invalid="ignore"):
         amp = np.where(k2 > 0, sigma / k2, 0.0) * float(p.nx * (p.ny // 2 * 2) * p.NZ)
     rng = np.random.Generator(np.random.PCG64(seed))
     g = rng.standard_normal((nxy, 4, nz, 2))

@@ -99,6 +99,20 @@ class QLSolver:
         _capi.check(self.L.qlgpu_step(self.h, int(nsteps), 0, None, 0, None), self.h)
         return np.zeros((0, 15))
 
+    def set_noise(self, f_noise: float, k_low: float, k_high: float, seed: int = 0):
+        """Model::DrivingNoise after every step (MHD_BQlin); f_noise = 0 turns it off."""
+        _capi.check(self.L.qlgpu_set_noise(self.h, float(f_noise), float(k_low), float(k_high), int(seed)), self.h)
+
+    def set_cfl(self, cfl: float, dt_max: float = 0.0):
+        """Variable dt = cfl / Calculate_CFL capped at dt_max (cfl = 0: fixed dt)."""
+        _capi.check(self.L.qlgpu_set_cfl(self.h, float(cfl), float(dt_max)), self.h)
+
+    def mean_time_step(self) -> float:
+        """Integrator::mean_time_step(): mean dt since set_state."""
+        v = ctypes.c_double()
+        _capi.check(self.L.qlgpu_mean_time_step(self.h, ctypes.byref(v)), self.h)
+        return v.value
+
     def step_timed(self) -> np.ndarray:
         """One step; returns the device time (ms) of each of its three stage kernels."""
         ms = (ctypes.c_float * 3)()
