@@ -198,6 +198,17 @@ int qlgpu_fp64_peak(int device, double* tflops);
 int qlgpu_adjoint_maxwell(qlgpu_t* h, double t0, const double* lin0, const double* mf0, const double* kx0,
                           int nsteps, int checkpoint_every, double* J, double* grad_lin, double* grad_mf);
 
+/* The same for nseeds initial states at once, one handle per seed (handles of
+ * equal dimensions, each with its own stream): every phase of the sweeps
+ * (forward steps, checkpoint restore, window recompute, reverse steps) is
+ * enqueued for all seeds before the next, so the seeds' kernels run
+ * concurrently on the device.  lin0 [nseeds][nxy][4][nz], mf0 [nseeds][nmf][nz],
+ * kx0 [nseeds][nxy] or NULL; J [nseeds], grad_lin / grad_mf like lin0 / mf0.
+ * Each seed's results equal those of qlgpu_adjoint_maxwell on its handle. */
+int qlgpu_adjoint_maxwell_batch(qlgpu_t* const* handles, int nseeds, double t0, const double* lin0,
+                                const double* mf0, const double* kx0, int nsteps, int checkpoint_every, double* J,
+                                double* grad_lin, double* grad_mf);
+
 /* ------------------------------------------------------------------------
  * Batched ensemble.  No counterpart in the reference, which runs one case per
  * MPI job (QL_DNS/main.cpp:23-180): here many independent cases, each with

@@ -2,17 +2,17 @@
 
     python -m ql_dns_b200.adjoint_run [--seeds 16] [--steps 2000] [--checkpoint 100] [--fd-dirs 8]
 
-For every seed: J = the fluctuation Maxwell stress averaged over the steps and
-dJ/d lin0 from qlgpu_adjoint_maxwell (checkpoints every --checkpoint steps,
-stages recomputed per window), checked along --fd-dirs random unit directions
-(unit in the norm of lin0, so eps is a relative perturbation of the initial
-state) against central finite differences of the GPU forward run with step eps
-and eps/2.  Per direction it reports the relative error |adj - fd| / |fd| and
-the error relative to |grad| |d|, which stays meaningful for directions nearly
-orthogonal to the gradient.  The
-adjoint's wall time is compared with the forward run's (both include the
-host-device copies of one call).  Seeds run one after another on one GPU.
-Prints one JSON line.
+All seeds run together: J = the fluctuation Maxwell stress averaged over the
+steps and dJ/d lin0 come from one qlgpu_adjoint_maxwell_batch call (one handle
+and stream per seed, checkpoints every --checkpoint steps, stages recomputed
+per window).  The forward cost it is compared with is the same seeds' forward
+run with a record every step through the batched ensemble (one persistent
+launch for all seeds, QLBatch).  Gradients are checked along --fd-dirs random
+directions per seed (scaled to |lin0|, so eps is a relative perturbation)
+against central finite differences of the batched forward run with step eps
+and eps/2.  Per direction: the relative error |adj - fd| / |fd| and the error
+relative to |grad| |d|, which stays meaningful for directions nearly
+orthogonal to the gradient.  Prints one JSON line.
 """
 from __future__ import annotations
 
@@ -22,15 +22,17 @@ import time
 
 import numpy as np
 
+from .batch import QLBatch
 from .initial import initial_state
 from .params import adjoint_32x32_nz64
 from .solver import QLSolver
 
 
-def forward_J(s: QLSolver, lin, mf, kx0, n):
-    s.set_state(0.0, lin, mf, kx0)
-    d = s.step(n, diag_every=1)
-    return float(d[:, 8].mean())
+def batch_J(b: QLBatch, states, n):
+    for c, (lin, mf, kx0) in enumerate(states):
+        b.set_state(c, 0.0, lin, mf, kx0)
+    recs = b.step(n, diag_every=1)
+    return np.array([float(r[:, 8].mean()) for r in recs])
 
 
 def main(argv=None):
@@ -42,45 +44,63 @@ def main(argv=None):
     ap.add_argument("--eps", type=float, default=1e-6)
     a = ap.parse_args(argv)
     p = adjoint_32x32_nz64()
+    S = a.seeds
+    states = [initial_state(p, seed, sigma=1e-3) for seed in range(S)]
     out = {"workload": f"MHD_BQlin + RK3CN_Elin, {p.nx}x{p.ny} modes x NZ={p.NZ}, Re=Rm={1 / p.nu:.0f}, "
-                       f"dt={p.dt}, {a.steps} steps, checkpoint every {a.checkpoint}",
-           "eps": a.eps, "seeds": []}
-    with QLSolver(p) as s:
-        for seed in range(a.seeds):
-            lin, mf, kx0 = initial_state(p, seed, sigma=1e-3)
-            forward_J(s, lin, mf, kx0, 3)  # warm-up
+                       f"dt={p.dt}, {a.steps} steps, checkpoint every {a.checkpoint}, {S} seeds together",
+           "eps": a.eps}
+    with QLBatch([p] * S) as b:
+        batch_J(b, states, 3)  # warm-up
+        t0 = time.perf_counter()
+        Jf = batch_J(b, states, a.steps)
+        t_fwd = time.perf_counter() - t0
+        solvers = [QLSolver(p) for _ in range(S)]
+        try:
+            QLSolver.adjoint_maxwell_batch(solvers, 0.0, [s[0] for s in states], [s[1] for s in states],
+                                           [s[2] for s in states], 3, 3)  # warm-up
             t0 = time.perf_counter()
-            J = forward_J(s, lin, mf, kx0, a.steps)
-            t_fwd = time.perf_counter() - t0
-            t0 = time.perf_counter()
-            Ja, g, _ = s.adjoint_maxwell(0.0, lin, mf, kx0, a.steps, a.checkpoint)
+            Ja, G, _ = QLSolver.adjoint_maxwell_batch(solvers, 0.0, [s[0] for s in states], [s[1] for s in states],
+                                                      [s[2] for s in states], a.steps, a.checkpoint)
             t_adj = time.perf_counter() - t0
-            rng = np.random.default_rng(1000 + seed)
-            gnorm = float(np.linalg.norm(g))
-            dirs = []
-            for _ in range(a.fd_dirs):
+            t0 = time.perf_counter()
+            solvers[0].adjoint_maxwell(0.0, *states[0], a.steps, a.checkpoint)
+            t_adj1 = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            solvers[0].set_state(0.0, *states[0])
+            solvers[0].step(a.steps, diag_every=1)
+            t_fwd1 = time.perf_counter() - t0
+        finally:
+            for s in solvers:
+                s.close()
+        rng = np.random.default_rng(1000)
+        dirs = []
+        for _ in range(a.fd_dirs):
+            ds = []
+            for lin, _, _ in states:
                 d = rng.normal(size=lin.shape) + 1j * rng.normal(size=lin.shape)
-                d *= np.linalg.norm(lin) / np.linalg.norm(d)
-                adj = float(np.real(np.vdot(g, d)))
-                fd = []
-                for eps in (a.eps, a.eps / 2):
-                    fd.append((forward_J(s, lin + eps * d, mf, kx0, a.steps) -
-                               forward_J(s, lin - eps * d, mf, kx0, a.steps)) / (2 * eps))
-                scale = gnorm * float(np.linalg.norm(d))
-                dirs.append({"adjoint": adj, "fd_eps": fd[0], "fd_eps_half": fd[1],
-                             "cos": adj / scale,  # directional derivative / (|grad| |d|)
-                             "rel_err": abs(adj - fd[0]) / abs(fd[0]),
-                             "norm_err": abs(adj - fd[0]) / scale})  # error / (|grad| |d|)
-            out["seeds"].append({"seed": seed, "J": Ja, "J_forward": J, "grad_norm": gnorm, "dirs": dirs,
-                                 "forward_s": t_fwd, "adjoint_s": t_adj, "adjoint_over_forward": t_adj / t_fwd})
-    sd = out["seeds"]
-    out["adjoint_over_forward_median"] = float(np.median([x["adjoint_over_forward"] for x in sd]))
-    out["adjoint_over_forward_max"] = float(np.max([x["adjoint_over_forward"] for x in sd]))
-    alld = [d for x in sd for d in x["dirs"]]
-    if alld:
-        out["fd_rel_err_max"] = max(d["rel_err"] for d in alld)
-        out["fd_rel_err_median"] = float(np.median([d["rel_err"] for d in alld]))
-        out["fd_norm_err_max"] = max(d["norm_err"] for d in alld)
+                ds.append(d * (np.linalg.norm(lin) / np.linalg.norm(d)))
+            fd = []
+            for eps in (a.eps, a.eps / 2):
+                Jp = batch_J(b, [(lin + eps * d, mf, kx0) for (lin, mf, kx0), d in zip(states, ds)], a.steps)
+                Jm = batch_J(b, [(lin - eps * d, mf, kx0) for (lin, mf, kx0), d in zip(states, ds)], a.steps)
+                fd.append((Jp - Jm) / (2 * eps))
+            for k in range(S):
+                adj = float(np.real(np.vdot(G[k], ds[k])))
+                scale = float(np.linalg.norm(G[k]) * np.linalg.norm(ds[k]))
+                dirs.append({"seed": k, "adjoint": adj, "fd_eps": float(fd[0][k]), "fd_eps_half": float(fd[1][k]),
+                             "cos": adj / scale, "rel_err": abs(adj - fd[0][k]) / abs(fd[0][k]),
+                             "norm_err": abs(adj - fd[0][k]) / scale})
+    out.update({"J_adjoint": Ja.tolist(), "J_forward": Jf.tolist(),
+                "J_rel_diff_max": float(np.max(np.abs(Ja - Jf) / np.abs(Jf))),
+                "forward_batch_s": t_fwd, "adjoint_batch_s": t_adj,
+                "adjoint_over_forward": t_adj / t_fwd,
+                "single_seed": {"forward_s": t_fwd1, "adjoint_s": t_adj1, "adjoint_over_forward": t_adj1 / t_fwd1},
+                "batch_speedup_vs_sequential_adjoint": S * t_adj1 / t_adj})
+    if dirs:
+        out["fd_rel_err_median"] = float(np.median([d["rel_err"] for d in dirs]))
+        out["fd_rel_err_max"] = max(d["rel_err"] for d in dirs)
+        out["fd_norm_err_max"] = max(d["norm_err"] for d in dirs)
+        out["directions"] = len(dirs)
     print(json.dumps(out))
     return 0
 

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -24,7 +25,7 @@ struct AdjOps {
     void (*modes)(const AdjStageArgs&, const DevParams&, int nxy, cudaStream_t);
     void (*mf_post)(const double*, const cplx*, const DevParams&, cplx*, cudaStream_t);
     void (*jgrad)(const cplx*, const double*, const double*, const int*, const double*, const DevParams&, double,
-                  double, cplx*, cudaStream_t);
+                  const double*, double, cplx*, cudaStream_t);
     const void* modes_kernel;
     size_t modes_smem;
 };
@@ -43,8 +44,8 @@ void ops_mf_post(const double* bsum, const cplx* tw, const DevParams& P, cplx* l
 }
 template <int NZ>
 void ops_jgrad(const cplx* U, const double* kx0, const double* ky, const int* kyi, const double* il2,
-               const DevParams& P, double t, double w, cplx* lam, cudaStream_t st) {
-    adj_jgrad_kernel<NZ><<<148, 256, 0, st>>>(U, kx0, ky, kyi, il2, P, t, w, lam);
+               const DevParams& P, double t, const double* t_dev, double w, cplx* lam, cudaStream_t st) {
+    adj_jgrad_kernel<NZ><<<148, 256, 0, st>>>(U, kx0, ky, kyi, il2, P, t, t_dev, w, lam);
 }
 template <int NZ>
 AdjOps make_ops() {
@@ -98,192 +99,407 @@ struct Pool {
     }
 };
 
+
+// One seed's adjoint: the buffers and the position of its sweeps.  The phases
+// below only enqueue work on the handle's stream (except where a host copy is
+// needed), so several jobs, one per handle, advance together on their own
+// streams: qlgpu_adjoint_maxwell_batch interleaves them phase by phase.
+struct AdjJob {
+    qlgpu_t* h = nullptr;
+    AdjOps ops{};
+    int N = 0, C = 0, NC = 0;
+    size_t nlin = 0, nmfe = 0, nxy = 0;
+    Pool pool;
+    cplx *ck_lin = nullptr, *ck_mf = nullptr;
+    double* ck_kx0 = nullptr;
+    DevClock* ck_clk = nullptr;
+    cplx *fin_lin = nullptr, *fin_mf = nullptr;
+    double* fin_kx0 = nullptr;
+    DevClock* fin_clk = nullptr;
+    int fin_cur = 0;
+    std::vector<double> rec;
+    DevClock cend{};
+    cplx *stU = nullptr, *stB = nullptr, *postU = nullptr;
+    double *kx_pre = nullptr, *kx_post = nullptr, *t_pre = nullptr;
+    cplx *lamU[2] = {nullptr, nullptr}, *lamB[2] = {nullptr, nullptr};
+    cplx *lamF[2] = {nullptr, nullptr}, *lamG[2] = {nullptr, nullptr};
+    double *prof = nullptr, *bpart = nullptr, *bsum = nullptr;
+    int iu = 0, ib = 0;
+    double J = 0.0;
+    // full-window graphs (replayed for every window of C steps when C is even)
+    cudaGraphExec_t g_fwd = nullptr, g_rec = nullptr, g_bwd = nullptr;
+    ~AdjJob() {
+        for (cudaGraphExec_t g : {g_fwd, g_rec, g_bwd})
+            if (g) cudaGraphExecDestroy(g);
+    }
+};
+
+int adj_begin(AdjJob& j, qlgpu_t* h, double t0, const double* lin0, const double* mf0, const double* kx0, int nsteps,
+              int checkpoint_every) {
+    j.h = h;
+    if (!lin0 || !mf0 || nsteps < 1 || checkpoint_every < 1)
+        return afail(h, QLGPU_ERR_ARG, "null argument, nsteps < 1 or checkpoint_every < 1");
+    if (h->p.model != QLGPU_MODEL_MHD_BQLIN || h->p.integrator != QLGPU_INTEG_RK3CN_ELIN)
+        return afail(h, QLGPU_ERR_UNSUPPORTED, "the adjoint covers MHD_BQlin with RK3CN_Elin");
+    if (h->noise_f != 0.0 || h->cfl > 0) return afail(h, QLGPU_ERR_UNSUPPORTED, "the adjoint runs at fixed dt, no noise");
+    if (!pick_ops(h->NZ, &j.ops)) return afail(h, QLGPU_ERR_UNSUPPORTED, "unsupported NZ");
+    QA_CK(cudaSetDevice(h->device));
+    QA_CK(ensure_smem_attr(j.ops.modes_kernel, j.ops.modes_smem));
+    int rc = qlgpu_set_state(h, t0, lin0, mf0, kx0);
+    if (rc) return rc;
+    j.N = nsteps;
+    j.C = std::min(checkpoint_every, nsteps);
+    j.NC = (j.N + j.C - 1) / j.C;
+    j.nlin = (size_t)h->nxy * 4 * h->nz;
+    j.nmfe = (size_t)h->nmf * h->nz;
+    j.nxy = (size_t)h->nxy;
+    QA_CK(j.pool.get(&j.ck_lin, (size_t)j.NC * j.nlin));
+    QA_CK(j.pool.get(&j.ck_mf, (size_t)j.NC * j.nmfe));
+    QA_CK(j.pool.get(&j.ck_kx0, (size_t)j.NC * j.nxy));
+    QA_CK(j.pool.get(&j.ck_clk, (size_t)j.NC));
+    QA_CK(j.pool.get(&j.fin_lin, j.nlin));
+    QA_CK(j.pool.get(&j.fin_mf, j.nmfe));
+    QA_CK(j.pool.get(&j.fin_kx0, j.nxy));
+    QA_CK(j.pool.get(&j.fin_clk, 1));
+    if (h->diag_cap < j.N) {
+        if (h->d_diag) cudaFree(h->d_diag);
+        h->d_diag = nullptr;
+        h->diag_cap = 0;
+        QA_CK(cudaMalloc(&h->d_diag, sizeof(double) * 15 * (size_t)j.N));
+        h->diag_cap = j.N;
+    }
+    const int zero = 0;
+    QA_CK(cudaMemcpyAsync(&h->d_clk->ndiag, &zero, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    h->dp.tv_interval = h->p.dt;  // the AM_b record of every step
+    return QLGPU_OK;
+}
+
+// checkpoint c of the forward sweep (the state at the start of window c)
+int adj_checkpoint(AdjJob& j, int c) {
+    qlgpu_t* h = j.h;
+    cudaStream_t st = h->stream;
+    QA_CK(cudaMemcpyAsync(j.ck_lin + c * j.nlin, h->d_lin[h->cur], j.nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(j.ck_mf + c * j.nmfe, h->d_mf, j.nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(j.ck_kx0 + c * j.nxy, h->d_kx0, j.nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(j.ck_clk + c, h->d_clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, st));
+    return QLGPU_OK;
+}
+
+int adj_forward_step(AdjJob& j, int) {
+    qlgpu_enqueue_step(j.h, nullptr, nullptr);
+    return QLGPU_OK;
+}
+
+int adj_forward_end(AdjJob& j) {
+    qlgpu_t* h = j.h;
+    cudaStream_t st = h->stream;
+    QA_CK(cudaGetLastError());
+    j.rec.assign((size_t)15 * j.N, 0.0);
+    QA_CK(cudaMemcpyAsync(j.rec.data(), h->d_diag, j.rec.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    QA_CK(cudaMemcpyAsync(&j.cend, h->d_clk, sizeof(DevClock), cudaMemcpyDeviceToHost, st));
+    QA_CK(cudaMemcpyAsync(j.fin_lin, h->d_lin[h->cur], j.nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(j.fin_mf, h->d_mf, j.nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(j.fin_kx0, h->d_kx0, j.nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(j.fin_clk, h->d_clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, st));
+    j.fin_cur = h->cur;
+    return QLGPU_OK;
+}
+
+// after the stream is synchronised: J and the backward buffers
+int adj_forward_finish(AdjJob& j) {
+    qlgpu_t* h = j.h;
+    h->dp.tv_interval = 0.0;
+    if (j.cend.status & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE))
+        return afail(h, QLGPU_ERR_STATUS, "forward run: non-finite or unstable solution");
+    if (j.cend.ndiag != j.N) return afail(h, QLGPU_ERR_STATUS, "forward run: missing diagnostic records");
+    double s = 0.0;
+    for (int n = 0; n < j.N; ++n) s += j.rec[(size_t)15 * n + 8];  // AM_b (MHD_BQlin.cpp:459)
+    j.J = s / j.N;
+    QA_CK(j.pool.get(&j.stU, (size_t)j.C * 3 * j.nlin));
+    QA_CK(j.pool.get(&j.stB, (size_t)j.C * 3 * j.nmfe));
+    QA_CK(j.pool.get(&j.postU, j.nlin));
+    QA_CK(j.pool.get(&j.kx_pre, (size_t)j.C * j.nxy));
+    QA_CK(j.pool.get(&j.kx_post, j.nxy));
+    QA_CK(j.pool.get(&j.t_pre, (size_t)j.C + 1));
+    for (int i = 0; i < 2; ++i) {
+        QA_CK(j.pool.get(&j.lamU[i], j.nlin));
+        QA_CK(j.pool.get(&j.lamB[i], j.nmfe));
+        QA_CK(j.pool.get(&j.lamF[i], j.nlin));
+        QA_CK(j.pool.get(&j.lamG[i], j.nmfe));
+    }
+    QA_CK(j.pool.get(&j.prof, (size_t)5 * h->NZ));
+    QA_CK(j.pool.get(&j.bpart, (size_t)3 * h->NZ * j.nxy));
+    QA_CK(j.pool.get(&j.bsum, (size_t)3 * h->NZ));
+    return QLGPU_OK;
+}
+
+int window_steps(const AdjJob& j, int w) { return std::min(j.N, w * j.C + j.C) - w * j.C; }
+
+// restore checkpoint w before recomputing its window
+int adj_window_begin(AdjJob& j, int w) {
+    qlgpu_t* h = j.h;
+    cudaStream_t st = h->stream;
+    h->cur = 0;
+    QA_CK(cudaMemcpyAsync(h->d_lin[0], j.ck_lin + w * j.nlin, j.nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(h->d_mf, j.ck_mf + w * j.nmfe, j.nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(h->d_kx0, j.ck_kx0 + w * j.nxy, j.nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(h->d_clk, j.ck_clk + w, sizeof(DevClock), cudaMemcpyDeviceToDevice, st));
+    // the mean-field profile cache holds a later mean field: recompute it in the first stage
+    const int zero = 0;
+    QA_CK(cudaMemcpyAsync(&h->d_clk->mfr_valid, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+    return QLGPU_OK;
+}
+
+// recompute step n of the window, recording every stage's input
+int adj_recompute_step(AdjJob& j, int n) {
+    qlgpu_t* h = j.h;
+    cudaStream_t st = h->stream;
+    QA_CK(cudaMemcpyAsync(j.kx_pre + n * j.nxy, h->d_kx0, j.nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(j.t_pre + n, &h->d_clk->t, sizeof(double), cudaMemcpyDeviceToDevice, st));
+    cudaError_t herr = cudaSuccess;
+    qlgpu_enqueue_step(h, nullptr, [&](int s) {
+        const cudaError_t e1 = cudaMemcpyAsync(j.stU + ((size_t)n * 3 + s) * j.nlin, h->d_lin[h->cur],
+                                               j.nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+        const cudaError_t e2 = cudaMemcpyAsync(j.stB + ((size_t)n * 3 + s) * j.nmfe, h->d_mf, j.nmfe * sizeof(cplx),
+                                               cudaMemcpyDeviceToDevice, st);
+        if (herr == cudaSuccess) herr = e1 != cudaSuccess ? e1 : e2;
+    });
+    QA_CK(herr);
+    return QLGPU_OK;
+}
+
+int adj_window_end(AdjJob& j, int w) {
+    qlgpu_t* h = j.h;
+    cudaStream_t st = h->stream;
+    const int steps = window_steps(j, w);
+    QA_CK(cudaMemcpyAsync(j.postU, h->d_lin[h->cur], j.nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(j.kx_post, h->d_kx0, j.nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(j.t_pre + steps, &h->d_clk->t, sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return QLGPU_OK;
+}
+
+// the adjoint of step n of a window of `steps` steps (stream-ordered after
+// adj_window_end; the step times are read on the device from t_pre)
+int adj_backward_step(AdjJob& j, int steps, int n) {
+    qlgpu_t* h = j.h;
+    cudaStream_t st = h->stream;
+    const cplx* Upost = (n + 1 < steps) ? j.stU + (size_t)(n + 1) * 3 * j.nlin : j.postU;
+    const double* kxa = (n + 1 < steps) ? j.kx_pre + (n + 1) * j.nxy : j.kx_post;
+    // J = (1/N) sum AM_b(post-step state), recorded after the remap (main.cpp:122-130)
+    j.ops.jgrad(Upost, kxa, h->d_ky, h->d_kyi, h->d_ilap2, h->dp, 0.0, j.t_pre + n + 1, 1.0 / j.N, j.lamU[j.iu], st);
+    adj_remap_kernel<<<148, 256, 0, st>>>(j.kx_pre + n * j.nxy, kxa, h->nxy, h->nz, j.lamU[j.iu]);
+    for (int s = 2; s >= 0; --s) {
+        const StageConst& S = h->sc[s];
+        AdjMfArgs M;
+        std::memset(&M, 0, sizeof(M));
+        M.B = j.stB + ((size_t)n * 3 + s) * j.nmfe;
+        M.lamB_out = j.lamB[j.ib];
+        M.lamG_out = (s == 2) ? nullptr : j.lamG[0];
+        M.lamB_in = j.lamB[j.ib ^ 1];
+        M.lamGp = (s == 0) ? nullptr : j.lamG[1];
+        M.prof = j.prof;
+        M.tw = h->d_tw;
+        M.sc = S;
+        j.ops.mf_pre(M, h->dp, st);
+        AdjStageArgs A;
+        std::memset(&A, 0, sizeof(A));
+        A.U = j.stU + ((size_t)n * 3 + s) * j.nlin;
+        A.lamU_out = j.lamU[j.iu];
+        A.lamF_out = (s == 2) ? nullptr : j.lamF[0];
+        A.lamU_in = j.lamU[j.iu ^ 1];
+        A.lamFp = (s == 0) ? nullptr : j.lamF[1];
+        A.kx0 = j.kx_pre + n * j.nxy;
+        A.ky = h->d_ky;
+        A.kxi = h->d_kxi;
+        A.kyi = h->d_kyi;
+        A.ilap2 = h->d_ilap2;
+        A.tw = h->d_tw;
+        A.prof = j.prof;
+        A.bpart = j.bpart;
+        A.t_dev = j.t_pre + n;
+        A.sc = S;
+        j.ops.modes(A, h->dp, h->nxy, st);
+        const int nout = 3 * h->NZ;
+        adj_bsum_kernel<<<(nout + 7) / 8, 256, 0, st>>>(j.bpart, h->nxy, nout, j.bsum);
+        j.ops.mf_post(j.bsum, h->d_tw, h->dp, j.lamB[j.ib ^ 1], st);
+        j.iu ^= 1;
+        j.ib ^= 1;
+        std::swap(j.lamF[0], j.lamF[1]);
+        std::swap(j.lamG[0], j.lamG[1]);
+    }
+    QA_CK(cudaGetLastError());
+    return QLGPU_OK;
+}
+
+// gradients out, and the handle left at the end of the forward run
+int adj_finish(AdjJob& j, double* grad_lin, double* grad_mf) {
+    qlgpu_t* h = j.h;
+    cudaStream_t st = h->stream;
+    QA_CK(cudaMemcpyAsync(grad_lin, j.lamU[j.iu], j.nlin * sizeof(cplx), cudaMemcpyDeviceToHost, st));
+    if (grad_mf) QA_CK(cudaMemcpyAsync(grad_mf, j.lamB[j.ib], j.nmfe * sizeof(cplx), cudaMemcpyDeviceToHost, st));
+    h->cur = j.fin_cur;
+    QA_CK(cudaMemcpyAsync(h->d_lin[h->cur], j.fin_lin, j.nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(h->d_mf, j.fin_mf, j.nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(h->d_kx0, j.fin_kx0, j.nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    QA_CK(cudaMemcpyAsync(h->d_clk, j.fin_clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, st));
+    return QLGPU_OK;
+}
+
+int sync_job(AdjJob& j) {
+    qlgpu_t* h = j.h;
+    QA_CK(cudaStreamSynchronize(h->stream));
+    return QLGPU_OK;
+}
+
+// Capture `body` on the job's stream into an executable graph.
+template <class F>
+int capture(AdjJob& j, cudaGraphExec_t* out, F body) {
+    qlgpu_t* h = j.h;
+    QA_CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    QA_CK(e);
+    const cudaError_t e2 = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    QA_CK(e2);
+    return QLGPU_OK;
+}
+
+int launch_graph(AdjJob& j, cudaGraphExec_t g) {
+    qlgpu_t* h = j.h;
+    QA_CK(cudaGraphLaunch(g, h->stream));
+    return QLGPU_OK;
+}
+
+// All jobs phase by phase; every job's work goes to its own handle's stream.
+// Optionally a window of C steps (forward, recompute, reverse) is one graph
+// launch per job after its first capture: the buffers a window uses do not
+// depend on the window, and with C even the adjoint's ping-pong buffers are
+// back in the same order after every window, so the graphs replay unchanged.
+int run_jobs(std::vector<AdjJob>& jobs, double* J, double* const* grad_lin, double* const* grad_mf) {
+    const int nj = (int)jobs.size();
+    const int N = jobs[0].N, C = jobs[0].C, NC = jobs[0].NC;
+    // opt-in (QLGPU_ADJ_GRAPH=1): at 16 seeds x 496 modes the graphs measured slower
+    // (5.4 s) than direct launches (3.5 s) for 2000 steps
+    const char* env = getenv("QLGPU_ADJ_GRAPH");
+    const bool graphs = (C % 2 == 0) && env && env[0] == '1';
+#define QA_ALL(expr)                                    \
+    for (int q_ = 0; q_ < nj; ++q_) {                   \
+        AdjJob& jj = jobs[q_];                          \
+        (void)jj;                                       \
+        int rc_ = (expr);                               \
+        if (rc_) return rc_;                            \
+    }
+    auto fwd_window = [&](AdjJob& j, int steps) -> int {
+        for (int n = 0; n < steps; ++n) {
+            int rc = adj_forward_step(j, n);
+            if (rc) return rc;
+        }
+        return QLGPU_OK;
+    };
+    auto rec_window = [&](AdjJob& j, int w, int steps) -> int {
+        for (int n = 0; n < steps; ++n) {
+            int rc = adj_recompute_step(j, n);
+            if (rc) return rc;
+        }
+        return adj_window_end(j, w);
+    };
+    auto bwd_window = [&](AdjJob& j, int steps) -> int {
+        for (int n = steps - 1; n >= 0; --n) {
+            int rc = adj_backward_step(j, steps, n);
+            if (rc) return rc;
+        }
+        return QLGPU_OK;
+    };
+    for (int w = 0; w < NC; ++w) {
+        const int steps = std::min(N, w * C + C) - w * C;
+        QA_ALL(adj_checkpoint(jj, w));
+        if (graphs && steps == C) {
+            QA_ALL(jj.g_fwd ? QLGPU_OK : capture(jj, &jj.g_fwd, [&] { return fwd_window(jj, C); }));
+            QA_ALL(launch_graph(jj, jj.g_fwd));
+        } else {
+            for (int n = 0; n < steps; ++n) QA_ALL(adj_forward_step(jj, n));
+        }
+    }
+    QA_ALL(adj_forward_end(jj));
+    QA_ALL(sync_job(jj));
+    QA_ALL(adj_forward_finish(jj));
+    for (int w = NC - 1; w >= 0; --w) {
+        const int steps = std::min(N, w * C + C) - w * C;
+        QA_ALL(adj_window_begin(jj, w));
+        if (graphs && steps == C) {
+            QA_ALL(jj.g_rec ? QLGPU_OK : capture(jj, &jj.g_rec, [&] { return rec_window(jj, w, C); }));
+            QA_ALL(launch_graph(jj, jj.g_rec));
+            QA_ALL(jj.g_bwd ? QLGPU_OK : capture(jj, &jj.g_bwd, [&] { return bwd_window(jj, C); }));
+            QA_ALL(launch_graph(jj, jj.g_bwd));
+        } else {
+            for (int n = 0; n < steps; ++n) QA_ALL(adj_recompute_step(jj, n));
+            QA_ALL(adj_window_end(jj, w));
+            for (int n = steps - 1; n >= 0; --n) QA_ALL(adj_backward_step(jj, steps, n));
+        }
+    }
+    for (int q = 0; q < nj; ++q) {
+        int rc = adj_finish(jobs[q], grad_lin[q], grad_mf ? grad_mf[q] : nullptr);
+        if (rc) return rc;
+    }
+    QA_ALL(sync_job(jj));
+#undef QA_ALL
+    for (int q = 0; q < nj; ++q) J[q] = jobs[q].J;
+    return QLGPU_OK;
+}
+
 }  // namespace
 
 extern "C" int qlgpu_adjoint_maxwell(qlgpu_t* h, double t0, const double* lin0, const double* mf0,
                                      const double* kx0, int nsteps, int checkpoint_every, double* J,
                                      double* grad_lin, double* grad_mf) {
     if (!h) return QLGPU_ERR_ARG;
-    if (!lin0 || !mf0 || !J || !grad_lin || nsteps < 1 || checkpoint_every < 1)
-        return afail(h, QLGPU_ERR_ARG, "null argument, nsteps < 1 or checkpoint_every < 1");
-    if (h->p.model != QLGPU_MODEL_MHD_BQLIN || h->p.integrator != QLGPU_INTEG_RK3CN_ELIN)
-        return afail(h, QLGPU_ERR_UNSUPPORTED, "the adjoint covers MHD_BQlin with RK3CN_Elin");
-    AdjOps ops;
-    if (!pick_ops(h->NZ, &ops)) return afail(h, QLGPU_ERR_UNSUPPORTED, "unsupported NZ");
-    QA_CK(cudaSetDevice(h->device));
-    QA_CK(ensure_smem_attr(ops.modes_kernel, ops.modes_smem));
-    int rc = qlgpu_set_state(h, t0, lin0, mf0, kx0);
+    if (!J || !grad_lin) return afail(h, QLGPU_ERR_ARG, "null argument");
+    std::vector<AdjJob> jobs(1);
+    int rc = adj_begin(jobs[0], h, t0, lin0, mf0, kx0, nsteps, checkpoint_every);
     if (rc) return rc;
-    const int N = nsteps, C = std::min(checkpoint_every, nsteps);
-    const int NC = (N + C - 1) / C;
-    const size_t nlin = (size_t)h->nxy * 4 * h->nz, nmfe = (size_t)h->nmf * h->nz, nxy = (size_t)h->nxy;
-    cudaStream_t st = h->stream;
-    Pool pool;
-    cplx *ck_lin, *ck_mf;
-    double* ck_kx0;
-    DevClock* ck_clk;
-    QA_CK(pool.get(&ck_lin, (size_t)NC * nlin));
-    QA_CK(pool.get(&ck_mf, (size_t)NC * nmfe));
-    QA_CK(pool.get(&ck_kx0, (size_t)NC * nxy));
-    QA_CK(pool.get(&ck_clk, (size_t)NC));
-    cplx *fin_lin, *fin_mf;
-    double* fin_kx0;
-    DevClock* fin_clk;
-    QA_CK(pool.get(&fin_lin, nlin));
-    QA_CK(pool.get(&fin_mf, nmfe));
-    QA_CK(pool.get(&fin_kx0, nxy));
-    QA_CK(pool.get(&fin_clk, 1));
-    // ---- forward sweep: checkpoints and the AM_b record of every step
-    {
-        if (h->diag_cap < N) {
-            if (h->d_diag) cudaFree(h->d_diag);
-            h->d_diag = nullptr;
-            h->diag_cap = 0;
-            QA_CK(cudaMalloc(&h->d_diag, sizeof(double) * 15 * (size_t)N));
-            h->diag_cap = N;
-        }
-        const int zero = 0;
-        QA_CK(cudaMemcpyAsync(&h->d_clk->ndiag, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
-        h->dp.tv_interval = h->p.dt;
-        for (int n = 0; n < N; ++n) {
-            if (n % C == 0) {
-                const int c = n / C;
-                QA_CK(cudaMemcpyAsync(ck_lin + c * nlin, h->d_lin[h->cur], nlin * sizeof(cplx),
-                                      cudaMemcpyDeviceToDevice, st));
-                QA_CK(cudaMemcpyAsync(ck_mf + c * nmfe, h->d_mf, nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
-                QA_CK(cudaMemcpyAsync(ck_kx0 + c * nxy, h->d_kx0, nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
-                QA_CK(cudaMemcpyAsync(ck_clk + c, h->d_clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, st));
-            }
-            qlgpu_enqueue_step(h, nullptr, nullptr);
-        }
-        QA_CK(cudaGetLastError());
-        std::vector<double> rec((size_t)15 * N);
-        QA_CK(cudaMemcpyAsync(rec.data(), h->d_diag, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-        DevClock c;
-        QA_CK(cudaMemcpyAsync(&c, h->d_clk, sizeof(DevClock), cudaMemcpyDeviceToHost, st));
-        QA_CK(cudaStreamSynchronize(st));
-        h->dp.tv_interval = 0.0;
-        if (c.status & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE))
-            return afail(h, QLGPU_ERR_STATUS, "forward run: non-finite or unstable solution");
-        if (c.ndiag != N) return afail(h, QLGPU_ERR_STATUS, "forward run: missing diagnostic records");
-        double s = 0.0;
-        for (int n = 0; n < N; ++n) s += rec[(size_t)15 * n + 8];  // AM_b (MHD_BQlin.cpp:459)
-        *J = s / N;
-        QA_CK(cudaMemcpyAsync(fin_lin, h->d_lin[h->cur], nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
-        QA_CK(cudaMemcpyAsync(fin_mf, h->d_mf, nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
-        QA_CK(cudaMemcpyAsync(fin_kx0, h->d_kx0, nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        QA_CK(cudaMemcpyAsync(fin_clk, h->d_clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, st));
+    double* gl[1] = {grad_lin};
+    double* gm[1] = {grad_mf};
+    return run_jobs(jobs, J, gl, grad_mf ? gm : nullptr);
+}
+
+extern "C" int qlgpu_adjoint_maxwell_batch(qlgpu_t* const* handles, int nseeds, double t0, const double* lin0,
+                                           const double* mf0, const double* kx0, int nsteps, int checkpoint_every,
+                                           double* J, double* grad_lin, double* grad_mf) {
+    if (!handles || nseeds < 1 || !handles[0]) return QLGPU_ERR_ARG;
+    qlgpu_t* h0 = handles[0];
+    if (!lin0 || !mf0 || !J || !grad_lin) return afail(h0, QLGPU_ERR_ARG, "null argument");
+    for (int q = 0; q < nseeds; ++q) {
+        if (!handles[q]) return afail(h0, QLGPU_ERR_ARG, "null handle");
+        for (int r = 0; r < q; ++r)
+            if (handles[r] == handles[q]) return afail(h0, QLGPU_ERR_ARG, "each seed needs its own handle");
+        if (handles[q]->nxy != h0->nxy || handles[q]->nz != h0->nz || handles[q]->nmf != h0->nmf)
+            return afail(h0, QLGPU_ERR_ARG, "handles of a batch must have the same dimensions");
     }
-    const int fin_cur = h->cur;
-    // ---- backward sweep
-    cplx *stU, *stB, *postU;
-    double *kx_pre, *kx_post, *t_pre;
-    QA_CK(pool.get(&stU, (size_t)C * 3 * nlin));
-    QA_CK(pool.get(&stB, (size_t)C * 3 * nmfe));
-    QA_CK(pool.get(&postU, nlin));
-    QA_CK(pool.get(&kx_pre, (size_t)C * nxy));
-    QA_CK(pool.get(&kx_post, nxy));
-    QA_CK(pool.get(&t_pre, (size_t)C + 1));
-    cplx *lamU[2], *lamB[2], *lamF[2], *lamG[2];
-    for (int i = 0; i < 2; ++i) {
-        QA_CK(pool.get(&lamU[i], nlin));
-        QA_CK(pool.get(&lamB[i], nmfe));
-        QA_CK(pool.get(&lamF[i], nlin));
-        QA_CK(pool.get(&lamG[i], nmfe));
+    const size_t nlin = (size_t)h0->nxy * 4 * h0->nz, nmfe = (size_t)h0->nmf * h0->nz;
+    std::vector<AdjJob> jobs(nseeds);
+    std::vector<double*> gl(nseeds), gm(nseeds);
+    for (int q = 0; q < nseeds; ++q) {
+        int rc = adj_begin(jobs[q], handles[q], t0, lin0 + q * 2 * nlin, mf0 + q * 2 * nmfe,
+                           kx0 ? kx0 + q * (size_t)h0->nxy : nullptr, nsteps, checkpoint_every);
+        if (rc) {
+            if (handles[q] != h0) h0->err = handles[q]->err;
+            return rc;
+        }
+        gl[q] = grad_lin + q * 2 * nlin;
+        gm[q] = grad_mf ? grad_mf + q * 2 * nmfe : nullptr;
     }
-    double *prof, *bpart, *bsum;
-    QA_CK(pool.get(&prof, (size_t)5 * h->NZ));
-    QA_CK(pool.get(&bpart, (size_t)3 * h->NZ * nxy));
-    QA_CK(pool.get(&bsum, (size_t)3 * h->NZ));
-    int iu = 0, ib = 0;
-    std::vector<double> tp((size_t)C + 1);
-    for (int w = NC - 1; w >= 0; --w) {
-        const int n0 = w * C, steps = std::min(N, n0 + C) - n0;
-        // restore the checkpoint and recompute the window, recording the stage inputs
-        h->cur = 0;
-        QA_CK(cudaMemcpyAsync(h->d_lin[0], ck_lin + w * nlin, nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
-        QA_CK(cudaMemcpyAsync(h->d_mf, ck_mf + w * nmfe, nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
-        QA_CK(cudaMemcpyAsync(h->d_kx0, ck_kx0 + w * nxy, nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        QA_CK(cudaMemcpyAsync(h->d_clk, ck_clk + w, sizeof(DevClock), cudaMemcpyDeviceToDevice, st));
-        {
-            // the mean-field profile cache holds a later mean field: recompute it in the first stage
-            const int zero = 0;
-            QA_CK(cudaMemcpyAsync(&h->d_clk->mfr_valid, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
-        }
-        cudaError_t herr = cudaSuccess;
-        for (int n = 0; n < steps; ++n) {
-            QA_CK(cudaMemcpyAsync(kx_pre + n * nxy, h->d_kx0, nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
-            QA_CK(cudaMemcpyAsync(t_pre + n, &h->d_clk->t, sizeof(double), cudaMemcpyDeviceToDevice, st));
-            qlgpu_enqueue_step(h, nullptr, [&](int s) {
-                const cudaError_t e1 = cudaMemcpyAsync(stU + ((size_t)n * 3 + s) * nlin, h->d_lin[h->cur],
-                                                       nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
-                const cudaError_t e2 = cudaMemcpyAsync(stB + ((size_t)n * 3 + s) * nmfe, h->d_mf,
-                                                       nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
-                if (herr == cudaSuccess) herr = e1 != cudaSuccess ? e1 : e2;
-            });
-        }
-        QA_CK(herr);
-        QA_CK(cudaMemcpyAsync(postU, h->d_lin[h->cur], nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
-        QA_CK(cudaMemcpyAsync(kx_post, h->d_kx0, nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        QA_CK(cudaMemcpyAsync(t_pre + steps, &h->d_clk->t, sizeof(double), cudaMemcpyDeviceToDevice, st));
-        QA_CK(cudaMemcpyAsync(tp.data(), t_pre, sizeof(double) * (steps + 1), cudaMemcpyDeviceToHost, st));
-        QA_CK(cudaStreamSynchronize(st));
-        for (int n = steps - 1; n >= 0; --n) {
-            const cplx* Upost = (n + 1 < steps) ? stU + (size_t)(n + 1) * 3 * nlin : postU;
-            const double* kxa = (n + 1 < steps) ? kx_pre + (n + 1) * nxy : kx_post;
-            // J = (1/N) sum AM_b(post-step state), recorded after the remap (main.cpp:122-130)
-            ops.jgrad(Upost, kxa, h->d_ky, h->d_kyi, h->d_ilap2, h->dp, tp[n + 1], 1.0 / N, lamU[iu], st);
-            adj_remap_kernel<<<148, 256, 0, st>>>(kx_pre + n * nxy, kxa, h->nxy, h->nz, lamU[iu]);
-            for (int s = 2; s >= 0; --s) {
-                const StageConst& S = h->sc[s];
-                AdjMfArgs M;
-                std::memset(&M, 0, sizeof(M));
-                M.B = stB + ((size_t)n * 3 + s) * nmfe;
-                M.lamB_out = lamB[ib];
-                M.lamG_out = (s == 2) ? nullptr : lamG[0];
-                M.lamB_in = lamB[ib ^ 1];
-                M.lamGp = (s == 0) ? nullptr : lamG[1];
-                M.prof = prof;
-                M.tw = h->d_tw;
-                M.sc = S;
-                ops.mf_pre(M, h->dp, st);
-                AdjStageArgs A;
-                std::memset(&A, 0, sizeof(A));
-                A.U = stU + ((size_t)n * 3 + s) * nlin;
-                A.lamU_out = lamU[iu];
-                A.lamF_out = (s == 2) ? nullptr : lamF[0];
-                A.lamU_in = lamU[iu ^ 1];
-                A.lamFp = (s == 0) ? nullptr : lamF[1];
-                A.kx0 = kx_pre + n * nxy;
-                A.ky = h->d_ky;
-                A.kxi = h->d_kxi;
-                A.kyi = h->d_kyi;
-                A.ilap2 = h->d_ilap2;
-                A.tw = h->d_tw;
-                A.prof = prof;
-                A.bpart = bpart;
-                A.t_s = tp[n] + S.t_off;
-                A.sc = S;
-                ops.modes(A, h->dp, h->nxy, st);
-                const int nout = 3 * h->NZ;
-                adj_bsum_kernel<<<(nout + 7) / 8, 256, 0, st>>>(bpart, h->nxy, nout, bsum);
-                ops.mf_post(bsum, h->d_tw, h->dp, lamB[ib ^ 1], st);
-                iu ^= 1;
-                ib ^= 1;
-                std::swap(lamF[0], lamF[1]);
-                std::swap(lamG[0], lamG[1]);
-            }
-        }
-        QA_CK(cudaGetLastError());
+    // one host thread interleaves the seeds phase by phase (threads per seed were
+    // slower: their launches contend in the driver)
+    int rc = run_jobs(jobs, J, gl.data(), grad_mf ? gm.data() : nullptr);
+    if (rc) {
+        for (int q = 0; q < nseeds; ++q)
+            if (!handles[q]->err.empty() && handles[q] != h0) h0->err = handles[q]->err;
     }
-    QA_CK(cudaMemcpyAsync(grad_lin, lamU[iu], nlin * sizeof(cplx), cudaMemcpyDeviceToHost, st));
-    if (grad_mf) QA_CK(cudaMemcpyAsync(grad_mf, lamB[ib], nmfe * sizeof(cplx), cudaMemcpyDeviceToHost, st));
-    // leave the handle at the end of the forward run
-    h->cur = fin_cur;
-    QA_CK(cudaMemcpyAsync(h->d_lin[h->cur], fin_lin, nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
-    QA_CK(cudaMemcpyAsync(h->d_mf, fin_mf, nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
-    QA_CK(cudaMemcpyAsync(h->d_kx0, fin_kx0, nxy * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    QA_CK(cudaMemcpyAsync(h->d_clk, fin_clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, st));
-    QA_CK(cudaStreamSynchronize(st));
-    return QLGPU_OK;
+    return rc;
 }

@@ -42,7 +42,8 @@ struct AdjStageArgs {
     const cplx* tw;        // transform twiddles [NZ]
     const double* prof;    // [5][NZ]: By, dBy, ddBy, px, py (real space)
     double* bpart;         // [3][NZ][nxy] per-mode adjoint of the mean-field profiles
-    double t_s;            // stage time
+    double t_s;            // stage time (when t_dev is null)
+    const double* t_dev;   // the step's start time on the device: stage time = *t_dev + sc.t_off
     StageConst sc;
 };
 
@@ -86,7 +87,8 @@ __global__ void __launch_bounds__(AdjGeom<NZ>::THREADS) adj_modes_kernel(AdjStag
     const double ky = A.ky[mode];
     const double kx0 = A.kx0[mode];
     const int kyi = A.kyi[mode], kxi = A.kxi[mode];
-    const double a = kx_at(kx0, P.q, A.t_s, ky);
+    const double ts = A.t_dev ? __dadd_rn(*A.t_dev, S.t_off) : A.t_s;
+    const double a = kx_at(kx0, P.q, ts, ky);
     const double b = ky;
     const double ab = __dmul_rn(a, b);
     const double kxe = __dadd_rn(a, __dmul_rn(__dmul_rn(P.q, S.dt_lin), ky));
@@ -392,9 +394,11 @@ __global__ void adj_mf_post_kernel(const double* bsum, const cplx* tw, DevParams
 // d/db = 2 a b_y il2 b + i c il2 eta, d/deta = -i c il2 b.  Adds to lamU.
 template <int NZ>
 __global__ void adj_jgrad_kernel(const cplx* U, const double* kx0, const double* ky, const int* kyi,
-                                 const double* ilap2, DevParams P, double t, double weight, cplx* lamU) {
+                                 const double* ilap2, DevParams P, double t_host, const double* t_dev, double weight,
+                                 cplx* lamU) {
     using G = Geom<NZ>;
     const int nz = P.nz;
+    const double t = t_dev ? *t_dev : t_host;
     const size_t n = (size_t)P.nxy * nz;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const int mode = (int)(i / nz), s = (int)(i % nz);

@@ -153,6 +153,27 @@ class QLSolver:
                                                  _capi.dptr(gm)), self.h)
         return J.value, gl, gm
 
+    @staticmethod
+    def adjoint_maxwell_batch(solvers, t0: float, lin0s, mf0s, kx0s, nsteps: int, checkpoint_every: int = 100):
+        """qlgpu_adjoint_maxwell for several initial states at once, one solver (handle and
+        stream) per seed; the seeds' sweeps run concurrently.  Returns (J[n], grad_lin[n], grad_mf[n])."""
+        n = len(solvers)
+        lin = np.ascontiguousarray(np.stack(lin0s), dtype=np.complex128)
+        mf = np.ascontiguousarray(np.stack(mf0s), dtype=np.complex128)
+        k = None
+        if kx0s is not None:
+            kx = np.ascontiguousarray(np.stack(kx0s), dtype=np.float64)
+            k = _capi.dptr(kx)
+        hs = (ctypes.c_void_p * n)(*[s.h.value for s in solvers])
+        J = np.zeros(n)
+        gl = np.empty_like(lin)
+        gm = np.empty_like(mf)
+        L = solvers[0].L
+        _capi.check(L.qlgpu_adjoint_maxwell_batch(hs, n, float(t0), _capi.dptr(lin), _capi.dptr(mf), k, int(nsteps),
+                                                  int(checkpoint_every), _capi.dptr(J), _capi.dptr(gl),
+                                                  _capi.dptr(gm)), solvers[0].h)
+        return J, gl, gm
+
     def launch_info(self) -> dict:
         a = (ctypes.c_int * 8)()
         _capi.check(self.L.qlgpu_launch_info(self.h, a), self.h)

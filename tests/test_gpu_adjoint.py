@@ -119,3 +119,45 @@ def test_torch_autograd_wrapper():
     d = directions(lin.shape, 1, 8, np.linalg.norm(lin))[0]
     _, dJ = O.tlm_maxwell(p, 0.0, lin, mf, kx0, d, None, 16)
     assert abs(float(np.real(np.vdot(gx.numpy(), d))) - dJ) <= 1e-8 * abs(dJ)
+
+
+def test_batch_of_seeds_equals_single_calls():
+    # qlgpu_adjoint_maxwell_batch interleaves the seeds on their own streams; each seed's
+    # arithmetic is that of the single call, so the results are identical
+    require_gpu()
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=32)
+    sts = [initial_state(p, 20 + k, sigma=0.2) for k in range(3)]
+    n, ck = 18, 5
+    singles = []
+    for lin, mf, kx0 in sts:
+        with QLSolver(p) as s:
+            singles.append(s.adjoint_maxwell(0.0, lin, mf, kx0, n, checkpoint_every=ck))
+    solvers = [QLSolver(p) for _ in sts]
+    try:
+        J, gl, gm = QLSolver.adjoint_maxwell_batch(solvers, 0.0, [s[0] for s in sts], [s[1] for s in sts],
+                                                   [s[2] for s in sts], n, ck)
+        for k in range(3):
+            assert J[k] == singles[k][0]
+            assert np.array_equal(gl[k], singles[k][1]) and np.array_equal(gm[k], singles[k][2])
+            # the handles are left at the end of the forward run
+            t, lo, mo, ko = solvers[k].get_state()
+            t2, lo2, mo2, ko2, _ = O.run(p, 0.0, *sts[k], n)
+            assert rel(lo, lo2) < 1e-10
+    finally:
+        for s in solvers:
+            s.close()
+
+
+def test_window_graphs_equal_direct_launches(monkeypatch):
+    # QLGPU_ADJ_GRAPH=1 with an even checkpoint interval: every full window is one graph launch per sweep;
+    # the partial last window runs with direct launches; results are bitwise those of
+    # direct launches throughout
+    require_gpu()
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=32)
+    lin, mf, kx0 = initial_state(p, 9, sigma=0.2)
+    with QLSolver(p) as s:
+        monkeypatch.setenv("QLGPU_ADJ_GRAPH", "1")
+        a = s.adjoint_maxwell(0.0, lin, mf, kx0, 22, checkpoint_every=4)
+        monkeypatch.setenv("QLGPU_ADJ_GRAPH", "0")
+        b = s.adjoint_maxwell(0.0, lin, mf, kx0, 22, checkpoint_every=4)
+    assert a[0] == b[0] and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
