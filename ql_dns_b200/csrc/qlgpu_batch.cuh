@@ -65,6 +65,15 @@ __device__ __forceinline__ void cta_copy8(void* dst, const void* src, int n) {
 // keeps the compile time of the kernel linear in the number of classes.  The
 // shared-memory objects are declared here so that every access stays a
 // shared-space access.
+// Field staging in the persistent kernel: only for transforms of up to 8 points
+// per thread (NZ <= 64).  At NZ = 128 the staging buffers cost the warp per SM
+// that the 255-register CTA could still hold; the batch measured 8% faster
+// without them (the single-case kernel keeps them: 6% faster with).
+template <int NZ>
+struct BatchStaging {
+    static constexpr bool ON = Geom<NZ>::P <= 8;
+};
+
 template <int NZ, int MODEL, int INTEG, int MAXNZ>
 __device__ __noinline__ bool batch_item_stage(const BatchCase* cs, int s, int swap, int cta, int ncta, uint32_t tmem) {
     static_assert(sizeof(StageArgs) % 8 == 0 && sizeof(DevParams) % 8 == 0, "8-byte copies");
@@ -85,7 +94,7 @@ __device__ __noinline__ bool batch_item_stage(const BatchCase* cs, int s, int sw
         }
     }
     __syncthreads();
-    return stage_body<NZ, MODEL, INTEG, true>(sA, sP, cta, ncta, smem_raw, ss);
+    return stage_body<NZ, MODEL, INTEG, true, BatchStaging<NZ>::ON>(sA, sP, cta, ncta, smem_raw, ss);
 }
 
 // MAXNZ: the largest NZ class the kernel steps.  With TMEM one CTA runs per

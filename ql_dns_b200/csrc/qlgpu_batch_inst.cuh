@@ -28,22 +28,22 @@ const void* batch_ptr() {
 template <int MODEL>
 size_t batch_smem(int NZ, int warps) {
     switch (NZ) {
-        case 16: return StageKind<16, MODEL, true>::SM::bytes(warps);
-        case 32: return StageKind<32, MODEL, true>::SM::bytes(warps);
-        case 64: return StageKind<64, MODEL, true>::SM::bytes(warps);
-        case 128: return StageKind<128, MODEL, true>::SM::bytes(warps);
-        case 256: return StageKind<256, MODEL, true>::SM::bytes(warps);
+        case 16: return StageKind<16, MODEL, true, BatchStaging<16>::ON>::SM::bytes(warps);
+        case 32: return StageKind<32, MODEL, true, BatchStaging<32>::ON>::SM::bytes(warps);
+        case 64: return StageKind<64, MODEL, true, BatchStaging<64>::ON>::SM::bytes(warps);
+        case 128: return StageKind<128, MODEL, true, BatchStaging<128>::ON>::SM::bytes(warps);
+        case 256: return StageKind<256, MODEL, true, BatchStaging<256>::ON>::SM::bytes(warps);
         default: return 0;
     }
 }
 template <int MODEL>
 int batch_tmem(int NZ, int warps) {
     switch (NZ) {
-        case 16: return StageKind<16, MODEL, true>::SM::tmem_cols(warps);
-        case 32: return StageKind<32, MODEL, true>::SM::tmem_cols(warps);
-        case 64: return StageKind<64, MODEL, true>::SM::tmem_cols(warps);
-        case 128: return StageKind<128, MODEL, true>::SM::tmem_cols(warps);
-        case 256: return StageKind<256, MODEL, true>::SM::tmem_cols(warps);
+        case 16: return StageKind<16, MODEL, true, BatchStaging<16>::ON>::SM::tmem_cols(warps);
+        case 32: return StageKind<32, MODEL, true, BatchStaging<32>::ON>::SM::tmem_cols(warps);
+        case 64: return StageKind<64, MODEL, true, BatchStaging<64>::ON>::SM::tmem_cols(warps);
+        case 128: return StageKind<128, MODEL, true, BatchStaging<128>::ON>::SM::tmem_cols(warps);
+        case 256: return StageKind<256, MODEL, true, BatchStaging<256>::ON>::SM::tmem_cols(warps);
         default: return 0;
     }
 }

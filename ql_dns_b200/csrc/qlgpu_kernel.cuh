@@ -219,7 +219,7 @@ __device__ __forceinline__ void mean_field_stage(const StageArgs& A, const DevPa
 // ---------------------------------------------------------------------------
 // Shared-memory carve-up of the stage kernel
 // ---------------------------------------------------------------------------
-template <class G, int MODEL, class Priv>
+template <class G, int MODEL, class Priv, bool STG>
 struct Smem {
     static constexpr int SW = 32 / G::T;                        // groups per warp
     static constexpr int NMFR = MODEL == MODEL_BQLIN ? 3 : 8;   // real-space mean-field profiles
@@ -236,7 +236,8 @@ struct Smem {
     // per pair of groups: BQlin R_uz, R_bz (2 NZ cplx); FullQlin the six components (6 NZ cplx)
     static constexpr size_t GS_BYTES = sizeof(cplx) * G::NZ * (MODEL == MODEL_BQLIN ? 1 : 3);
     // per pair of groups: the 4 nz fields of the mode being transformed, staged once per mode
-    static constexpr size_t STG_BYTES = sizeof(cplx) * 4 * G::nz;
+    // (STG; otherwise the fields are read from L2 where they are used)
+    static constexpr size_t STG_BYTES = STG ? sizeof(cplx) * 4 * G::nz : 0;
     __host__ __device__ static size_t work_bytes(int warps) {
         const size_t xch = sizeof(cplx) * (size_t)warps * SW * G::XSIZE;
         const size_t red = sizeof(double) * ((size_t)warps * NEMF * G::NZ + (size_t)warps * 32 * 6);
@@ -264,13 +265,16 @@ struct StageShared {
     int pad;
 };
 
-// Types of one stage variant.
-template <int NZ, int MODEL, bool USE_TMEM>
+// Types of one stage variant.  STG: each pair stages its mode's fields in
+// shared memory (the single-case kernel always; the persistent batch kernel for
+// transforms of up to 8 points per thread, where the shared memory it frees
+// for 16-point transforms buys a warp per SM more than staging saves).
+template <int NZ, int MODEL, bool USE_TMEM, bool STG = true>
 struct StageKind {
     using G = Geom<NZ>;
     static constexpr int NB = MODEL == MODEL_BQLIN ? (int)PB_COUNT : (int)PF_COUNT;
     using Priv = typename std::conditional<USE_TMEM, PrivTmem<G, NB>, PrivSmem<G, NB>>::type;
-    using SM = Smem<G, MODEL, Priv>;
+    using SM = Smem<G, MODEL, Priv, STG>;
 };
 
 // One stage over the modes of one case, executed by one CTA that is number
@@ -278,10 +282,10 @@ struct StageKind {
 // any) are allocated by the caller and passed in ss.tmem.  Returns true in the
 // one CTA that arrived last and ran the mean-field stage; every other CTA
 // returns as soon as its partial sums are published.
-template <int NZ, int MODEL, int INTEG, bool USE_TMEM>
+template <int NZ, int MODEL, int INTEG, bool USE_TMEM, bool STG = true>
 __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& P, const int cta, const int ncta,
                                            unsigned char* smem_raw, StageShared& ss) {
-    using K = StageKind<NZ, MODEL, USE_TMEM>;
+    using K = StageKind<NZ, MODEL, USE_TMEM, STG>;
     using G = typename K::G;
     constexpr int NB = K::NB;
     using Priv = typename K::Priv;
@@ -325,7 +329,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     const int pi = slot >> 1;
     const unsigned pmask = (2 * G::T == 32) ? 0xffffffffu : (((1u << (2 * G::T)) - 1u) << (pi * 2 * G::T));
     PairShared ps;
-    cplx* stg;  // this pair's staged mode fields
+    cplx* stg_buf;  // this pair's staged mode fields
     {
         unsigned char* gbase = work + SM::work_bytes(warps) + Priv::smem_bytes_per_warp() * (size_t)warps;
         cplx* k_all = reinterpret_cast<cplx*>(gbase);
@@ -333,7 +337,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
         ps.KU = kpair;
         ps.KB = kpair + G::NZ;
         cplx* s_all = reinterpret_cast<cplx*>(gbase + SM::GS_BYTES * (size_t)warps * SW);
-        stg = s_all + (size_t)(warp * (SW / 2) + pi) * 4 * G::nz;
+        stg_buf = s_all + (size_t)(warp * (SW / 2) + pi) * 4 * G::nz;
     }
     {   // zero the stress accumulators
         cplx z4[4] = {mk(0, 0), mk(0, 0), mk(0, 0), mk(0, 0)};
@@ -414,22 +418,24 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
             l2_prefetch(A.lin_in + (size_t)(mode_raw + WG * PW) * 4 * P.nz, pf_bytes);
             if (pf_prev) l2_prefetch(pf_prev + (size_t)(mode_raw + WG * PW) * 4 * P.nz, pf_bytes);
         }
-        {
+        const cplx* src = A.lin_in + (size_t)mode * 4 * P.nz;
+        const cplx* stg = src;
+        if constexpr (STG) {
+            stg = stg_buf;
             // stage the mode's 4 nz fields (contiguous, 16-byte aligned) into the pair's buffer:
             // one round trip per mode instead of one per transform and per update chunk
-            const cplx* src = A.lin_in + (size_t)mode * 4 * P.nz;
             const int lp = role * G::T + t;  // lane within the pair
             __syncwarp(pmask);               // the previous mode's readers are done
-            for (int i = lp; i < 4 * G::nz; i += 2 * G::T) cp_async16(stg + i, src + i);
+            for (int i = lp; i < 4 * G::nz; i += 2 * G::T) cp_async16(stg_buf + i, src + i);
             cp_async_commit();
             cp_async_wait_all();
             __syncwarp(pmask);
         }
         if constexpr (MODEL == MODEL_BQLIN)
-            bqlin_pair<G, INTEG, Priv>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps, pv, tw_s, mfr, tclock,
+            bqlin_pair<G, INTEG, Priv, STG>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps, pv, tw_s, mfr, tclock,
                                        cn, stg);
         else
-            fullqlin_pair<G, INTEG, Priv>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps.KU, pv, tw_s, mfr,
+            fullqlin_pair<G, INTEG, Priv, STG>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps.KU, pv, tw_s, mfr,
                                           tclock, cn, stg);
         if (last && valid && role == 0) {
             // ShearingBox_Remap(q t) after t += dt (main.cpp:122-123, MHD_BQlin.cpp:319-329)

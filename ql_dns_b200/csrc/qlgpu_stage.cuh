@@ -34,6 +34,13 @@ __device__ __forceinline__ cplx ldc(const cplx* p) {
 }
 // The fields of the mode being transformed, staged in shared memory by its pair.
 __device__ __forceinline__ cplx lds(const cplx* p) { return *p; }
+// A read of the mode's input fields: the pair's staged copy in shared memory
+// (STG) or an L2-coherent global load where the field is used.
+template <bool STG>
+__device__ __forceinline__ cplx ldu(const cplx* p) {
+    if constexpr (STG) return lds(p);
+    else return ldc(p);
+}
 __device__ __forceinline__ cplx ldc_cg(const cplx* p) {
     double2 v = __ldcg(reinterpret_cast<const double2*>(p));
     return mk(v.x, v.y);
@@ -193,7 +200,7 @@ struct PairShared {
     cplx* KB;  // R_bz, [P][T]
 };
 
-template <class G, int INTEG, class Priv>
+template <class G, int INTEG, class Priv, bool STG>
 __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& P, const StageTables& TB, int mode,
                                            bool valid, int role, int t, unsigned gmask, unsigned pmask, cplx* xch,
                                            const PairShared& ps, const Priv& pv, const cplx* tw, const double* mfr,
@@ -211,7 +218,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
     const double ab = __dmul_rn(a, b);
     const double Om2 = __dmul_rn(2.0, P.Omega);
     const double mult = valid ? ((ky == 0.0) ? 1.0 : 2.0) : 0.0;
-    const cplx* __restrict__ u_in = stg;  // this mode's lin_in fields, staged in shared memory
+    const cplx* __restrict__ u_in = stg;  // this mode's lin_in fields (staged copy or global, STG)
     cplx* u_out = A.lin_out + (size_t)mode * 4 * P.nz;
     const cplx* Fp = (A.Fprev && S.has_prev) ? A.Fprev + (size_t)mode * 4 * P.nz : nullptr;
     cplx* Fo = A.Fout ? A.Fout + (size_t)mode * 4 * P.nz : nullptr;
@@ -272,11 +279,11 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
                 const int s = stored_index<G>(k);
                 cplx v = mk(0.0, 0.0);
                 if (s >= 0 && kind != 4) {
-                    const cplx g0 = lds(p0 + s);
+                    const cplx g0 = ldu<STG>(p0 + s);
                     if (kind == 0) {
                         v = g0;
                     } else {
-                        const cplx g1 = lds(p1 + s);
+                        const cplx g1 = ldu<STG>(p1 + s);
                         const double c = kzval(kz_int<G>(k), P.kzL);
                         const double il2 = __ldg(il2row + s);
                         if (kind == 3) {
@@ -419,10 +426,10 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
             for (int i = 0; i < 4; ++i) {
                 const int s = stored_index<G>(t + G::T * (4 * c4 + i));
                 const int sl = s < 0 ? 0 : s;
-                uin[i] = lds(fin + sl);
+                uin[i] = ldu<STG>(fin + sl);
                 fpv[i] = fpp ? ldc(fpp + sl) : mk(0.0, 0.0);
-                l0[i] = lds(lin0 + sl);
-                l1[i] = lds(zin + sl);
+                l0[i] = ldu<STG>(lin0 + sl);
+                l1[i] = ldu<STG>(zin + sl);
             }
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
@@ -522,7 +529,7 @@ __device__ __forceinline__ void update_coef(const StageArgs& A, const DevParams&
 // ---------------------------------------------------------------------------
 enum { PF_E = 0, PF_E2 = 1, PF_S1 = 2, PF_S2 = 3, PF_COUNT = 4 };
 
-template <class G, int INTEG, class Priv>
+template <class G, int INTEG, class Priv, bool STG>
 __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParams& P, const StageTables& TB, int mode,
                                               bool valid, int role, int t, unsigned gmask, unsigned pmask, cplx* xch,
                                               cplx* SH, const Priv& pv, const cplx* tw, const double* mfr,
@@ -539,7 +546,7 @@ __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParam
     const double ab = __dmul_rn(a, b);
     const double Om2 = __dmul_rn(2.0, P.Omega);
     const double mult = valid ? ((ky == 0.0) ? 1.0 : 2.0) : 0.0;
-    const cplx* __restrict__ u_in = stg;  // this mode's lin_in fields, staged in shared memory
+    const cplx* __restrict__ u_in = stg;  // this mode's lin_in fields (staged copy or global, STG)
     cplx* u_out = A.lin_out + (size_t)mode * 4 * P.nz;
     const cplx* Fp = (A.Fprev && S.has_prev) ? A.Fprev + (size_t)mode * 4 * P.nz : nullptr;
     cplx* Fo = A.Fout ? A.Fout + (size_t)mode * 4 * P.nz : nullptr;
@@ -584,12 +591,12 @@ __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParam
                 const int s = stored_index<G>(k);
                 cplx v = mk(0.0, 0.0);
                 if (s >= 0) {
-                    const cplx g0 = lds(p0 + s);
+                    const cplx g0 = ldu<STG>(p0 + s);
                     const double c = kzval(kz_int<G>(k), P.kzL);
                     if (kind == 0 || kind == 5) {
                         v = g0;
                     } else {
-                        const cplx g1 = lds(p1 + s);
+                        const cplx g1 = ldu<STG>(p1 + s);
                         const double il2 = __ldg(il2row + s);
                         if (kind == 1) v = cscale(csub(cscale(g0, __dmul_rn(a, c)), imul(g1, b)), il2);
                         else v = cscale(cadd(cscale(g0, ab), imul(g1, c)), il2);  // (MHD_FullQlin.cpp:220-221)
@@ -692,8 +699,8 @@ __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParam
                 if (s < 0) continue;
                 const double c = kzval(kz_int<G>(k), P.kzL);
                 const double kz2 = kz2val(c);
-                const cplx u0 = lds(u_in + s), ze = lds(u_in + P.nz + s), b0 = lds(u_in + 2 * P.nz + s),
-                           et = lds(u_in + 3 * P.nz + s);
+                const cplx u0 = ldu<STG>(u_in + s), ze = ldu<STG>(u_in + P.nz + s), b0 = ldu<STG>(u_in + 2 * P.nz + s),
+                           et = ldu<STG>(u_in + 3 * P.nz + s);
                 if (step == 3) {
                     // F_b = B0z kz u - s1 (MHD_FullQlin.cpp:303)
                     const cplx F = csub(imul(u0, P.B0z * c), x[k2]);
