@@ -21,8 +21,9 @@ QL_DNS/Models/MHD_BQlin.cpp:498):
     db/dt = i k x E + (0, -q b_x, 0) + i kz B0z u
 with T_ij = u_i u_j - b_i b_j and E = u x b (products in real space, u and b
 including the mean column), P = I - k k^T / k^2 (identity on z-removal at
-k = 0), dissipation -nu |k|^order on u and -eta |k|^order on b handled by the
-integrators exactly as RK3CN_Elin / RK3CN (QL_DNS/Integrators/RK3CN_Elin.cpp:
+k = 0), dissipation -nu |k|^order on u and -eta |k|^order on b (ordinary diffusion
+-nu kz^2, -eta kz^2 on the kx = ky = 0 column, as MHD_FullQlin's mean fields)
+handled by the integrators exactly as RK3CN_Elin / RK3CN (QL_DNS/Integrators/RK3CN_Elin.cpp:
 74-188, RK3CN.cpp:77-202) with the operator at kx(t + dt_lin)
 (MHD_FullQlin.cpp:371-376).  After every stage update the new state is
 (i) zeroed where |kx(t')| > Mx/3 (2 pi/Lx) at the next evaluation time t'
@@ -158,6 +159,10 @@ class DNSOracle:
         L = np.empty((self.nxy, 6, self.nz))
         L[:, 0:3] = (p.nu * lapF)[:, None, :]
         L[:, 3:6] = (p.eta * lapF)[:, None, :]
+        # the kx = ky = 0 column (the means): ordinary diffusion at every order, as the
+        # mean-field operator of MHD_FullQlin (linOpMF = coef kz2, MHD_FullQlin.cpp:449-455)
+        L[0, 0:3] = p.nu * kz2
+        L[0, 3:6] = p.eta * kz2
         return L
 
     # ---- constraints after an update ---------------------------------------

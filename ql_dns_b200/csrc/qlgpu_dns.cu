@@ -37,7 +37,7 @@ bool pick_zx(int MX, KernFn* inv, KernFn* fwd, size_t* s_inv, size_t* s_fwd, int
 }
 
 bool pick_kernels(int NZ, int MX, int MY, int ncol, KernFn* inv, KernFn* fwd, KernFn* phys, size_t* s_inv,
-                  size_t* s_fwd, size_t* s_phys, int* zc) {
+                  size_t* s_fwd, size_t* s_phys, int* zc, int* phys_threads) {
     bool ok = false;
     switch (NZ) {
         case 16: ok = pick_zx<16>(MX, inv, fwd, s_inv, s_fwd, ncol); break;
@@ -47,11 +47,11 @@ bool pick_kernels(int NZ, int MX, int MY, int ncol, KernFn* inv, KernFn* fwd, Ke
     }
     if (!ok) return false;
     switch (MY) {
-        case 16: *phys = dns_phys<16>; *s_phys = Phys<16>::smem(); *zc = Phys<16>::ZC; break;
-        case 32: *phys = dns_phys<32>; *s_phys = Phys<32>::smem(); *zc = Phys<32>::ZC; break;
-        case 64: *phys = dns_phys<64>; *s_phys = Phys<64>::smem(); *zc = Phys<64>::ZC; break;
-        case 128: *phys = dns_phys<128>; *s_phys = Phys<128>::smem(); *zc = Phys<128>::ZC; break;
-        case 256: *phys = dns_phys<256>; *s_phys = Phys<256>::smem(); *zc = Phys<256>::ZC; break;
+        case 16: *phys = dns_phys<16>; *s_phys = Phys<16>::smem(); *zc = Phys<16>::ZC; *phys_threads = Phys<16>::THREADS; break;
+        case 32: *phys = dns_phys<32>; *s_phys = Phys<32>::smem(); *zc = Phys<32>::ZC; *phys_threads = Phys<32>::THREADS; break;
+        case 64: *phys = dns_phys<64>; *s_phys = Phys<64>::smem(); *zc = Phys<64>::ZC; *phys_threads = Phys<64>::THREADS; break;
+        case 128: *phys = dns_phys<128>; *s_phys = Phys<128>::smem(); *zc = Phys<128>::ZC; *phys_threads = Phys<128>::THREADS; break;
+        case 256: *phys = dns_phys<256>; *s_phys = Phys<256>::smem(); *zc = Phys<256>::ZC; *phys_threads = Phys<256>::THREADS; break;
         default: return false;
     }
     return true;
@@ -70,7 +70,7 @@ struct qlgpu_dns {
     DnsStage st[3]{};
     KernFn k_inv = nullptr, k_fwd = nullptr, k_phys = nullptr;
     size_t s_inv = 0, s_fwd = 0, s_phys = 0;
-    int zc = 16;
+    int zc = 16, phys_threads = 256;
     double t = 0.0;
     double divf = 0.0, kzmax = 0.0;
     double* d_part = nullptr;
@@ -135,7 +135,7 @@ static void make_stages(qlgpu_dns* h) {
 static cudaError_t enqueue_products(qlgpu_dns* h) {
     const DnsArgs& a = h->a;
     h->k_inv<<<dim3(h->Kyn, 6), BLOCK, h->s_inv, h->stream>>>(a);
-    h->k_phys<<<dim3(h->p.Mx, h->p.NZ / h->zc), BLOCK, h->s_phys, h->stream>>>(a);
+    h->k_phys<<<dim3(h->p.Mx, h->p.NZ / h->zc), h->phys_threads, h->s_phys, h->stream>>>(a);
     h->k_fwd<<<dim3(h->Kyn, NPROD), BLOCK, h->s_fwd, h->stream>>>(a);
     return cudaGetLastError();
 }
@@ -194,7 +194,7 @@ int qlgpu_dns_create(const qlgpu_dns_params* p, int device, qlgpu_dns_t** out) {
     h->nxy = h->ncol * h->Kyn;
     h->nz = stored_nz(p->NZ);
     if (!pick_kernels(p->NZ, p->Mx, p->My, h->ncol, &h->k_inv, &h->k_fwd, &h->k_phys, &h->s_inv, &h->s_fwd,
-                      &h->s_phys, &h->zc)) {
+                      &h->s_phys, &h->zc, &h->phys_threads)) {
         delete h;
         return fail(nullptr, QLGPU_ERR_UNSUPPORTED, "grid combination not built");
     }

@@ -147,9 +147,12 @@ __global__ void __launch_bounds__(BLOCK, 2) dns_inv_zx(DnsArgs a) {
 template <int MY>
 struct Phys {
     using GY = Geom<MY>;
-    static constexpr int ZC = MY >= 256 ? 8 : 16;
+    // 192 threads and 8 lines (4 at MY = 256) keep the shared memory near 105 KB, so two
+    // CTAs share an SM; the inverse phase (3 transforms per line) is one round of the groups
+    static constexpr int THREADS = 192;
+    static constexpr int ZC = MY >= 256 ? 4 : 8;
     static constexpr int PY = MY + 1;
-    static constexpr int NG = BLOCK / GY::T;
+    static constexpr int NG = THREADS / GY::T;
     static constexpr int XS = GY::XSIZE > MY ? GY::XSIZE : MY;
     static size_t smem() {
         size_t ph = sizeof(double) * 6 * ZC * PY;
@@ -175,7 +178,7 @@ __device__ __forceinline__ double product(int p, const double* v) {
 }
 
 template <int MY>
-__global__ void __launch_bounds__(BLOCK) dns_phys(DnsArgs a) {
+__global__ void __launch_bounds__(Phys<MY>::THREADS, 2) dns_phys(DnsArgs a) {
     using K = Phys<MY>;
     using GY = typename K::GY;
     constexpr int T = GY::T, NG = K::NG, ZC = K::ZC, PY = K::PY;
@@ -390,8 +393,12 @@ __global__ void __launch_bounds__(BLOCK) dns_update(DnsArgs a, DnsStage st) {
     for (int c = 0; c < 6; ++c) Fc[((size_t)mode * 6 + c) * a.nz + s] = F[c];
     if (st.rhs_only) return;
     // update (RK3CN_Elin.cpp:102-104 / RK3CN.cpp:105-107), operator at t_s + dt_lin
-    const double Lu = a.nu * lap_order(a, kx0, ky, kz, ts, st.dt_lin);
-    const double Lb = a.eta * lap_order(a, kx0, ky, kz, ts, st.dt_lin);
+    // the kx = ky = 0 column (the means) has ordinary diffusion at every order, as the
+    // mean-field operator of MHD_FullQlin (linOpMF = coef kz2, MHD_FullQlin.cpp:449-455)
+    const bool mean_col = (mode == 0);
+    const double kz2m = -__dmul_rn(kz, kz);
+    const double Lu = mean_col ? a.nu * kz2m : a.nu * lap_order(a, kx0, ky, kz, ts, st.dt_lin);
+    const double Lb = mean_col ? a.eta * kz2m : a.eta * lap_order(a, kx0, ky, kz, ts, st.dt_lin);
     const cplx* Fp = a.F[st.prev];
     cplx nw[6];
     if (a.integ == 0) {
@@ -403,8 +410,8 @@ __global__ void __launch_bounds__(BLOCK) dns_update(DnsArgs a, DnsStage st) {
             nw[c] = cscale(cadd(acc, u[c]), c < 3 ? eu : eb);
         }
     } else {
-        const double Lou = a.nu * lap_order(a, kx0, ky, kz, ts, 0.0);
-        const double Lob = a.eta * lap_order(a, kx0, ky, kz, ts, 0.0);
+        const double Lou = mean_col ? Lu : a.nu * lap_order(a, kx0, ky, kz, ts, 0.0);
+        const double Lob = mean_col ? Lb : a.eta * lap_order(a, kx0, ky, kz, ts, 0.0);
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
             const double L = c < 3 ? Lu : Lb, Lo = c < 3 ? Lou : Lob;

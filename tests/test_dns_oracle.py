@@ -24,9 +24,10 @@ def series_rel(d1, d2):
     return max(np.abs(d1[:, c] - d2[:, c]).max() / max(np.abs(d2[:, c]).max(), 1e-300) for c in range(1, 15))
 
 
-@pytest.mark.parametrize("integ", [0, 1])
-def test_ql_projection_reproduces_fullqlin(integ):
-    p = DNSParams(Mx=16, My=32, NZ=16, B0z=0.03, dt=0.01, integrator=integ, nu=1 / 300, eta=1 / 500)
+@pytest.mark.parametrize("integ,order", [(0, 2), (1, 2), (1, 4)])
+def test_ql_projection_reproduces_fullqlin(integ, order):
+    p = DNSParams(Mx=16, My=32, NZ=16, B0z=0.03, dt=0.01, integrator=integ, viscosity_order=order,
+                  nu=1 / 300 if order == 2 else 1e-5, eta=1 / 500 if order == 2 else 2e-5)
     q = p.ql()
     lin, mf, kx0 = initial_state(q, 5, sigma=0.3, B0=0.1, mean_u=0.05)
     kt = ktables(q)

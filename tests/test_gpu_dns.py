@@ -142,3 +142,22 @@ def test_unsupported_grid_is_refused():
     with pytest.raises(QLGPUError) as ei:
         QLDns(DNSParams(Mx=128, My=128, NZ=64))
     assert ei.value.code == 2
+
+
+@pytest.mark.parametrize("name", ["dns_exp", "dns_cn_hyper"])
+def test_golden_fixtures_on_gpu(name):
+    # the frozen oracle trajectories (tests/golden/make_dns_golden.py), incl. RK3CN with order-4 dissipation
+    require_gpu()
+    import os
+    from ql_dns_b200.dns import QLDns
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    p = DNSParams(integrator=int(g["integrator"]), Mx=int(g["Mx"]), My=int(g["My"]), NZ=int(g["NZ"]),
+                  L=tuple(g["L"]), q=float(g["q"]), omega=float(g["omega"]), nu=float(g["nu"]), eta=float(g["eta"]),
+                  B0z=float(g["B0z"]), viscosity_order=int(g["viscosity_order"]), dt=float(g["dt"]),
+                  remap=int(g["remap"]), dealias_xy=int(g["dealias_xy"]))
+    with QLDns(p) as d:
+        d.set_state(0.0, g["lin0"], g["kx00"])
+        rec = d.step(int(g["nsteps"]), diag_every=1)
+        t, lo, ko = d.get_state()
+    assert t == float(g["t"]) and np.array_equal(ko, g["kx0"])
+    assert rel(lo, g["lin"]) < 1e-10 and series_rel(rec, g["diag"]) < 1e-10
