@@ -79,6 +79,21 @@ def algorithmic_bytes_per_step(p) -> float:
     return 10.0 * 4 * p.nz * 16 * p.nxy
 
 
+def reference_flops_per_step(p) -> float:
+    """FP64 flops of one mode-step in the reference's formulation of MHD_BQlin: 3 rhs per
+    step x (15 inverse + 7 forward) length-NZ transforms x 5 NZ log2 NZ, per mode column."""
+    import math
+    return p.nxy * 3 * (15 + 7) * 5 * p.NZ * math.log2(p.NZ)
+
+
+def fp64_peak(local) -> float:
+    import ctypes
+    from ql_dns_b200 import _capi
+    v = ctypes.c_double()
+    _capi.check(_capi.load().qlgpu_fp64_peak(local, ctypes.byref(v)))
+    return v.value
+
+
 def stage_bytes(p):
     unit = 4 * p.nz * 16 * p.nxy
     return [3 * unit, 4 * unit, 3 * unit]
@@ -338,11 +353,9 @@ def dns_flops_per_step(p, nxy, Kyn) -> float:
 
 def run_dns(args, local):
     """The 64x128x64 DNS through QLDns: K steps timed with CUDA events on the handle's stream."""
-    from ql_dns_b200 import _capi
     from ql_dns_b200.dns import QLDns
     from ql_dns_b200.initial import dns_initial_state
     from ql_dns_b200.params import dns_64x128x64
-    import ctypes
     p = dns_64x128x64()
     lin, kx0 = dns_initial_state(p, 2, sigma=1e-2, B0=0.05)
     steps = max(1, min(args.steps, 1000))
@@ -354,15 +367,14 @@ def run_dns(args, local):
         rec = d.diagnostics()
         nxy = d.nxy
         Kyn = d.ny // 2
-    peak = ctypes.c_double()
-    _capi.check(_capi.load().qlgpu_fp64_peak(local, ctypes.byref(peak)))
+    pk = fp64_peak(local)
     flops = dns_flops_per_step(p, nxy, Kyn)
     achieved = flops * steps / (ms / 1e3) / 1e12
     out = {"workload": DNS_WORKLOAD, "value": nxy * steps / (ms / 1e3), "unit": UNIT, "steps": steps,
            "ms_per_step": ms / steps, "grid_points_per_s": p.Mx * p.My * p.NZ * steps / (ms / 1e3),
            "l2": "not flushed: the DNS state and transform scratch (~75 MB) stay in L2 across steps, as in a run",
-           "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                        "frac": achieved / peak.value, "peak_source": "measured FP64 FMA loop (qlgpu_fp64_peak)",
+           "roofline": {"bound": "fp64", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
+                        "frac": achieved / pk, "peak_source": "measured FP64 FMA loop (qlgpu_fp64_peak)",
                         "flops_per_step": flops,
                         "kernels": "dns_inv_zx<64,64>, dns_phys<128>, dns_fwd_xz<64,64>, dns_update (x3 per step)"},
            "energy_at_end": {"t": rec[0], "E_u": rec[3], "E_b": rec[4], "E_By_mean": rec[2]},
@@ -414,6 +426,9 @@ def run_gpu(args):
     peak, peak_kind = hbm_peak()
     alg_step = sum(algorithmic_bytes_per_step(p) for p in cases)
     achieved = alg_step * args.steps / (ms / 1e3) / 1e9
+    flops_step = sum(reference_flops_per_step(p) for p in cases)
+    fp64_pk = fp64_peak(local)
+    fp64_ach = flops_step * args.steps / (ms / 1e3) / 1e12
 
     # end to end through the batch C ABI: H2D of every case's state from pinned
     # host memory, then per step one call that advances all cases and reads the
@@ -468,7 +483,13 @@ def run_gpu(args):
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": read_traffic("batch_kernel_mri_ensemble48.md"),
                          "kernel": "batch_kernel<MHD_BQlin,RK3CN_Elin> (one launch of K steps)",
-                         "algorithmic_bytes_per_step": alg_step, "avg_launch_ms": ms},
+                         "algorithmic_bytes_per_step": alg_step, "avg_launch_ms": ms,
+                         "fp64": {"achieved": fp64_ach, "peak": fp64_pk, "unit": "TFLOP/s", "frac": fp64_ach / fp64_pk,
+                                  "flops_per_step": flops_step,
+                                  "count": "reference formulation: 3 x (15 + 7) transforms x 5 NZ log2 NZ per "
+                                           "mode-step; peak: measured FP64 FMA loop (qlgpu_fp64_peak)",
+                                  "hbm_roofline_needs_fp64_frac": flops_step / (alg_step / (peak * 1e9)) / 1e12
+                                  / fp64_pk}},
             "plain_per_case": plain,
             "speedup_vs_plain_per_case": value / plain["value"],
             "single_case": single,

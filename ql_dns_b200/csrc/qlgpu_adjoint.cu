@@ -14,6 +14,7 @@
 
 #include "../../include/qlgpu.h"
 #include "qlgpu_adjoint.cuh"
+#include "qlgpu_batch_internal.h"
 #include "qlgpu_handle.h"
 
 using namespace qlgpu;
@@ -205,6 +206,8 @@ int adj_forward_end(AdjJob& j) {
     return QLGPU_OK;
 }
 
+int adj_alloc_backward(AdjJob& j);
+
 // after the stream is synchronised: J and the backward buffers
 int adj_forward_finish(AdjJob& j) {
     qlgpu_t* h = j.h;
@@ -215,6 +218,11 @@ int adj_forward_finish(AdjJob& j) {
     double s = 0.0;
     for (int n = 0; n < j.N; ++n) s += j.rec[(size_t)15 * n + 8];  // AM_b (MHD_BQlin.cpp:459)
     j.J = s / j.N;
+    return adj_alloc_backward(j);
+}
+
+int adj_alloc_backward(AdjJob& j) {
+    qlgpu_t* h = j.h;
     QA_CK(j.pool.get(&j.stU, (size_t)j.C * 3 * j.nlin));
     QA_CK(j.pool.get(&j.stB, (size_t)j.C * 3 * j.nmfe));
     QA_CK(j.pool.get(&j.postU, j.nlin));
@@ -348,6 +356,179 @@ int adj_finish(AdjJob& j, double* grad_lin, double* grad_mf) {
 int sync_job(AdjJob& j) {
     qlgpu_t* h = j.h;
     QA_CK(cudaStreamSynchronize(h->stream));
+    return QLGPU_OK;
+}
+
+// The seeds' forward sweep and window recompute in the persistent batch kernel
+// (one launch per window for all seeds, the recompute recording every stage's
+// input through the kernel's record pointers); the reverse sweep per seed on
+// its handle's stream as in run_jobs.  The batch's reduction order differs from
+// the single-case kernel's, so each seed's results agree with
+// qlgpu_adjoint_maxwell to round-off rather than bit for bit.
+template <class F>
+int capture(AdjJob& j, cudaGraphExec_t* out, F body);
+int launch_graph(AdjJob& j, cudaGraphExec_t g);
+
+struct BatchGuard {
+    qlgpu_batch_t* b = nullptr;
+    ~BatchGuard() {
+        if (b) qlgpu_batch_destroy(b);
+    }
+};
+
+int run_jobs_persistent(std::vector<AdjJob>& jobs, double t0, const double* lin0, const double* mf0, const double* kx0,
+                        double* J, double* const* grad_lin, double* const* grad_mf) {
+    const int nj = (int)jobs.size();
+    const int N = jobs[0].N, C = jobs[0].C, NC = jobs[0].NC;
+    qlgpu_t* h0 = jobs[0].h;
+    qlgpu_t* h = h0;  // for QA_CK
+    std::vector<qlgpu_params> ps(nj);
+    for (int q = 0; q < nj; ++q) ps[q] = jobs[q].h->p;
+    BatchGuard g;
+    int rc = qlgpu_batch_create(ps.data(), nj, h0->device, &g.b);
+    if (rc) {
+        char buf[256];
+        qlgpu_batch_last_error(nullptr, buf, sizeof(buf));
+        return afail(h0, rc, std::string("adjoint batch: ") + buf);
+    }
+    qlgpu_batch_t* b = g.b;
+    cudaStream_t bs = qlgpu_batch_cuda_stream(b);
+    const size_t nlin = jobs[0].nlin, nmfe = jobs[0].nmfe, nxy = jobs[0].nxy;
+    // reverse windows as graphs (C even keeps the ping-pong buffers in place across
+    // windows) only with QLGPU_ADJ_GRAPH=1: at 16 seeds x 496 modes they measured
+    // slower (3.9 s) than direct launches (3.4 s) for 2000 steps
+    const char* genv = getenv("QLGPU_ADJ_GRAPH");
+    const bool graphs = (C % 2 == 0) && genv && genv[0] == '1';
+    for (int q = 0; q < nj; ++q) {
+        rc = qlgpu_batch_set_state(b, q, t0, lin0 + q * 2 * nlin, mf0 + q * 2 * nmfe, kx0 ? kx0 + q * nxy : nullptr);
+        if (rc) return afail(h0, rc, "adjoint batch: set_state");
+    }
+    // ---- forward sweep: checkpoints, then one launch per window with a record every step
+    std::vector<double> recs((size_t)nj * C * 15);
+    std::vector<int> nd(nj);
+    std::vector<double> Js(nj, 0.0);
+    for (int w = 0; w < NC; ++w) {
+        const int steps = std::min(N, w * C + C) - w * C;
+        for (int q = 0; q < nj; ++q) {
+            AdjJob& j = jobs[q];
+            BatchCaseDev d;
+            qlgpu_batch_case_dev(b, q, &d);
+            QA_CK(cudaMemcpyAsync(j.ck_lin + w * nlin, d.lin, nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, bs));
+            QA_CK(cudaMemcpyAsync(j.ck_mf + w * nmfe, d.mf, nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, bs));
+            QA_CK(cudaMemcpyAsync(j.ck_kx0 + w * nxy, d.kx0, nxy * sizeof(double), cudaMemcpyDeviceToDevice, bs));
+            QA_CK(cudaMemcpyAsync(j.ck_clk + w, d.clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, bs));
+        }
+        rc = qlgpu_batch_step(b, steps, 1, recs.data(), C, nd.data());
+        if (rc) {
+            char buf[256];
+            qlgpu_batch_last_error(b, buf, sizeof(buf));
+            return afail(h0, rc, std::string("adjoint forward sweep: ") + buf);
+        }
+        for (int q = 0; q < nj; ++q) {
+            if (nd[q] != steps) return afail(h0, QLGPU_ERR_STATUS, "forward run: missing diagnostic records");
+            for (int n = 0; n < steps; ++n) Js[q] += recs[((size_t)q * C + n) * 15 + 8];  // AM_b
+        }
+    }
+    for (int q = 0; q < nj; ++q) {
+        AdjJob& j = jobs[q];
+        j.J = Js[q] / N;
+        BatchCaseDev d;
+        qlgpu_batch_case_dev(b, q, &d);
+        QA_CK(cudaMemcpyAsync(j.fin_lin, d.lin, nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, bs));
+        QA_CK(cudaMemcpyAsync(j.fin_mf, d.mf, nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, bs));
+        QA_CK(cudaMemcpyAsync(j.fin_kx0, d.kx0, nxy * sizeof(double), cudaMemcpyDeviceToDevice, bs));
+        QA_CK(cudaMemcpyAsync(j.fin_clk, d.clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, bs));
+        j.fin_cur = 0;
+        j.h->dp.tv_interval = 0.0;
+        rc = adj_alloc_backward(j);
+        if (rc) return rc;
+    }
+    // ---- reverse sweep, window by window
+    cudaEvent_t ev_b = nullptr;
+    std::vector<cudaEvent_t> ev_h(nj, nullptr);
+    struct EvGuard {
+        cudaEvent_t* e;
+        std::vector<cudaEvent_t>* v;
+        ~EvGuard() {
+            if (*e) cudaEventDestroy(*e);
+            for (cudaEvent_t x : *v)
+                if (x) cudaEventDestroy(x);
+        }
+    } evg{&ev_b, &ev_h};
+    QA_CK(cudaEventCreateWithFlags(&ev_b, cudaEventDisableTiming));
+    for (int q = 0; q < nj; ++q) QA_CK(cudaEventCreateWithFlags(&ev_h[q], cudaEventDisableTiming));
+    const int zero = 0;
+    for (int w = NC - 1; w >= 0; --w) {
+        const int steps = std::min(N, w * C + C) - w * C;
+        // the previous window's reverse steps must be done with stU before the recompute rewrites it
+        if (w != NC - 1)
+            for (int q = 0; q < nj; ++q) {
+                QA_CK(cudaEventRecord(ev_h[q], jobs[q].h->stream));
+                QA_CK(cudaStreamWaitEvent(bs, ev_h[q], 0));
+            }
+        for (int q = 0; q < nj; ++q) {
+            AdjJob& j = jobs[q];
+            BatchCaseDev d;
+            qlgpu_batch_case_dev(b, q, &d);
+            QA_CK(cudaMemcpyAsync(d.lin, j.ck_lin + w * nlin, nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, bs));
+            QA_CK(cudaMemcpyAsync(d.mf, j.ck_mf + w * nmfe, nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, bs));
+            QA_CK(cudaMemcpyAsync(d.kx0, j.ck_kx0 + w * nxy, nxy * sizeof(double), cudaMemcpyDeviceToDevice, bs));
+            QA_CK(cudaMemcpyAsync(d.clk, j.ck_clk + w, sizeof(DevClock), cudaMemcpyDeviceToDevice, bs));
+            // the mean-field profile cache holds a later mean field: recompute it in the first stage
+            QA_CK(cudaMemcpyAsync(&d.clk->mfr_valid, &zero, sizeof(int), cudaMemcpyHostToDevice, bs));
+            qlgpu_batch_set_record(b, q, j.stU, j.stB, j.kx_pre, j.t_pre);
+        }
+        rc = qlgpu_batch_step(b, steps, 0, nullptr, 0, nullptr);
+        if (rc) {
+            char buf[256];
+            qlgpu_batch_last_error(b, buf, sizeof(buf));
+            return afail(h0, rc, std::string("adjoint recompute: ") + buf);
+        }
+        for (int q = 0; q < nj; ++q) {
+            AdjJob& j = jobs[q];
+            BatchCaseDev d;
+            qlgpu_batch_case_dev(b, q, &d);  // the buffer parity after the launch
+            QA_CK(cudaMemcpyAsync(j.postU, d.lin, nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, bs));
+            QA_CK(cudaMemcpyAsync(j.kx_post, d.kx0, nxy * sizeof(double), cudaMemcpyDeviceToDevice, bs));
+            QA_CK(cudaMemcpyAsync(j.t_pre + steps, &d.clk->t, sizeof(double), cudaMemcpyDeviceToDevice, bs));
+        }
+        QA_CK(cudaEventRecord(ev_b, bs));
+        for (int q = 0; q < nj; ++q) {
+            AdjJob& j = jobs[q];
+            QA_CK(cudaStreamWaitEvent(j.h->stream, ev_b, 0));
+            if (graphs && steps == C) {
+                // a full window's reverse steps: 14 small kernels per step, one graph launch
+                if (!j.g_bwd) {
+                    rc = capture(j, &j.g_bwd, [&] {
+                        for (int n = C - 1; n >= 0; --n) {
+                            int r = adj_backward_step(j, C, n);
+                            if (r) return r;
+                        }
+                        return (int)QLGPU_OK;
+                    });
+                    if (rc) return rc;
+                }
+                rc = launch_graph(j, j.g_bwd);
+                if (rc) return rc;
+                continue;
+            }
+            for (int n = steps - 1; n >= 0; --n) {
+                rc = adj_backward_step(j, steps, n);
+                if (rc) return rc;
+            }
+        }
+    }
+    for (int q = 0; q < nj; ++q) qlgpu_batch_set_record(b, q, nullptr, nullptr, nullptr, nullptr);
+    for (int q = 0; q < nj; ++q) {
+        rc = adj_finish(jobs[q], grad_lin[q], grad_mf ? grad_mf[q] : nullptr);
+        if (rc) return rc;
+    }
+    for (int q = 0; q < nj; ++q) {
+        rc = sync_job(jobs[q]);
+        if (rc) return rc;
+    }
+    QA_CK(cudaStreamSynchronize(bs));
+    for (int q = 0; q < nj; ++q) J[q] = jobs[q].J;
     return QLGPU_OK;
 }
 
@@ -494,9 +675,14 @@ extern "C" int qlgpu_adjoint_maxwell_batch(qlgpu_t* const* handles, int nseeds, 
         gl[q] = grad_lin + q * 2 * nlin;
         gm[q] = grad_mf ? grad_mf + q * 2 * nmfe : nullptr;
     }
-    // one host thread interleaves the seeds phase by phase (threads per seed were
-    // slower: their launches contend in the driver)
-    int rc = run_jobs(jobs, J, gl.data(), grad_mf ? gm.data() : nullptr);
+    // default: forward sweep and recompute of all seeds in the persistent batch kernel;
+    // QLGPU_ADJ_BATCH=streams interleaves the single-case path of every seed on its stream
+    // (results bit-identical to qlgpu_adjoint_maxwell) from one host thread (threads per
+    // seed were slower: their launches contend in the driver)
+    const char* mode = getenv("QLGPU_ADJ_BATCH");
+    const bool streams = mode && std::string(mode) == "streams";
+    int rc = streams ? run_jobs(jobs, J, gl.data(), grad_mf ? gm.data() : nullptr)
+                     : run_jobs_persistent(jobs, t0, lin0, mf0, kx0, J, gl.data(), grad_mf ? gm.data() : nullptr);
     if (rc) {
         for (int q = 0; q < nseeds; ++q)
             if (!handles[q]->err.empty() && handles[q] != h0) h0->err = handles[q]->err;

@@ -66,7 +66,7 @@ __device__ __forceinline__ double adj_efac(const DevParams& P, const StageConst&
 }
 
 template <int NZ>
-__global__ void __launch_bounds__(AdjGeom<NZ>::THREADS) adj_modes_kernel(AdjStageArgs A, DevParams P) {
+__global__ void __launch_bounds__(AdjGeom<NZ>::THREADS, 6) adj_modes_kernel(AdjStageArgs A, DevParams P) {
     using G = Geom<NZ>;
     using AG = AdjGeom<NZ>;
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -75,7 +75,8 @@ struct BatchStaging {
 };
 
 template <int NZ, int MODEL, int INTEG, int MAXNZ>
-__device__ __noinline__ bool batch_item_stage(const BatchCase* cs, int s, int swap, int cta, int ncta, uint32_t tmem) {
+__device__ __noinline__ bool batch_item_stage(const BatchCase* cs, int s, int swap, int cta, int ncta, uint32_t tmem,
+                                              int n) {
     static_assert(sizeof(StageArgs) % 8 == 0 && sizeof(DevParams) % 8 == 0, "8-byte copies");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ StageShared ss;
@@ -91,6 +92,14 @@ __device__ __noinline__ bool batch_item_stage(const BatchCase* cs, int s, int sw
             const cplx* in = sA.lin_in;
             sA.lin_in = sA.lin_out;
             sA.lin_out = const_cast<cplx*>(in);
+        }
+        cplx* rl = cs->rec_lin;
+        if (rl) {
+            const size_t nlin = (size_t)sP.nxy * 4 * sP.nz, nmfe = (size_t)sP.nmf * sP.nz;
+            sA.rec_lin = rl + ((size_t)n * 3 + s) * nlin;
+            sA.rec_mf = cs->rec_mf + ((size_t)n * 3 + s) * nmfe;
+            sA.rec_kx = s == 0 ? cs->rec_kx + (size_t)n * sP.nxy : nullptr;
+            sA.rec_t = s == 0 ? cs->rec_t + n : nullptr;
         }
     }
     __syncthreads();
@@ -133,16 +142,16 @@ __global__ void __launch_bounds__(BatchOcc<MAXNZ>::MAX_THREADS, 1) batch_kernel(
                 const BatchCase* cs = L.cases + it.c;
                 bool top = false;
                 if (it.NZ == 16) {
-                    top = batch_item_stage<16, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem);
+                    top = batch_item_stage<16, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem, n);
                 } else if (it.NZ == 32) {
-                    top = batch_item_stage<32, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem);
+                    top = batch_item_stage<32, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem, n);
                 } else if (it.NZ == 64) {
-                    top = batch_item_stage<64, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem);
+                    top = batch_item_stage<64, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem, n);
                 } else if constexpr (MAXNZ >= 128) {
                     if (it.NZ == 128)
-                        top = batch_item_stage<128, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem);
+                        top = batch_item_stage<128, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem, n);
                     else if (it.NZ == 256)
-                        top = batch_item_stage<256, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem);
+                        top = batch_item_stage<256, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem, n);
                 }
                 if (tid == 0) s_top[i] = top ? 1 : 0;
                 if (top) {

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "../../include/qlgpu.h"
+#include "qlgpu_batch_internal.h"
 #include "qlgpu_host.h"
 #include "qlgpu_kernel.cuh"
 
@@ -67,6 +68,9 @@ struct CaseHost {
     double* diag = nullptr;
     int diag_cap = 0;
     std::vector<double> kx_tab;
+    // stage-input record (qlgpu_batch_internal.h), null: off
+    cplx *rec_lin = nullptr, *rec_mf = nullptr;
+    double *rec_kx = nullptr, *rec_t = nullptr;
 };
 
 // One work item of the planner: CTA number i of the k given to case c.
@@ -326,6 +330,10 @@ int upload_descriptors(qlgpu_batch_t* b) {
             A.ekz_tab = h.ekz + (size_t)s * 2 * h.nz;
             A.sc = h.sc[s];
         }
+        d.rec_lin = h.rec_lin;
+        d.rec_mf = h.rec_mf;
+        d.rec_kx = h.rec_kx;
+        d.rec_t = h.rec_t;
     }
     QB_CK(cudaMemcpyAsync(b->d_cases, hc.data(), sizeof(BatchCase) * hc.size(), cudaMemcpyHostToDevice, b->stream));
     QB_CK(cudaStreamSynchronize(b->stream));
@@ -1056,3 +1064,32 @@ int qlgpu_batch_stream(qlgpu_batch_t* b, void** stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Internal entry points for the adjoint (qlgpu_batch_internal.h)
+// ---------------------------------------------------------------------------
+int qlgpu_batch_case_dev(qlgpu_batch_t* b, int c, BatchCaseDev* out) {
+    if (!b || c < 0 || c >= b->ncases || !out) return QLGPU_ERR_ARG;
+    CaseHost& h = b->cs[c];
+    out->lin = h.lin[b->cur];
+    out->mf = h.mf;
+    out->kx0 = h.kx0;
+    out->clk = h.clk;
+    out->nlin = (size_t)h.nxy * 4 * h.nz;
+    out->nmfe = (size_t)h.nmf * h.nz;
+    out->nxy = h.nxy;
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_set_record(qlgpu_batch_t* b, int c, cplx* rec_lin, cplx* rec_mf, double* rec_kx, double* rec_t) {
+    if (!b || c < 0 || c >= b->ncases) return QLGPU_ERR_ARG;
+    CaseHost& h = b->cs[c];
+    h.rec_lin = rec_lin;
+    h.rec_mf = rec_lin ? rec_mf : nullptr;
+    h.rec_kx = rec_lin ? rec_kx : nullptr;
+    h.rec_t = rec_lin ? rec_t : nullptr;
+    b->descr_dirty = true;
+    return QLGPU_OK;
+}
+
+cudaStream_t qlgpu_batch_cuda_stream(qlgpu_batch_t* b) { return b ? b->stream : nullptr; }

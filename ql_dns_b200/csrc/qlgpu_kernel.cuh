@@ -395,6 +395,16 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     const double qt = __dmul_rn(P.q, t_new);
     double dacc[6] = {0, 0, 0, 0, 0, 0};
 
+    // ---- optional record of the stage input (the adjoint's window recompute): CTA 0 of the
+    // case copies the mean fields and, in a step's first stage, kx0 and the clock; stable
+    // here because the previous stage (and its remap) completed before any CTA started this one
+    if (A.rec_mf && cta == 0) {
+        const int nmfe = P.nmf * P.nz;
+        for (int i = threadIdx.x; i < nmfe; i += blockDim.x) A.rec_mf[i] = ldc(A.mf + i);
+        if (A.rec_kx)
+            for (int i = threadIdx.x; i < P.nxy; i += blockDim.x) A.rec_kx[i] = __ldcg(A.kx0 + i);
+        if (A.rec_t && threadIdx.x == 0) A.rec_t[0] = __ldcg(&A.clk->t);
+    }
     // ---- mode loop: one mode per pair of groups, warp-uniform trip count (TMEM access is warp-wide)
     constexpr int PW = SW / 2;  // pairs per warp
     if (tr) A.trace[6] = gtimer();
@@ -430,6 +440,10 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
             cp_async_commit();
             cp_async_wait_all();
             __syncwarp(pmask);
+        }
+        if (A.rec_lin && valid) {  // record the mode's input fields
+            cplx* dst = A.rec_lin + (size_t)mode * 4 * P.nz;
+            for (int i = role * G::T + t; i < 4 * G::nz; i += 2 * G::T) dst[i] = ldu<STG>(stg + i);
         }
         if constexpr (MODEL == MODEL_BQLIN)
             bqlin_pair<G, INTEG, Priv, STG>(A, P, TB, mode, valid, role, t, gmask, pmask, xch, ps, pv, tw_s, mfr, tclock,

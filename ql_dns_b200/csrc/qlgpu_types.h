@@ -85,6 +85,12 @@ struct StageArgs {
     unsigned long long* trace;  // optional %globaltimer trace (null: off), see qlgpu_kernel.cuh
     double* mfr_cache;      // [NMFR][NZ] real-space mean-field profiles written by the top CTA
     const double* ekz_tab;  // [2][nz] exp(linC nu kz2), exp(linC eta kz2) for this stage (null: compute)
+    // optional record of the stage input (null: off): the fields [nxy][4][nz], the mean
+    // fields [nmf][nz] and, in the first stage of a step, kx0 [nxy] and the clock t
+    cplx* rec_lin;
+    cplx* rec_mf;
+    double* rec_kx;
+    double* rec_t;
     StageConst sc;
 };
 
@@ -100,6 +106,12 @@ constexpr int BATCH_EPOCH_STRIDE = 32;  // words between the per-case stage coun
 struct BatchCase {
     DevParams P;
     StageArgs A[3];
+    // optional record of every stage input of a launch (null: off): step n, stage s at
+    // rec_lin + (3 n + s) nxy 4 nz, rec_mf + (3 n + s) nmf nz, rec_kx + n nxy, rec_t + n
+    cplx* rec_lin;
+    cplx* rec_mf;
+    double* rec_kx;
+    double* rec_t;
 };
 
 // One work item: CTA number `cta` of the `ncta` CTAs that step case `c`.

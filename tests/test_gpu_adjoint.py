@@ -121,10 +121,15 @@ def test_torch_autograd_wrapper():
     assert abs(float(np.real(np.vdot(gx.numpy(), d))) - dJ) <= 1e-8 * abs(dJ)
 
 
-def test_batch_of_seeds_equals_single_calls():
-    # qlgpu_adjoint_maxwell_batch interleaves the seeds on their own streams; each seed's
-    # arithmetic is that of the single call, so the results are identical
+@pytest.mark.parametrize("mode", ["persistent", "streams"])
+def test_batch_of_seeds_equals_single_calls(mode, monkeypatch):
+    # persistent (default): the seeds' forward sweep and window recompute run in the
+    # persistent batch kernel, whose reduction order differs from the single-case kernel:
+    # equal to round-off.  streams: every seed's single-case path interleaved on its own
+    # stream: bit for bit.
     require_gpu()
+    if mode == "streams":
+        monkeypatch.setenv("QLGPU_ADJ_BATCH", "streams")
     p = mri_16x16_nz32(nx=8, ny=8, NZ=32)
     sts = [initial_state(p, 20 + k, sigma=0.2) for k in range(3)]
     n, ck = 18, 5
@@ -137,12 +142,20 @@ def test_batch_of_seeds_equals_single_calls():
         J, gl, gm = QLSolver.adjoint_maxwell_batch(solvers, 0.0, [s[0] for s in sts], [s[1] for s in sts],
                                                    [s[2] for s in sts], n, ck)
         for k in range(3):
-            assert J[k] == singles[k][0]
-            assert np.array_equal(gl[k], singles[k][1]) and np.array_equal(gm[k], singles[k][2])
+            if mode == "streams":
+                assert J[k] == singles[k][0]
+                assert np.array_equal(gl[k], singles[k][1]) and np.array_equal(gm[k], singles[k][2])
+            else:
+                assert abs(J[k] - singles[k][0]) <= 1e-12 * abs(singles[k][0])
+                assert rel(gl[k], singles[k][1]) < 1e-10 and rel(gm[k], singles[k][2]) < 1e-10
             # the handles are left at the end of the forward run
             t, lo, mo, ko = solvers[k].get_state()
             t2, lo2, mo2, ko2, _ = O.run(p, 0.0, *sts[k], n)
-            assert rel(lo, lo2) < 1e-10
+            assert rel(lo, lo2) < 1e-10 and np.array_equal(ko, ko2)
+        # the gradient against the tangent-linear model, through the persistent path too
+        d = directions(sts[0][0].shape, 1, 3, np.linalg.norm(sts[0][0]))[0]
+        _, dJ = O.tlm_maxwell(p, 0.0, *sts[0], d, None, n)
+        assert abs(float(np.real(np.vdot(gl[0], d))) - dJ) <= 1e-8 * abs(dJ)
     finally:
         for s in solvers:
             s.close()
@@ -161,3 +174,25 @@ def test_window_graphs_equal_direct_launches(monkeypatch):
         monkeypatch.setenv("QLGPU_ADJ_GRAPH", "0")
         b = s.adjoint_maxwell(0.0, lin, mf, kx0, 22, checkpoint_every=4)
     assert a[0] == b[0] and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+
+
+def test_batch_reverse_graphs_equal_direct_launches(monkeypatch):
+    # QLGPU_ADJ_GRAPH=1: the persistent path replays every full reverse window (even
+    # checkpoint interval) as one graph per seed; with 0 every kernel is launched directly
+    require_gpu()
+    monkeypatch.setenv("QLGPU_ADJ_GRAPH", "1")
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=32)
+    sts = [initial_state(p, 30 + k, sigma=0.2) for k in range(2)]
+    args = (0.0, [s[0] for s in sts], [s[1] for s in sts], [s[2] for s in sts], 22, 6)
+    solvers = [QLSolver(p) for _ in sts]
+    try:
+        a = QLSolver.adjoint_maxwell_batch(solvers, *args)
+        monkeypatch.setenv("QLGPU_ADJ_GRAPH", "0")
+        b = QLSolver.adjoint_maxwell_batch(solvers, *args)
+    finally:
+        for s in solvers:
+            s.close()
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    with QLSolver(p) as s:
+        J, g, _ = s.adjoint_maxwell(0.0, *sts[1], 22, 6)
+    assert abs(a[0][1] - J) <= 1e-12 * abs(J) and rel(a[1][1], g) < 1e-10
