@@ -306,3 +306,38 @@ class RK3CN_Elin(_Integrator):
 
 class RK3CN(_Integrator):
     integ_id = INTEGRATOR_RK3_CN
+
+
+def main(argv=None):
+    """One case through the single-case path:
+
+        python -m ql_dns_b200.solver [--case production|small] [--steps 20] [--diag-every 0]
+
+    production: 64x64 modes x NZ=128 (Re=Rm=8000, dt=0.005, seed 1); small: 16x16 x NZ=32
+    (Re=Rm=2000, dt=0.01, seed 0).  Prints the device time per step (CUDA events of the
+    three stage kernels) and the last diagnostic record as JSON."""
+    import argparse
+    import json
+    from .initial import initial_state
+    from .params import mri_16x16_nz32, mri_64x64_nz128
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="production", choices=["production", "small"])
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--diag-every", type=int, default=0)
+    a = ap.parse_args(argv)
+    p, seed = (mri_64x64_nz128(), 1) if a.case == "production" else (mri_16x16_nz32(), 0)
+    lin, mf, kx0 = initial_state(p, seed, sigma=1e-3)
+    with QLSolver(p) as s:
+        s.set_state(0.0, lin, mf, kx0)
+        ms = np.zeros(3)
+        for _ in range(a.steps):
+            ms += s.step_timed()
+        rec = s.step(a.diag_every, diag_every=1) if a.diag_every else s.diagnostics()[None]
+        print(json.dumps({"case": a.case, "steps": a.steps, "ms_per_step": float(ms.sum() / max(a.steps, 1)),
+                          "stage_ms": list(ms / max(a.steps, 1)), "launch": s.launch_info(),
+                          "last_record": list(rec[-1])}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
