@@ -1,4 +1,5 @@
-"""Load the golden fixtures written by tests/golden/make_golden.py."""
+"""Load the QL golden fixtures written by tests/golden/make_golden.py (the DNS
+fixtures, dns_*.npz from make_dns_golden.py, are read by the DNS tests)."""
 import glob
 import os
 
@@ -10,7 +11,8 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def names():
-    return sorted(os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    return sorted(os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLDEN, "*.npz"))
+                  if not os.path.basename(f).startswith("dns_"))
 
 
 def load(name):

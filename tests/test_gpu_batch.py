@@ -190,3 +190,18 @@ def test_batch_wait_bound_reports_timeout():
             t, lo, mo, ko = b.get_state(c)
             t2, lo2, mo2, ko2, _ = O.run(p, 0.0, lin, mf, kx0, 4)
             assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL
+
+
+def test_batch_of_tiny_and_ragged_cases():
+    # one-column, ky = 0 only and odd-sized mode grids next to a regular case, and a batch of one
+    shapes = [(2, 2), (4, 2), (2, 4), (6, 10), (4, 18), (16, 16)]
+    cases = [QLParams(nx=nx, ny=ny, NZ=32, dt=0.02, nu=1 / 1500, eta=1 / 1500) for nx, ny in shapes]
+    sts = [initial_state(p, 50 + i, sigma=0.3, B0=0.05) for i, p in enumerate(cases)]
+    for sub in (cases, cases[3:4]):
+        idx = [cases.index(p) for p in sub]
+        res, m = run_batch(sub, [sts[i] for i in idx], 8)
+        for p, i, (t, lo, mo, ko, d) in zip(sub, idx, res):
+            t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, *sts[i], 8, diag_every=1)
+            assert np.array_equal(ko, ko2)
+            assert (np.linalg.norm(lo2) == 0 and np.abs(lo).max() == 0) or rel(lo, lo2) < TOL
+            assert rel(mo, mo2) < TOL and series_rel(d, d2) < TOL

@@ -149,3 +149,30 @@ def test_fullqlin_200_steps(integ, order):
     assert t == t2 and np.array_equal(ko, ko2)
     assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL
     assert series_rel(d, d2) < TOL
+
+
+@pytest.mark.parametrize("nx,ny", [(2, 2), (4, 2), (2, 4), (6, 10), (4, 18), (96, 6)])
+@pytest.mark.parametrize("model", [0, 1])
+def test_ragged_and_tiny_mode_grids(nx, ny, model):
+    # a single column (the mean-field column only), ky = 0 only, kx = 0 only, mode counts
+    # that are not multiples of the pairs per CTA, and many kx with few ky: the mode split
+    # over CTAs and transform pairs has ragged tails
+    p = mri_16x16_nz32(nx=nx, ny=ny, NZ=32, model=model, B0z=0.02 if model else 0.0, dt=0.02)
+    lin, mf, kx0 = initial_state(p, nx * 10 + ny, sigma=0.3, mean_u=0.02)
+    _, lo, mo, ko, d = run_gpu(p, lin, mf, kx0, 6)
+    _, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, 6, diag_every=1)
+    assert np.array_equal(ko, ko2)
+    assert (np.linalg.norm(lo2) == 0 and np.abs(lo).max() == 0) or rel(lo, lo2) < TOL
+    assert rel(mo, mo2) < TOL
+    assert series_rel(d, d2) < TOL
+
+
+def test_odd_mode_counts_are_refused():
+    # Kdata fills (nx/2) + (nx/2 - 1) kx values while Model::Dimxy counts nx - 1
+    # (Kdata.cpp:29-46, Model.h:36): an odd nx would leave a column unset in the reference
+    from ql_dns_b200._capi import QLGPUError
+    require_gpu()
+    for nx, ny in ((5, 8), (8, 7)):
+        with pytest.raises(QLGPUError) as ei:
+            QLSolver(mri_16x16_nz32(nx=nx, ny=ny))
+        assert ei.value.code == 1 and "even" in str(ei.value)
