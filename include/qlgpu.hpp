@@ -51,6 +51,11 @@ struct Inputs {
     int viscosity_order = 2;
     double q = 1.5, omega = 1.0, B0z = 0.0;
     bool remapQ = true, QuasiLinearQ = true;
+    // dt < 0: variable dt = CFL / Calculate_CFL capped at -dt (RK3CN_Elin.cpp:22-27)
+    double CFL = 1.0;
+    // driving noise (Input_parameters.cpp:107-109); the generator's seed replaces the clock
+    double f_noise = 0.0, noise_range_low = 0.0, noise_range_high = 1e16;
+    unsigned long long noise_seed = 0;
 };
 
 class Model;
@@ -123,6 +128,10 @@ public:
         check(qlgpu_diagnostics(h_, out.data()), h_);
         return out;
     }
+    // Model::DrivingNoise (Model.h:85): the integrator's handle adds the noise after every
+    // step when Inputs::f_noise != 0 (qlgpu_set_noise), so the call of main.cpp:112-113
+    // has nothing left to do.
+    void DrivingNoise(double, double, solution*) {}
     qlgpu_params params() const { return p_; }
 
 protected:
@@ -165,8 +174,11 @@ public:
     Integrator(double t0, const Inputs& sp, Model* mod, int integ_id) : t0_(t0), model_(mod) {
         p_ = mod->params();
         p_.integrator = integ_id;
-        p_.dt = sp.dt;
+        p_.dt = sp.dt < 0 ? -sp.dt : sp.dt;
         check(qlgpu_create(&p_, -1, &h_), nullptr);
+        if (sp.dt < 0) check(qlgpu_set_cfl(h_, sp.CFL, -sp.dt), h_);
+        if (sp.f_noise != 0.0)
+            check(qlgpu_set_noise(h_, sp.f_noise, sp.noise_range_low, sp.noise_range_high, sp.noise_seed), h_);
     }
     virtual ~Integrator() {
         if (h_) qlgpu_destroy(h_);
@@ -178,12 +190,15 @@ public:
                   h_);
             bound_ = sol;
         }
+        double t0 = 0, t1 = 0;
+        check(qlgpu_time(h_, &t0), h_);
         check(qlgpu_step(h_, 1, 0, nullptr, 0, nullptr), h_);
+        check(qlgpu_time(h_, &t1), h_);
         sol->host_stale = true;
         sol->model = model_;
         last_handle_ = h_;
         ++steps_;
-        return p_.dt;
+        return t1 - t0;  // the step's dt (variable with CFL)
     }
     // main-loop form: n steps with a diagnostic record every diag_every steps
     std::vector<double> Run(double t, solution* sol, int n, int diag_every) {
@@ -212,7 +227,11 @@ public:
               h_);
         sol->host_stale = false;
     }
-    double mean_time_step() const { return p_.dt; }
+    double mean_time_step() const {
+        double m = p_.dt;
+        qlgpu_mean_time_step(h_, &m);
+        return m;
+    }
     qlgpu_t* handle() const { return h_; }
     static qlgpu_t* last_handle_;
 

@@ -54,7 +54,12 @@ int main(int argc, char** argv) {
     SP.remapQ = read_key<int>(full, "Remap?", 1) != 0;
     SP.QuasiLinearQ = read_key<int>(full, "QuasiLinear?", 1) != 0;
     SP.equations_to_use = read_key<std::string>(full, "equations_to_use_", std::string("MHD_BQlin"));
-    const double tv_save = read_key<double>(full, "tv_save_", SP.dt);
+    SP.CFL = read_key<double>(full, "CFL_", 1.0);
+    SP.f_noise = read_key<double>(full, "f_noise_", 0.0);
+    SP.noise_range_low = read_key<double>(full, "noise_range_low_", 0.0);
+    SP.noise_range_high = read_key<double>(full, "noise_range_high_", 1e16);
+    SP.noise_seed = (unsigned long long)read_key<double>(full, "noise_seed_", 0.0);
+    const double tv_save = read_key<double>(full, "tv_save_", SP.dt < 0 ? -SP.dt : SP.dt);
     const int integ = read_key<int>(full, "integrator_", 0);  // 0 RK3CN_Elin (main.cpp:95), 1 RK3CN
     const int nsteps = std::atoi(argv[3]);
     try {
@@ -79,7 +84,9 @@ int main(int argc, char** argv) {
         const std::vector<qlgpu::dcmplx> mf0 = sol.mf;
         qlgpu::Integrator* integrator = integ == 1 ? static_cast<qlgpu::Integrator*>(new qlgpu::RK3CN(t, SP, model))
                                                    : static_cast<qlgpu::Integrator*>(new qlgpu::RK3CN_Elin(t, SP, model));
-        const int every = (int)(tv_save / SP.dt + 0.5);
+        // a record every tv_save_ of time at a fixed dt; with the CFL dt (dt_ < 0) every
+        // tv_save_ / |dt_| steps
+        const int every = (int)(tv_save / (SP.dt < 0 ? -SP.dt : SP.dt) + 0.5);
         std::vector<double> diag = integrator->Run(t, &sol, nsteps, every);
         double tout = 0;
         qlgpu_time(integrator->handle(), &tout);

@@ -79,3 +79,39 @@ def test_cpp_driver_matches_oracle(tmp_path, integ):
     tl, ll, ml, kl = io.load_solution(str(odir / "FullSave.bin"), p)
     assert tl == t and np.array_equal(ll, lo.astype(np.complex64).astype(np.complex128))
     assert np.array_equal(ml, mo.astype(np.complex64).astype(np.complex128))
+
+
+def test_cpp_driver_with_noise_and_cfl(tmp_path):
+    # dt_ < 0 (variable dt = CFL_ / Calculate_CFL, at most |dt_|) and f_noise_ != 0
+    # (DrivingNoise after every step) read from the input file, as main.cpp:112-113 and
+    # RK3CN_Elin.cpp:22-27,76-80 use them
+    require_gpu()
+    build()
+    p = mri_16x16_nz32(dt=0.02)
+    lin, mf, kx0 = initial_state(p, 4, sigma=1e-3, B0=0.2)
+    inp = tmp_path / "case.DSSinput"
+    write_input(inp, p, 0, 5)  # tv_save_ = 5 |dt_|
+    txt = open(inp).read().replace(f"dt_ = {p.dt!r}", f"dt_ = {-p.dt!r}")
+    open(inp, "w").write(txt)
+    with open(inp, "a") as f:
+        f.write("CFL_ = 0.2\nf_noise_ = 0.05\nnoise_range_low_ = 1.0\nnoise_range_high_ = 30.0\nnoise_seed_ = 77\n")
+    st = tmp_path / "state.bin"
+    with open(st, "wb") as f:
+        np.array([0.0]).tofile(f)
+        lin.tofile(f)
+        mf.tofile(f)
+        kx0.tofile(f)
+    out, dg = tmp_path / "out.bin", tmp_path / "diag.bin"
+    r = subprocess.run([MAIN, str(inp), str(st), "40", str(out), str(dg)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    raw = np.fromfile(out, dtype=np.float64)
+    n_lin, n_mf = lin.size * 2, mf.size * 2
+    t = raw[0]
+    lo = raw[1:1 + n_lin].view(np.complex128).reshape(lin.shape)
+    mo = raw[1 + n_lin:1 + n_lin + n_mf].view(np.complex128).reshape(mf.shape)
+    d = np.fromfile(dg, dtype=np.float64).reshape(-1, 15)
+    t2, lo2, mo2, ko2, d2, dtm = O.run_forced(p, 0.0, lin, mf, kx0, 40, diag_every=5, cfl=0.2, dt_max=0.02,
+                                             f_noise=0.05, k_lo=1.0, k_hi=30.0, seed=77)
+    assert dtm < 0.02 and abs(t - t2) <= 1e-13 * t2
+    assert rel(lo, lo2) < 1e-10 and rel(mo, mo2) < 1e-10
+    assert d.shape == d2.shape and rel(d[:, 1:13], d2[:, 1:13]) < 1e-10
