@@ -6,6 +6,7 @@
 // advance (qlgpu_dns.cuh), captured once in a CUDA graph and replayed.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -307,8 +308,22 @@ int qlgpu_dns_set_state(qlgpu_dns_t* h, double t, const double* lin, const doubl
     if (!std::isfinite(t)) return fail(h, QLGPU_ERR_ARG, "t must be finite");
     DNS_CK(h, cudaSetDevice(h->device));
     const size_t ns = (size_t)h->nxy * 6 * h->nz;
-    DNS_CK(h, cudaMemcpyAsync(h->a.lin, lin, ns * sizeof(cplx), cudaMemcpyHostToDevice, h->stream));
     const double* kx = kx0 ? kx0 : h->kx_tab.data();
+    if (kx0) {
+        // every kx0 on the lattice of 2 pi/Lx, and the columns of each ky plane in distinct
+        // x bins (kx0 mod Mx): the remap keeps nx-1 consecutive integers per plane
+        std::vector<int> used((size_t)h->Kyn * h->p.Mx, -1);
+        for (int i = 0; i < h->nxy; ++i) {
+            const double m = std::nearbyint(kx[i] / h->a.dkx);
+            if (!std::isfinite(kx[i]) || std::fabs(kx[i] - m * h->a.dkx) > 1e-9 * std::max(1.0, std::fabs(kx[i])))
+                return fail(h, QLGPU_ERR_ARG, "kx0 is not a multiple of 2 pi / Lx");
+            const int b = (int)(((long long)m % h->p.Mx + h->p.Mx) % h->p.Mx);
+            int& u = used[(size_t)(i % h->Kyn) * h->p.Mx + b];
+            if (u >= 0) return fail(h, QLGPU_ERR_ARG, "two columns of one ky plane share an x bin (kx0 mod Mx)");
+            u = i;
+        }
+    }
+    DNS_CK(h, cudaMemcpyAsync(h->a.lin, lin, ns * sizeof(cplx), cudaMemcpyHostToDevice, h->stream));
     DNS_CK(h, cudaMemcpyAsync(h->a.kx0, kx, h->nxy * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     double clk[2] = {t, 0.0};
     DNS_CK(h, cudaMemcpyAsync(h->a.clock, clk, sizeof(clk), cudaMemcpyHostToDevice, h->stream));

@@ -161,3 +161,24 @@ def test_golden_fixtures_on_gpu(name):
         t, lo, ko = d.get_state()
     assert t == float(g["t"]) and np.array_equal(ko, g["kx0"])
     assert rel(lo, g["lin"]) < 1e-10 and series_rel(rec, g["diag"]) < 1e-10
+
+
+def test_bad_kx0_is_refused():
+    require_gpu()
+    from ql_dns_b200._capi import QLGPUError
+    from ql_dns_b200.dns import QLDns
+    p = DNSParams(Mx=16, My=32, NZ=16)
+    _, lin, kx0 = make(p, 1)
+    with QLDns(p) as g:
+        bad = kx0.copy()
+        bad[7] += 0.3  # off the lattice
+        with pytest.raises(QLGPUError) as ei:
+            g.set_state(0.0, lin, bad)
+        assert ei.value.code == 1
+        bad = kx0.copy()
+        Kyn = g.ny // 2
+        bad[Kyn] = bad[2 * Kyn]  # two columns of the ky = 0 plane in one x bin
+        with pytest.raises(QLGPUError):
+            g.set_state(0.0, lin, bad)
+        g.set_state(0.0, lin, kx0)
+        g.step(1)
