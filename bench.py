@@ -175,15 +175,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(backend: str = "nccl"):
-    """One process per GPU (torchrun env); N > 1 runs independent replicas."""
+def dist_setup(backend: str = "nccl", timeout_s: float = 120.0):
+    """One process per GPU (torchrun env); N > 1 runs independent replicas.  A rank
+    that dies or never arrives ends the others' next collective with an error within
+    timeout_s instead of a hang."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
     return ws, rank, local
 
 
