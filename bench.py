@@ -424,6 +424,7 @@ def run_gpu(args):
     st, ls = batch.status()
     assert ls == 0 and not any(st), (st, ls)
     mapping = batch.mapping()
+    cost = batch.cost_model()
 
     peak, peak_kind = hbm_peak()
     alg_step = sum(algorithmic_bytes_per_step(p) for p in cases)
@@ -480,7 +481,8 @@ def run_gpu(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "l2": "not flushed: the ensemble state (~0.5 GB with RK buffers) exceeds the 126 MB L2",
-                       "cases": NCASES, "mode_columns": modes, "mapping": mapping, "tune_probe_ms": tune_ms},
+                       "cases": NCASES, "mode_columns": modes, "mapping": mapping, "tune_probe_ms": tune_ms,
+                       "cost_model": cost},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": read_traffic("batch_kernel_mri_ensemble48.md"),

@@ -251,6 +251,11 @@ int qlgpu_batch_step_timed(qlgpu_batch_t* b, int nsteps, float* ms);
  * unchanged.  *best_ms (may be NULL) = time of the kept mapping's probe. */
 int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms);
 
+/* The planner's cost model (after qlgpu_batch_tune: fitted to the measured
+ * per-case stage times): out7 = {alpha (us per stage per launch), beta (us per
+ * work item per stage), r[NZ = 16, 32, 64, 128, 256] (us per pipeline pass)}. */
+int qlgpu_batch_cost_model(const qlgpu_batch_t* b, double* out7);
+
 /* Current mapping: info4 = {warps per CTA, CTAs launched, CTAs per SM,
  * dynamic shared bytes}; ncta[c] = CTAs that step case c (may be NULL). */
 int qlgpu_batch_mapping(const qlgpu_batch_t* b, int* info4, int* ncta);

@@ -36,7 +36,8 @@ EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "ql
            "qlgpu_dns_create", "qlgpu_dns_destroy", "qlgpu_dns_dims", "qlgpu_dns_set_state", "qlgpu_dns_get_state",
            "qlgpu_dns_step", "qlgpu_dns_diagnostics", "qlgpu_dns_rhs", "qlgpu_dns_status", "qlgpu_dns_last_error",
            "qlgpu_dns_step_timed", "qlgpu_dns_stream", "qlgpu_fp64_peak",
-           "qlgpu_set_noise", "qlgpu_set_cfl", "qlgpu_mean_time_step", "qlgpu_adjoint_maxwell_batch"]
+           "qlgpu_set_noise", "qlgpu_set_cfl", "qlgpu_mean_time_step", "qlgpu_adjoint_maxwell_batch",
+           "qlgpu_batch_cost_model"]
 
 
 class qlgpu_params(ctypes.Structure):
@@ -148,6 +149,7 @@ def load(path: str = LIB_PATH):
     L.qlgpu_set_noise.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong]
     L.qlgpu_set_cfl.argtypes = [vp, ctypes.c_double, ctypes.c_double]
     L.qlgpu_mean_time_step.argtypes = [vp, dp]
+    L.qlgpu_batch_cost_model.argtypes = [vp, dp]
     L.qlgpu_adjoint_maxwell_batch.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_double, dp, dp, dp,
                                               ctypes.c_int, ctypes.c_int, dp, dp, dp]
     for name in EXPORTS:

@@ -112,6 +112,13 @@ class QLBatch:
         _capi.check_batch(self.L.qlgpu_batch_mapping(self.b, info, k), self.b)
         return {"warps": info[0], "grid": info[1], "ctas_per_sm": info[2], "smem": info[3], "ncta": list(k)}
 
+    def cost_model(self) -> dict:
+        """The planner's cost model (fitted by tune()): alpha = us per stage per launch,
+        beta = us per work item per stage, r = us per pipeline pass per NZ class."""
+        v = (ctypes.c_double * 7)()
+        _capi.check_batch(self.L.qlgpu_batch_cost_model(self.b, v), self.b)
+        return {"alpha_us": v[0], "beta_us": v[1], "r_us": dict(zip([16, 32, 64, 128, 256], list(v)[2:]))}
+
     def set_mapping(self, warps: int, ncta: list[int]):
         k = (ctypes.c_int * len(ncta))(*ncta)
         _capi.check_batch(self.L.qlgpu_batch_set_mapping(self.b, int(warps), k), self.b)

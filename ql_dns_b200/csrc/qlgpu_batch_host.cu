@@ -985,6 +985,14 @@ int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms) {
     return QLGPU_OK;
 }
 
+int qlgpu_batch_cost_model(const qlgpu_batch_t* b, double* out7) {
+    if (!b || !out7) return QLGPU_ERR_ARG;
+    out7[0] = b->cost.alpha;
+    out7[1] = b->cost.beta;
+    for (int i = 0; i < NCLASS; ++i) out7[2 + i] = b->cost.r[i];
+    return QLGPU_OK;
+}
+
 int qlgpu_batch_mapping(const qlgpu_batch_t* b, int* info4, int* ncta) {
     if (!b) return QLGPU_ERR_ARG;
     if (info4) {

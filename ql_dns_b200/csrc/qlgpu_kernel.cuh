@@ -510,8 +510,17 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
         }
     }
     double* dred = red + (size_t)warps * NEMF * G::NZ;
+    if (diag_due) {
+        // the diagnostic sums (zero in stages without a record): lanes by a fixed
+        // shuffle tree, then warps in order
 #pragma unroll
-    for (int c = 0; c < 6; ++c) dred[tid * 6 + c] = dacc[c];
+        for (int c = 0; c < 6; ++c) {
+            double v = dacc[c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if ((tid & 31) == 0) dred[warp * 6 + c] = v;
+        }
+    }
     if constexpr (USE_TMEM) tmem_fence_before_sync();
     __syncthreads();
     if constexpr (USE_TMEM) tmem_fence_after_sync();
@@ -523,7 +532,8 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     }
     if (tid < 6) {
         double s = 0.0;
-        for (int r = 0; r < (int)blockDim.x; ++r) s += dred[r * 6 + tid];
+        if (diag_due)
+            for (int w = 0; w < warps; ++w) s += dred[w * 6 + tid];
         part[NEMF * G::NZ + tid] = s;
     }
 
@@ -544,8 +554,16 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     __threadfence();
     double* gpart = A.gpartials + (size_t)grp * PL;
     for (int idx = tid; idx < PL; idx += blockDim.x) {
+        // CTAs in order; four loads in flight at a time
         double s = 0.0;
-        for (int c = 0; c < cn_in; ++c) s += __ldcg(A.partials + (size_t)(c0 + c) * PL + idx);
+        for (int c = 0; c < cn_in; c += 4) {
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = c + u < cn_in ? __ldcg(A.partials + (size_t)(c0 + c + u) * PL + idx) : 0.0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (c + u < cn_in) s += v[u];
+        }
         gpart[idx] = s;
     }
     if (tid == 0) atomicExch(&A.clk->cnt_group[grp], 0u);
@@ -560,7 +578,14 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     __threadfence();
     for (int idx = tid; idx < PL; idx += blockDim.x) {
         double s = 0.0;
-        for (int g = 0; g < ngroups; ++g) s += __ldcg(A.gpartials + (size_t)g * PL + idx);
+        for (int g = 0; g < ngroups; g += 4) {
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = g + u < ngroups ? __ldcg(A.gpartials + (size_t)(g + u) * PL + idx) : 0.0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (g + u < ngroups) s += v[u];
+        }
         tot[idx] = s;
     }
     if (tid == 0) atomicExch(&A.clk->cnt_top, 0u);
