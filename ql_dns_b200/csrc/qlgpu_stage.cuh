@@ -387,19 +387,6 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
             break;
         }
         // ---- forward transform and the update of one field
-        // Transforms of up to 8 points per thread: the previous stage's rhs of the field
-        // updated after this transform is loaded now, so that the transform covers the L2
-        // latency instead of every update chunk waiting for it.
-        constexpr bool PRE = Pn <= 8;
-        cplx fpa[PRE ? Pn : 1];
-        if constexpr (PRE) {
-            const cplx* fq = (fupd >= 0 && Fp) ? Fp + fupd * P.nz : nullptr;
-#pragma unroll
-            for (int k2 = 0; k2 < Pn; ++k2) {
-                const int s = stored_index<G>(t + G::T * k2);
-                fpa[k2] = (fq && s >= 0) ? ldc(fq + s) : mk(0.0, 0.0);
-            }
-        }
         if (trs) A.trace[25] = ctimer();
         fwd_fft<G>(x, xch, tw, t, gmask);
         if (trs) A.trace[26] = ctimer();
@@ -440,8 +427,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
                 const int s = stored_index<G>(t + G::T * (4 * c4 + i));
                 const int sl = s < 0 ? 0 : s;
                 uin[i] = ldu<STG>(fin + sl);
-                if constexpr (PRE) fpv[i] = fpa[4 * c4 + i];
-                else fpv[i] = fpp ? ldc(fpp + sl) : mk(0.0, 0.0);
+                fpv[i] = fpp ? ldc(fpp + sl) : mk(0.0, 0.0);
                 l0[i] = ldu<STG>(lin0 + sl);
                 l1[i] = ldu<STG>(zin + sl);
             }
