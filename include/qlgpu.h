@@ -199,12 +199,15 @@ int qlgpu_adjoint_maxwell(qlgpu_t* h, double t0, const double* lin0, const doubl
                           int nsteps, int checkpoint_every, double* J, double* grad_lin, double* grad_mf);
 
 /* The same for nseeds initial states at once, one handle per seed (handles of
- * equal dimensions, each with its own stream): every phase of the sweeps
- * (forward steps, checkpoint restore, window recompute, reverse steps) is
- * enqueued for all seeds before the next, so the seeds' kernels run
- * concurrently on the device.  lin0 [nseeds][nxy][4][nz], mf0 [nseeds][nmf][nz],
- * kx0 [nseeds][nxy] or NULL; J [nseeds], grad_lin / grad_mf like lin0 / mf0.
- * Each seed's results equal those of qlgpu_adjoint_maxwell on its handle. */
+ * equal dimensions).  The forward sweep and every window recompute of all
+ * seeds run in the persistent batch kernel (one launch per window); the
+ * reverse sweep launches each of its kernels once for all seeds when the
+ * seeds share every parameter, else per seed on the seed's stream.
+ * lin0 [nseeds][nxy][4][nz], mf0 [nseeds][nmf][nz], kx0 [nseeds][nxy] or
+ * NULL; J [nseeds], grad_lin / grad_mf like lin0 / mf0.  Each seed's results
+ * equal those of qlgpu_adjoint_maxwell on its handle to round-off (the batch
+ * kernel sums in another order); with the environment variable
+ * QLGPU_ADJ_BATCH=streams every seed runs the single-case path, bit for bit. */
 int qlgpu_adjoint_maxwell_batch(qlgpu_t* const* handles, int nseeds, double t0, const double* lin0,
                                 const double* mf0, const double* kx0, int nsteps, int checkpoint_every, double* J,
                                 double* grad_lin, double* grad_mf);

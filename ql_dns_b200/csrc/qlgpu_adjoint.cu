@@ -29,6 +29,12 @@ struct AdjOps {
                   const double*, double, cplx*, cudaStream_t);
     const void* modes_kernel;
     size_t modes_smem;
+    // one launch for all seeds of a batch (seed = blockIdx.y)
+    void (*mf_pre_s)(const AdjMfArgs&, const DevParams&, const AdjRevPos&, int, cudaStream_t);
+    void (*modes_s)(const AdjStageArgs&, const DevParams&, const AdjRevPos&, int nxy, int, cudaStream_t);
+    void (*mf_post_s)(const cplx*, const DevParams&, const AdjRevPos&, int, cudaStream_t);
+    void (*jgrad_s)(const double*, const int*, const double*, const DevParams&, const AdjRevPos&, int, cudaStream_t);
+    const void* modes_seeds_kernel;
 };
 
 template <int NZ>
@@ -49,6 +55,23 @@ void ops_jgrad(const cplx* U, const double* kx0, const double* ky, const int* ky
     adj_jgrad_kernel<NZ><<<148, 256, 0, st>>>(U, kx0, ky, kyi, il2, P, t, t_dev, w, lam);
 }
 template <int NZ>
+void ops_mf_pre_s(const AdjMfArgs& M, const DevParams& P, const AdjRevPos& X, int ns, cudaStream_t st) {
+    adj_mf_pre_seeds_kernel<NZ><<<dim3(1, ns), 128, 0, st>>>(M, P, X);
+}
+template <int NZ>
+void ops_modes_s(const AdjStageArgs& A, const DevParams& P, const AdjRevPos& X, int nxy, int ns, cudaStream_t st) {
+    adj_modes_seeds_kernel<NZ><<<dim3(nxy, ns), AdjGeom<NZ>::THREADS, AdjGeom<NZ>::BYTES, st>>>(A, P, X);
+}
+template <int NZ>
+void ops_mf_post_s(const cplx* tw, const DevParams& P, const AdjRevPos& X, int ns, cudaStream_t st) {
+    adj_mf_post_seeds_kernel<NZ><<<dim3(1, ns), 64, 0, st>>>(tw, P, X);
+}
+template <int NZ>
+void ops_jgrad_s(const double* ky, const int* kyi, const double* il2, const DevParams& P, const AdjRevPos& X, int ns,
+                 cudaStream_t st) {
+    adj_jgrad_seeds_kernel<NZ><<<dim3(148, ns), 256, 0, st>>>(ky, kyi, il2, P, X);
+}
+template <int NZ>
 AdjOps make_ops() {
     AdjOps o;
     o.mf_pre = &ops_mf_pre<NZ>;
@@ -57,6 +80,11 @@ AdjOps make_ops() {
     o.jgrad = &ops_jgrad<NZ>;
     o.modes_kernel = reinterpret_cast<const void*>(&adj_modes_kernel<NZ>);
     o.modes_smem = AdjGeom<NZ>::BYTES;
+    o.mf_pre_s = &ops_mf_pre_s<NZ>;
+    o.modes_s = &ops_modes_s<NZ>;
+    o.mf_post_s = &ops_mf_post_s<NZ>;
+    o.jgrad_s = &ops_jgrad_s<NZ>;
+    o.modes_seeds_kernel = reinterpret_cast<const void*>(&adj_modes_seeds_kernel<NZ>);
     return o;
 }
 bool pick_ops(int NZ, AdjOps* o) {
@@ -146,6 +174,7 @@ int adj_begin(AdjJob& j, qlgpu_t* h, double t0, const double* lin0, const double
     if (!pick_ops(h->NZ, &j.ops)) return afail(h, QLGPU_ERR_UNSUPPORTED, "unsupported NZ");
     QA_CK(cudaSetDevice(h->device));
     QA_CK(ensure_smem_attr(j.ops.modes_kernel, j.ops.modes_smem));
+    QA_CK(ensure_smem_attr(j.ops.modes_seeds_kernel, j.ops.modes_smem));
     int rc = qlgpu_set_state(h, t0, lin0, mf0, kx0);
     if (rc) return rc;
     j.N = nsteps;
@@ -339,6 +368,60 @@ int adj_backward_step(AdjJob& j, int steps, int n) {
     return QLGPU_OK;
 }
 
+// The reverse sweep of all seeds of a batch on one stream: the same kernels as
+// adj_backward_step, each launched once with one grid row per seed.  Every
+// seed's arithmetic is that of adj_backward_step (results bit for bit equal).
+struct SeedReverse {
+    qlgpu_t* h = nullptr;  // the first seed's handle: tables, parameters, error text
+    AdjOps ops{};
+    const AdjSeedBufs* d_seeds = nullptr;
+    int nseeds = 0;
+    int par = 0;  // stages reversed so far, mod 2
+    size_t nlin = 0, nmfe = 0, nxy = 0;
+    double weight = 0.0;
+};
+
+int adj_backward_step_seeds(SeedReverse& R, cudaStream_t st, int steps, int n) {
+    qlgpu_t* h = R.h;
+    const int ns = R.nseeds;
+    AdjRevPos X;
+    X.seeds = R.d_seeds;
+    X.n = n;
+    X.steps = steps;
+    X.s = 2;
+    X.par = R.par;
+    X.nlin = (long long)R.nlin;
+    X.nmfe = (long long)R.nmfe;
+    X.nxy = (long long)R.nxy;
+    X.weight = R.weight;
+    R.ops.jgrad_s(h->d_ky, h->d_kyi, h->d_ilap2, h->dp, X, ns, st);
+    adj_remap_seeds_kernel<<<dim3(148, ns), 256, 0, st>>>(X, h->nz);
+    for (int s = 2; s >= 0; --s) {
+        X.s = s;
+        X.par = R.par;
+        AdjMfArgs M;
+        std::memset(&M, 0, sizeof(M));
+        M.tw = h->d_tw;
+        M.sc = h->sc[s];
+        R.ops.mf_pre_s(M, h->dp, X, ns, st);
+        AdjStageArgs A;
+        std::memset(&A, 0, sizeof(A));
+        A.ky = h->d_ky;
+        A.kxi = h->d_kxi;
+        A.kyi = h->d_kyi;
+        A.ilap2 = h->d_ilap2;
+        A.tw = h->d_tw;
+        A.sc = h->sc[s];
+        R.ops.modes_s(A, h->dp, X, h->nxy, ns, st);
+        const int nout = 3 * h->NZ;
+        adj_bsum_seeds_kernel<<<dim3((nout + 7) / 8, ns), 256, 0, st>>>(X, nout);
+        R.ops.mf_post_s(h->d_tw, h->dp, X, ns, st);
+        R.par ^= 1;
+    }
+    QA_CK(cudaGetLastError());
+    return QLGPU_OK;
+}
+
 // gradients out, and the handle left at the end of the forward run
 int adj_finish(AdjJob& j, double* grad_lin, double* grad_mf) {
     qlgpu_t* h = j.h;
@@ -361,13 +444,25 @@ int sync_job(AdjJob& j) {
 
 // The seeds' forward sweep and window recompute in the persistent batch kernel
 // (one launch per window for all seeds, the recompute recording every stage's
-// input through the kernel's record pointers); the reverse sweep per seed on
-// its handle's stream as in run_jobs.  The batch's reduction order differs from
+// input through the kernel's record pointers); the reverse sweep on the batch's
+// stream, every kernel launched once for all seeds (per seed on its handle's
+// stream when the seeds differ in a parameter).  The batch's reduction order differs from
 // the single-case kernel's, so each seed's results agree with
 // qlgpu_adjoint_maxwell to round-off rather than bit for bit.
 template <class F>
 int capture(AdjJob& j, cudaGraphExec_t* out, F body);
 int launch_graph(AdjJob& j, cudaGraphExec_t g);
+
+// The reverse sweep runs once for all seeds (adj_backward_step_seeds) when the
+// seeds share every parameter and the device; otherwise per seed.
+bool same_setup(const qlgpu_t* a, const qlgpu_t* b) {
+    const qlgpu_params &p = a->p, &r = b->p;
+    return a->device == b->device && p.model == r.model && p.integrator == r.integrator && p.nx == r.nx &&
+           p.ny == r.ny && p.NZ == r.NZ && p.L[0] == r.L[0] && p.L[1] == r.L[1] && p.L[2] == r.L[2] && p.q == r.q &&
+           p.omega == r.omega && p.nu == r.nu && p.eta == r.eta && p.B0z == r.B0z &&
+           p.viscosity_order == r.viscosity_order && p.dt == r.dt && p.remap == r.remap &&
+           p.quasilinear == r.quasilinear;
+}
 
 struct BatchGuard {
     qlgpu_batch_t* b = nullptr;
@@ -443,6 +538,47 @@ int run_jobs_persistent(std::vector<AdjJob>& jobs, double t0, const double* lin0
         rc = adj_alloc_backward(j);
         if (rc) return rc;
     }
+    // the reverse sweep: one launch per kernel for all seeds (default), or every seed on its
+    // own stream (QLGPU_ADJ_REVERSE=streams, or seeds that differ in a parameter)
+    const char* renv = getenv("QLGPU_ADJ_REVERSE");
+    bool seeds_rev = !(renv && std::string(renv) == "streams");
+    for (int q = 1; q < nj; ++q)
+        if (!same_setup(jobs[q].h, h0)) seeds_rev = false;
+    Pool tab;
+    SeedReverse R;
+    if (seeds_rev) {
+        std::vector<AdjSeedBufs> hb(nj);
+        for (int q = 0; q < nj; ++q) {
+            const AdjJob& j = jobs[q];
+            AdjSeedBufs& e = hb[q];
+            e.stU = j.stU;
+            e.stB = j.stB;
+            e.postU = j.postU;
+            e.kx_pre = j.kx_pre;
+            e.kx_post = j.kx_post;
+            e.t_pre = j.t_pre;
+            for (int i = 0; i < 2; ++i) {
+                e.lamU[i] = j.lamU[i];
+                e.lamB[i] = j.lamB[i];
+                e.lamF[i] = j.lamF[i];
+                e.lamG[i] = j.lamG[i];
+            }
+            e.prof = j.prof;
+            e.bpart = j.bpart;
+            e.bsum = j.bsum;
+        }
+        AdjSeedBufs* d = nullptr;
+        QA_CK(tab.get(&d, (size_t)nj));
+        QA_CK(cudaMemcpy(d, hb.data(), sizeof(AdjSeedBufs) * nj, cudaMemcpyHostToDevice));
+        R.h = h0;
+        R.ops = jobs[0].ops;
+        R.d_seeds = d;
+        R.nseeds = nj;
+        R.nlin = nlin;
+        R.nmfe = nmfe;
+        R.nxy = nxy;
+        R.weight = 1.0 / N;
+    }
     // ---- reverse sweep, window by window
     cudaEvent_t ev_b = nullptr;
     std::vector<cudaEvent_t> ev_h(nj, nullptr);
@@ -461,7 +597,7 @@ int run_jobs_persistent(std::vector<AdjJob>& jobs, double t0, const double* lin0
     for (int w = NC - 1; w >= 0; --w) {
         const int steps = std::min(N, w * C + C) - w * C;
         // the previous window's reverse steps must be done with stU before the recompute rewrites it
-        if (w != NC - 1)
+        if (w != NC - 1 && !seeds_rev)
             for (int q = 0; q < nj; ++q) {
                 QA_CK(cudaEventRecord(ev_h[q], jobs[q].h->stream));
                 QA_CK(cudaStreamWaitEvent(bs, ev_h[q], 0));
@@ -492,6 +628,13 @@ int run_jobs_persistent(std::vector<AdjJob>& jobs, double t0, const double* lin0
             QA_CK(cudaMemcpyAsync(j.kx_post, d.kx0, nxy * sizeof(double), cudaMemcpyDeviceToDevice, bs));
             QA_CK(cudaMemcpyAsync(j.t_pre + steps, &d.clk->t, sizeof(double), cudaMemcpyDeviceToDevice, bs));
         }
+        if (seeds_rev) {
+            for (int n = steps - 1; n >= 0; --n) {
+                rc = adj_backward_step_seeds(R, bs, steps, n);
+                if (rc) return rc;
+            }
+            continue;
+        }
         QA_CK(cudaEventRecord(ev_b, bs));
         for (int q = 0; q < nj; ++q) {
             AdjJob& j = jobs[q];
@@ -516,6 +659,19 @@ int run_jobs_persistent(std::vector<AdjJob>& jobs, double t0, const double* lin0
                 rc = adj_backward_step(j, steps, n);
                 if (rc) return rc;
             }
+        }
+    }
+    if (seeds_rev) {
+        // every seed's buffers in the state adj_backward_step would have left them
+        QA_CK(cudaEventRecord(ev_b, bs));
+        for (int q = 0; q < nj; ++q) {
+            AdjJob& j = jobs[q];
+            j.iu = j.ib = R.par;
+            if (R.par) {
+                std::swap(j.lamF[0], j.lamF[1]);
+                std::swap(j.lamG[0], j.lamG[1]);
+            }
+            QA_CK(cudaStreamWaitEvent(j.h->stream, ev_b, 0));
         }
     }
     for (int q = 0; q < nj; ++q) qlgpu_batch_set_record(b, q, nullptr, nullptr, nullptr, nullptr);

@@ -57,6 +57,10 @@ struct AdjGeom {
     static constexpr size_t o_rw = o_prof + sizeof(double) * 5 * NZ;
     static constexpr size_t o_xch = o_rw + sizeof(cplx) * 14 * NZ;
     static constexpr size_t BYTES = o_xch + sizeof(cplx) * NG * G::XSIZE;
+    // E of the four fields at every stored index, [4][nz]: in the exchange buffers of
+    // groups 14 and 15, which no transform phase uses (14 inverse, 9 forward transforms)
+    static constexpr size_t o_etab = o_xch + sizeof(cplx) * 14 * G::XSIZE;
+    static_assert(sizeof(double) * 4 * G::nz <= sizeof(cplx) * 2 * G::XSIZE, "E table fits two exchange buffers");
 };
 
 // E = exp(linC L_f) of field f at stored index s (RK3CN_Elin.cpp:102-104), L at the stage end.
@@ -65,8 +69,10 @@ __device__ __forceinline__ double adj_efac(const DevParams& P, const StageConst&
     return exp(__dmul_rn(S.linC, linop_f<MODEL_BQLIN>(P, lap_end<MODEL_BQLIN>(P, kxe, ky, kz2), f)));
 }
 
+// The stage adjoint of one mode (one CTA).  A may live in parameter space (one
+// seed per launch) or in shared memory (a launch over many seeds).
 template <int NZ>
-__global__ void __launch_bounds__(AdjGeom<NZ>::THREADS, 6) adj_modes_kernel(AdjStageArgs A, DevParams P) {
+__device__ __forceinline__ void adj_modes_body(const AdjStageArgs& A, const DevParams& P, const int mode) {
     using G = Geom<NZ>;
     using AG = AdjGeom<NZ>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -79,7 +85,6 @@ __global__ void __launch_bounds__(AdjGeom<NZ>::THREADS, 6) adj_modes_kernel(AdjS
     const unsigned gmask =
         (G::T == 32 ? 0xffffffffu : (((1u << G::T) - 1u) << ((lane / G::T) * G::T)));
     cplx* xch = reinterpret_cast<cplx*>(smem_raw + AG::o_xch) + (size_t)g * G::XSIZE;
-    const int mode = blockIdx.x;
     const int nz = P.nz;
     for (int i = tid; i < NZ; i += blockDim.x) tw_s[i] = A.tw[i];
     for (int i = tid; i < 5 * NZ; i += blockDim.x) prof[i] = A.prof[i];
@@ -99,12 +104,17 @@ __global__ void __launch_bounds__(AdjGeom<NZ>::THREADS, 6) adj_modes_kernel(AdjS
     const cplx* lo = A.lamU_out + (size_t)mode * 4 * nz;
     const cplx* lf = A.lamF_out ? A.lamF_out + (size_t)mode * 4 * nz : nullptr;
     const double* il2row = A.ilap2 + (size_t)kyi * nz;
+    double* etab = reinterpret_cast<double*>(smem_raw + AG::o_etab);
+    for (int i = tid; i < 4 * nz; i += blockDim.x) {
+        const int f = i / nz, s = i % nz;
+        const int kzi = s <= G::H ? s : s - nz;
+        etab[i] = adj_efac(P, S, kxe, ky, kz2val(kzval(kzi, P.kzL)), f);
+    }
     __syncthreads();
 
     // lamF of field f at stored index s: n1 E lamU' + lamF_out
-    auto lamF = [&](int f, int s, double kz2) -> cplx {
-        const double e = adj_efac(P, S, kxe, ky, kz2, f);
-        cplx r = cscale(lo[f * nz + s], __dmul_rn(S.n1, e));
+    auto lamF = [&](int f, int s, double) -> cplx {
+        cplx r = cscale(lo[f * nz + s], __dmul_rn(S.n1, etab[f * nz + s]));
         if (lf) r = cadd(r, lf[f * nz + s]);
         return r;
     };
@@ -226,8 +236,7 @@ __global__ void __launch_bounds__(AdjGeom<NZ>::THREADS, 6) adj_modes_kernel(AdjS
         const double kz2 = kz2val(c);
         const bool z0 = (kyi == 0 && s == 0);
         const double il2 = il2row[s];
-        const double e = adj_efac(P, S, kxe, ky, kz2, f);
-        const cplx mu = cscale(lo[f * nz + s], e);
+        const cplx mu = cscale(lo[f * nz + s], etab[idx]);
         cplx r = mu;
         if (f == 0 || f == 1) {
             // uz = (a c u - i b zeta) il2, i c uz, uy = (a b u + i c zeta) il2
@@ -270,6 +279,71 @@ __global__ void __launch_bounds__(AdjGeom<NZ>::THREADS, 6) adj_modes_kernel(AdjS
     }
 }
 
+template <int NZ>
+__global__ void __launch_bounds__(AdjGeom<NZ>::THREADS, 6)
+    adj_modes_kernel(const __grid_constant__ AdjStageArgs A, const __grid_constant__ DevParams P) {
+    adj_modes_body<NZ>(A, P, blockIdx.x);
+}
+
+// ---- the reverse sweep of many seeds at once (same dimensions and parameters):
+// every kernel of a reverse step runs once for all seeds, seed = blockIdx.y.
+// The per-seed buffers are read from a device table; the position in the sweep
+// (step n of a window of `steps`, stage s, buffer parity) is a launch argument.
+struct AdjSeedBufs {
+    const cplx* stU;       // [C][3] recorded stage inputs
+    const cplx* stB;       // [C][3] recorded stage mean fields
+    const cplx* postU;     // the window's end state
+    const double* kx_pre;  // [C] kx0 at every step start
+    const double* kx_post; // kx0 at the window end
+    const double* t_pre;   // [C + 1] step start times
+    cplx* lamU[2];
+    cplx* lamB[2];
+    cplx* lamF[2];
+    cplx* lamG[2];
+    double* prof;
+    double* bpart;
+    double* bsum;
+};
+
+struct AdjRevPos {
+    const AdjSeedBufs* seeds;
+    int n, steps, s;
+    int par;  // stages already reversed, mod 2: lamU[par] is the current adjoint state
+    long long nlin, nmfe, nxy;
+    double weight;  // of AM_b in J
+};
+
+// the post-step state of step n and its kx0 (the window end for the last step)
+__device__ __forceinline__ const cplx* adj_upost(const AdjSeedBufs& B, const AdjRevPos& X) {
+    return X.n + 1 < X.steps ? B.stU + (size_t)(X.n + 1) * 3 * X.nlin : B.postU;
+}
+__device__ __forceinline__ const double* adj_kxpost(const AdjSeedBufs& B, const AdjRevPos& X) {
+    return X.n + 1 < X.steps ? B.kx_pre + (size_t)(X.n + 1) * X.nxy : B.kx_post;
+}
+
+template <int NZ>
+__global__ void __launch_bounds__(AdjGeom<NZ>::THREADS, 6)
+    adj_modes_seeds_kernel(const __grid_constant__ AdjStageArgs base, const __grid_constant__ DevParams P,
+                           const __grid_constant__ AdjRevPos X) {
+    __shared__ __align__(16) AdjStageArgs sA;
+    if (threadIdx.x == 0) {
+        const AdjSeedBufs& B = X.seeds[blockIdx.y];
+        const int p = X.par;
+        sA = base;
+        sA.U = B.stU + ((size_t)X.n * 3 + X.s) * X.nlin;
+        sA.lamU_out = B.lamU[p];
+        sA.lamF_out = X.s == 2 ? nullptr : B.lamF[p];
+        sA.lamU_in = B.lamU[p ^ 1];
+        sA.lamFp = X.s == 0 ? nullptr : B.lamF[p ^ 1];
+        sA.kx0 = B.kx_pre + (size_t)X.n * X.nxy;
+        sA.prof = B.prof;
+        sA.bpart = B.bpart;
+        sA.t_dev = B.t_pre + X.n;
+    }
+    __syncthreads();
+    adj_modes_body<NZ>(sA, P, blockIdx.x);
+}
+
 // Mean-field part before the mode pass: forward profiles of the stage input
 // mean field (By, dBy, ddBy; MHD_BQlin.cpp:122-127), the adjoint stress
 // profiles px, py, and the RK / mean-field-rhs adjoint of B:
@@ -289,7 +363,7 @@ struct AdjMfArgs {
 };
 
 template <int NZ>
-__global__ void adj_mf_pre_kernel(AdjMfArgs A, DevParams P) {
+__device__ __forceinline__ void adj_mf_pre_body(const AdjMfArgs& A, const DevParams& P) {
     using G = Geom<NZ>;
     __shared__ __align__(16) cplx tw_s[NZ];
     __shared__ __align__(16) cplx lamG[2][G::nz];
@@ -344,9 +418,33 @@ __global__ void adj_mf_pre_kernel(AdjMfArgs A, DevParams P) {
     }
 }
 
+template <int NZ>
+__global__ void adj_mf_pre_kernel(const __grid_constant__ AdjMfArgs A, const __grid_constant__ DevParams P) {
+    adj_mf_pre_body<NZ>(A, P);
+}
+
+template <int NZ>
+__global__ void adj_mf_pre_seeds_kernel(const __grid_constant__ AdjMfArgs base, const __grid_constant__ DevParams P,
+                                        const __grid_constant__ AdjRevPos X) {
+    __shared__ __align__(16) AdjMfArgs sM;
+    if (threadIdx.x == 0) {
+        const AdjSeedBufs& B = X.seeds[blockIdx.y];
+        const int p = X.par;
+        sM = base;
+        sM.B = B.stB + ((size_t)X.n * 3 + X.s) * X.nmfe;
+        sM.lamB_out = B.lamB[p];
+        sM.lamG_out = X.s == 2 ? nullptr : B.lamG[p];
+        sM.lamB_in = B.lamB[p ^ 1];
+        sM.lamGp = X.s == 0 ? nullptr : B.lamG[p ^ 1];
+        sM.prof = B.prof;
+    }
+    __syncthreads();
+    adj_mf_pre_body<NZ>(sM, P);
+}
+
 // Sum of the per-mode profile adjoints over modes, one warp per (profile, z),
 // fixed order (lane-strided partial sums, then a shuffle tree).
-__global__ void adj_bsum_kernel(const double* bpart, int nxy, int n_out, double* bsum) {
+__device__ __forceinline__ void adj_bsum_body(const double* bpart, int nxy, int n_out, double* bsum) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (w >= n_out) return;
     const double* row = bpart + (size_t)w * nxy;
@@ -357,10 +455,20 @@ __global__ void adj_bsum_kernel(const double* bpart, int nxy, int n_out, double*
     if (lane == 0) bsum[w] = s;
 }
 
+__global__ void adj_bsum_kernel(const double* bpart, int nxy, int n_out, double* bsum) {
+    adj_bsum_body(bpart, nxy, n_out, bsum);
+}
+
+__global__ void adj_bsum_seeds_kernel(const __grid_constant__ AdjRevPos X, int n_out) {
+    const AdjSeedBufs& B = X.seeds[blockIdx.y];
+    adj_bsum_body(B.bpart, (int)X.nxy, n_out, B.bsum);
+}
+
 // lamB_y += fac (T(pBy) - i c T(pdBy) - c^2 T(pddBy)): the adjoint of the
 // mean-field profiles of the stage (MHD_BQlin.cpp:122-127).  One CTA.
 template <int NZ>
-__global__ void adj_mf_post_kernel(const double* bsum, const cplx* tw, DevParams P, cplx* lamB_in) {
+__device__ __forceinline__ void adj_mf_post_body(const double* bsum, const cplx* tw, const DevParams& P,
+                                                 cplx* lamB_in) {
     using G = Geom<NZ>;
     __shared__ __align__(16) cplx tw_s[NZ];
     __shared__ __align__(16) cplx xchs[3][G::XSIZE];
@@ -389,13 +497,26 @@ __global__ void adj_mf_post_kernel(const double* bsum, const cplx* tw, DevParams
     }
 }
 
+template <int NZ>
+__global__ void adj_mf_post_kernel(const double* bsum, const cplx* tw, const __grid_constant__ DevParams P,
+                                   cplx* lamB_in) {
+    adj_mf_post_body<NZ>(bsum, tw, P, lamB_in);
+}
+
+template <int NZ>
+__global__ void adj_mf_post_seeds_kernel(const cplx* tw, const __grid_constant__ DevParams P,
+                                         const __grid_constant__ AdjRevPos X) {
+    const AdjSeedBufs& B = X.seeds[blockIdx.y];
+    adj_mf_post_body<NZ>(B.bsum, tw, P, B.lamB[X.par ^ 1]);
+}
+
 // Gradient of (weight) * AM_b at a post-step state (MHD_BQlin.cpp:388-392,424):
 // AM_b = divfac sum mult Re(b conj(by)), by = (a b_y b + i c eta) il2 gives
 // d/db = 2 a b_y il2 b + i c il2 eta, d/deta = -i c il2 b.  Adds to lamU.
 template <int NZ>
-__global__ void adj_jgrad_kernel(const cplx* U, const double* kx0, const double* ky, const int* kyi,
-                                 const double* ilap2, DevParams P, double t_host, const double* t_dev, double weight,
-                                 cplx* lamU) {
+__device__ __forceinline__ void adj_jgrad_body(const cplx* U, const double* kx0, const double* ky, const int* kyi,
+                                               const double* ilap2, const DevParams& P, double t_host,
+                                               const double* t_dev, double weight, cplx* lamU) {
     using G = Geom<NZ>;
     const int nz = P.nz;
     const double t = t_dev ? *t_dev : t_host;
@@ -419,14 +540,40 @@ __global__ void adj_jgrad_kernel(const cplx* U, const double* kx0, const double*
     }
 }
 
+template <int NZ>
+__global__ void adj_jgrad_kernel(const cplx* U, const double* kx0, const double* ky, const int* kyi,
+                                 const double* ilap2, const __grid_constant__ DevParams P, double t_host,
+                                 const double* t_dev, double weight, cplx* lamU) {
+    adj_jgrad_body<NZ>(U, kx0, ky, kyi, ilap2, P, t_host, t_dev, weight, lamU);
+}
+
+// J's gradient at the post-step state of step n (seed = blockIdx.y)
+template <int NZ>
+__global__ void adj_jgrad_seeds_kernel(const double* ky, const int* kyi, const double* ilap2,
+                                       const __grid_constant__ DevParams P, const __grid_constant__ AdjRevPos X) {
+    const AdjSeedBufs& B = X.seeds[blockIdx.y];
+    adj_jgrad_body<NZ>(adj_upost(B, X), adj_kxpost(B, X), ky, kyi, ilap2, P, 0.0, B.t_pre + X.n + 1, X.weight,
+                       B.lamU[X.par]);
+}
+
 // Adjoint of the shearing-box remap (MHD_BQlin.cpp:319-329): the fields of a
 // remapped mode were set to zero, so their adjoint is zero.
-__global__ void adj_remap_kernel(const double* kx0_before, const double* kx0_after, int nxy, int nz, cplx* lamU) {
+__device__ __forceinline__ void adj_remap_body(const double* kx0_before, const double* kx0_after, int nxy, int nz,
+                                               cplx* lamU) {
     const size_t n = (size_t)nxy * 4 * nz;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const int mode = (int)(i / (4 * (size_t)nz));
         if (kx0_before[mode] != kx0_after[mode]) lamU[i] = mk(0.0, 0.0);
     }
+}
+
+__global__ void adj_remap_kernel(const double* kx0_before, const double* kx0_after, int nxy, int nz, cplx* lamU) {
+    adj_remap_body(kx0_before, kx0_after, nxy, nz, lamU);
+}
+
+__global__ void adj_remap_seeds_kernel(const __grid_constant__ AdjRevPos X, int nz) {
+    const AdjSeedBufs& B = X.seeds[blockIdx.y];
+    adj_remap_body(B.kx_pre + (size_t)X.n * X.nxy, adj_kxpost(B, X), (int)X.nxy, nz, B.lamU[X.par]);
 }
 
 }  // namespace qlgpu

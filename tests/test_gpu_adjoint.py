@@ -177,9 +177,11 @@ def test_window_graphs_equal_direct_launches(monkeypatch):
 
 
 def test_batch_reverse_graphs_equal_direct_launches(monkeypatch):
-    # QLGPU_ADJ_GRAPH=1: the persistent path replays every full reverse window (even
-    # checkpoint interval) as one graph per seed; with 0 every kernel is launched directly
+    # QLGPU_ADJ_REVERSE=streams with QLGPU_ADJ_GRAPH=1: the persistent path replays every full
+    # reverse window (even checkpoint interval) as one graph per seed; with 0 every kernel is
+    # launched directly
     require_gpu()
+    monkeypatch.setenv("QLGPU_ADJ_REVERSE", "streams")
     monkeypatch.setenv("QLGPU_ADJ_GRAPH", "1")
     p = mri_16x16_nz32(nx=8, ny=8, NZ=32)
     sts = [initial_state(p, 30 + k, sigma=0.2) for k in range(2)]
@@ -196,3 +198,52 @@ def test_batch_reverse_graphs_equal_direct_launches(monkeypatch):
     with QLSolver(p) as s:
         J, g, _ = s.adjoint_maxwell(0.0, *sts[1], 22, 6)
     assert abs(a[0][1] - J) <= 1e-12 * abs(J) and rel(a[1][1], g) < 1e-10
+
+
+@pytest.mark.parametrize("ck", [6, 5])
+def test_seed_batched_reverse_equals_per_seed_reverse(ck, monkeypatch):
+    # default: the reverse sweep launches each kernel once for all seeds (grid row = seed);
+    # QLGPU_ADJ_REVERSE=streams: every seed's reverse on its own stream.  Same arithmetic per
+    # seed, so the gradients agree bit for bit (odd and even checkpoint intervals, a partial
+    # last window, remaps inside the run)
+    require_gpu()
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=32)
+    sts = [initial_state(p, 40 + k, sigma=0.2) for k in range(3)]
+    args = (0.0, [s[0] for s in sts], [s[1] for s in sts], [s[2] for s in sts], 23, ck)
+    solvers = [QLSolver(p) for _ in sts]
+    try:
+        monkeypatch.setenv("QLGPU_ADJ_REVERSE", "seeds")
+        a = QLSolver.adjoint_maxwell_batch(solvers, *args)
+        monkeypatch.setenv("QLGPU_ADJ_REVERSE", "streams")
+        b = QLSolver.adjoint_maxwell_batch(solvers, *args)
+        for k in range(3):
+            t, lo, mo, ko = solvers[k].get_state()
+            t2, lo2, mo2, ko2, _ = O.run(p, 0.0, *sts[k], 23)
+            assert rel(lo, lo2) < 1e-10 and np.array_equal(ko, ko2)
+    finally:
+        for s in solvers:
+            s.close()
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    d = directions(sts[2][0].shape, 1, 5, np.linalg.norm(sts[2][0]))[0]
+    _, dJ = O.tlm_maxwell(p, 0.0, *sts[2], d, None, 23)
+    assert abs(float(np.real(np.vdot(a[1][2], d))) - dJ) <= 1e-8 * abs(dJ)
+
+
+def test_seeds_with_different_parameters_reverse_per_seed():
+    # seeds whose parameters differ (here eta) cannot share the batched reverse launches: each
+    # runs its own reverse sweep, with the same gradient as a single-seed call to round-off
+    require_gpu()
+    p1 = mri_16x16_nz32(nx=8, ny=8, NZ=32)
+    p2 = mri_16x16_nz32(nx=8, ny=8, NZ=32, eta=p1.eta * 2)
+    sts = [initial_state(p1, 50 + k, sigma=0.2) for k in range(2)]
+    solvers = [QLSolver(p1), QLSolver(p2)]
+    try:
+        J, gl, gm = QLSolver.adjoint_maxwell_batch(solvers, 0.0, [s[0] for s in sts], [s[1] for s in sts],
+                                                   [s[2] for s in sts], 12, 4)
+    finally:
+        for s in solvers:
+            s.close()
+    for k, pk in enumerate((p1, p2)):
+        with QLSolver(pk) as s:
+            J1, g1, m1 = s.adjoint_maxwell(0.0, *sts[k], 12, 4)
+        assert abs(J[k] - J1) <= 1e-12 * abs(J1) and rel(gl[k], g1) < 1e-10 and rel(gm[k], m1) < 1e-10
