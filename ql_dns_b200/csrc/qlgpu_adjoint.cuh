@@ -173,44 +173,62 @@ __device__ __forceinline__ void adj_modes_body(const AdjStageArgs& A, const DevP
     const double* ddBy = prof + 2 * NZ;
     const double* px = prof + 3 * NZ;
     const double* py = prof + 4 * NZ;
-    for (int z = tid; z < NZ; z += blockDim.x) {
-        const cplx Ru = RW[0 * NZ + z], Rz = RW[1 * NZ + z], Rb = RW[2 * NZ + z], Re_ = RW[3 * NZ + z];
-        const cplx Ruz = RW[4 * NZ + z], Rbz = RW[5 * NZ + z], Rik = RW[6 * NZ + z];
+    // lamR = sum of conj(multiplier) W over the terms a field enters (reads slots 0..13 at z)
+    auto lam_r = [&](int z, cplx* o) {
+        const cplx Ru = RW[0 * NZ + z], Rb = RW[2 * NZ + z];
+        const cplx Ruz = RW[4 * NZ + z], Rbz = RW[5 * NZ + z];
         const cplx Ruy = RW[7 * NZ + z], Rby = RW[8 * NZ + z];
         const cplx Wb = RW[9 * NZ + z], Wz = RW[10 * NZ + z], We = RW[11 * NZ + z];
         const cplx WS = RW[12 * NZ + z], Wu2 = RW[13 * NZ + z];
         const double by = By[z], dby = dBy[z], ddby = ddBy[z];
         const double mx = mult * px[z], my = mult * py[z];
         const double bBy = b * by, adBy = a * dby;
-        // lamR = sum of conj(multiplier) W over the terms a field enters
-        const cplx lRu = cadd(cadd(imul(Wb, -bBy), imul(We, adBy)), cscale(Rbz, mx));
-        const cplx lRz = imul(We, -bBy);
-        const cplx lRb = csub(cadd(imul(Wz, adBy), imul(WS, -bBy)), cscale(Ruz, mx));
-        const cplx lRe = imul(Wz, -bBy);
-        const cplx lRuz = csub(csub(cscale(We, -ddby), cscale(Rb, mx)), cscale(Rby, my));
-        const cplx lRbz = cadd(cadd(cscale(Wz, ddby), cscale(Wu2, 2.0 * ab * dby)), cadd(cscale(Ru, mx), cscale(Ruy, my)));
-        const cplx lRik = cscale(We, -2.0 * dby);
-        const cplx lRuy = cscale(Rbz, my);
-        const cplx lRby = cscale(Ruz, -my);
-        // adjoint of the mean-field profiles: Re(conj(multiplier * R) W) per term
+        o[0] = cadd(cadd(imul(Wb, -bBy), imul(We, adBy)), cscale(Rbz, mx));
+        o[1] = imul(We, -bBy);
+        o[2] = csub(cadd(imul(Wz, adBy), imul(WS, -bBy)), cscale(Ruz, mx));
+        o[3] = imul(Wz, -bBy);
+        o[4] = csub(csub(cscale(We, -ddby), cscale(Rb, mx)), cscale(Rby, my));
+        o[5] = cadd(cadd(cscale(Wz, ddby), cscale(Wu2, 2.0 * ab * dby)), cadd(cscale(Ru, mx), cscale(Ruy, my)));
+        o[6] = cscale(We, -2.0 * dby);
+        o[7] = cscale(Rbz, my);
+        o[8] = cscale(Ruz, -my);
+    };
+    // adjoint of the mean-field profiles at z: Re(conj(multiplier * R) W) per term
+    auto prof_adj = [&](int z) {
+        const cplx Ru = RW[0 * NZ + z], Rz = RW[1 * NZ + z], Rb = RW[2 * NZ + z], Re_ = RW[3 * NZ + z];
+        const cplx Ruz = RW[4 * NZ + z], Rbz = RW[5 * NZ + z], Rik = RW[6 * NZ + z];
+        const cplx Wb = RW[9 * NZ + z], Wz = RW[10 * NZ + z], We = RW[11 * NZ + z];
+        const cplx WS = RW[12 * NZ + z], Wu2 = RW[13 * NZ + z];
         auto re_cw = [](cplx r, cplx w) { return r.x * w.x + r.y * w.y; };  // Re(conj(r) w)
         auto re_icw = [](cplx r, cplx w) { return r.y * w.x - r.x * w.y; };  // Re(i conj(r) w)
         const double pBy = -b * (re_icw(Ru, Wb) + re_icw(Re_, Wz) + re_icw(Rz, We) + re_icw(Rb, WS));
         const double pdBy = a * (re_icw(Rb, Wz) + re_icw(Ru, We)) - 2.0 * re_cw(Rik, We) + 2.0 * ab * re_cw(Rbz, Wu2);
         const double pddBy = re_cw(Rbz, Wz) - re_cw(Ruz, We);
-        RW[0 * NZ + z] = lRu;
-        RW[1 * NZ + z] = lRz;
-        RW[2 * NZ + z] = lRb;
-        RW[3 * NZ + z] = lRe;
-        RW[4 * NZ + z] = lRuz;
-        RW[5 * NZ + z] = lRbz;
-        RW[6 * NZ + z] = lRik;
-        RW[7 * NZ + z] = lRuy;
-        RW[8 * NZ + z] = lRby;
         const size_t nxy = (size_t)P.nxy;
         A.bpart[(0 * (size_t)NZ + z) * nxy + mode] = pBy;
         A.bpart[(1 * (size_t)NZ + z) * nxy + mode] = pdBy;
         A.bpart[(2 * (size_t)NZ + z) * nxy + mode] = pddBy;
+    };
+    if constexpr (AG::THREADS >= 2 * NZ) {
+        // two threads per z: lamR in the first NZ threads, the profile adjoints in the
+        // next NZ; slots 0..8 are overwritten only after both have read them
+        const int z = tid % NZ, part = tid / NZ;
+        cplx o[9];
+        if (part == 0) lam_r(z, o);
+        else if (part == 1) prof_adj(z);
+        __syncthreads();
+        if (part == 0) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) RW[k * NZ + z] = o[k];
+        }
+    } else {
+        for (int z = tid; z < NZ; z += blockDim.x) {
+            cplx o[9];
+            lam_r(z, o);
+            prof_adj(z);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) RW[k * NZ + z] = o[k];
+        }
     }
     __syncthreads();
 
