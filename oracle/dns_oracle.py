@@ -42,18 +42,33 @@ import math
 
 import numpy as np
 
-from ql_dns_b200.ktables import ktables
-
 A0, A1, A2 = 8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0
 B1, B2 = -17.0 / 60.0, -5.0 / 12.0
 P1, P2 = 8.0 / 15.0, 2.0 / 3.0
+
+
+def kdata(q) -> dict:
+    """Wavenumber tables of the (kx, ky) columns and of kz, restated from
+    QL_DNS/Auxiliary/Kdata.cpp:24-46 (columns ordered j + (Ny/2) i: kx integers
+    0 .. Nx/2-1 then -(Nx/2-1) .. -1, the Nyquist column dropped; ky integers
+    0 .. Ny/2-1) and Kdata.cpp:74-78 (kz integers 0 .. (nz-1)/2 then
+    -(nz-1)/2 .. -1).  The oracle keeps its own copy so that a table error in the
+    package cannot hide in both the initial state and its check."""
+    nxh, nyh = q.nx // 2, (q.ny // 2 * 2) // 2
+    ix = np.concatenate([np.arange(nxh), np.arange(1 - nxh, 0)])
+    kxi = np.repeat(ix, nyh)
+    kyi = np.tile(np.arange(nyh), ix.size)
+    nzl = (q.nz - 1) // 2
+    kzi = np.concatenate([np.arange(nzl + 1), np.arange(-nzl, 0)])
+    return {"kx": kxi * (2 * math.pi / q.L[0]), "ky": kyi * (2 * math.pi / q.L[1]), "kx_index": kxi,
+            "ky_index": kyi, "kz": kzi * (2 * math.pi / q.L[2])}
 
 
 class DNSOracle:
     def __init__(self, p):
         self.p = p
         q = p.ql()
-        kt = ktables(q)
+        kt = kdata(q)
         self.kt = kt
         self.nxy, self.nz, self.nx, self.ny = q.nxy, q.nz, q.nx, q.ny
         self.Kyn = q.ny // 2
@@ -269,7 +284,7 @@ def from_ql(p, t, lin4, mf, kx0):
     """DNS columns from a FullQlin state (u, zeta, b, eta; Bx, By, Ux, Uy),
     reconstructing u_y, u_z, b_y, b_z as MHD_FullQlin.cpp:220-265 at time t."""
     q = p.ql()
-    kt = ktables(q)
+    kt = kdata(q)
     kxc = 1j * (np.asarray(kx0) + q.q * t * kt["ky"])[:, None]
     kyc = 1j * kt["ky"][:, None]
     kzc = 1j * kt["kz"][None, :]
@@ -290,7 +305,7 @@ def from_ql(p, t, lin4, mf, kx0):
 def to_ql(p, t, lin6, kx0):
     """(lin4, mf) of the FullQlin layout from DNS columns at time t."""
     q = p.ql()
-    kt = ktables(q)
+    kt = kdata(q)
     kyc = 1j * kt["ky"][:, None]
     kzc = 1j * kt["kz"][None, :]
     s = float(q.nx * (q.ny // 2 * 2)) / float(p.Mx * p.My)

@@ -143,3 +143,16 @@ def test_initial_state_law():
     assert np.abs(by_mean - 0.05 * np.sin(2 * np.pi * z)).max() < 1e-14
     lin2, _ = dns_initial_state(p, 2, sigma=1e-2, B0=0.05)
     assert np.array_equal(lin, lin2)
+
+
+@pytest.mark.parametrize("Mx,My,NZ", [(16, 32, 16), (64, 128, 64), (6, 10, 32), (2, 2, 16)])
+def test_oracle_wavenumber_tables_agree_with_the_package(Mx, My, NZ):
+    # the oracle restates Kdata on its own; the package's tables (used to build the
+    # GPU initial state) must be the same numbers
+    from oracle.dns_oracle import kdata
+    q = DNSParams(Mx=Mx, My=My, NZ=NZ).ql()
+    a, b = kdata(q), ktables(q)
+    for key in ("kx_index", "ky_index"):
+        assert np.array_equal(a[key], b[key]), key
+    for key in ("kx", "ky", "kz"):
+        assert np.array_equal(a[key], b[key]), key
