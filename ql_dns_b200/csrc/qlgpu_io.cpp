@@ -338,19 +338,34 @@ int qlgpu_fullsave_read_latest(const char* path, const qlgpu_params* p, double* 
     Reader r;
     r.f = std::fopen(path, "rb");
     if (!r.f) return io_fail(QLGPU_ERR_ARG, std::string("cannot open ") + path);
+    std::fseek(r.f, 0, SEEK_END);
+    const long fsize = std::ftell(r.f);
     std::fseek(r.f, offs[best], SEEK_SET);
     (void)r.str();
     (void)r.get<double>();
     const uint32_t nds = r.get<uint32_t>();
-    bool have_kx = false;
+    bool have_kx = false, have_mean = false;
+    std::vector<char> seen((size_t)d.nxy, 0);
     std::vector<float> buf;
     for (uint32_t i = 0; i < nds && r.ok; ++i) {
         const std::string name = r.str();
         const uint32_t type = r.get<uint32_t>();
         const uint64_t count = r.get<uint64_t>();
         if (!r.ok) break;
+        // the sizes come from the file: check them against what is left of it before any allocation
+        const long pos = std::ftell(r.f);
+        const uint64_t left = (pos >= 0 && fsize >= pos) ? (uint64_t)(fsize - pos) / sizeof(float) : 0;
+        if (type > 1 || count > left / (type == 0 ? 2 : 1)) {
+            std::fclose(r.f);
+            return io_fail(QLGPU_ERR_ARG, "dataset " + name + " has an invalid type or size (corrupt file)");
+        }
         const size_t nfl = (size_t)count * (type == 0 ? 2 : 1);
-        buf.resize(nfl);
+        try {
+            buf.resize(nfl);
+        } catch (...) {
+            std::fclose(r.f);
+            return io_fail(QLGPU_ERR_ARG, "dataset " + name + " is too large");
+        }
         if (nfl && std::fread(buf.data(), sizeof(float), nfl, r.f) != nfl) {
             r.ok = false;
             break;
@@ -362,6 +377,7 @@ int qlgpu_fullsave_read_latest(const char* path, const qlgpu_params* p, double* 
                 std::fclose(r.f);
                 return io_fail(QLGPU_ERR_ARG, "dataset " + name + " does not match the parameters");
             }
+            seen[jj] = 1;
             if (lin)
                 for (size_t k = 0; k < nfl; ++k) lin[(size_t)jj * d.nlin * d.nz * 2 + k] = (double)buf[k];
         } else if (name == "Mean") {
@@ -369,6 +385,7 @@ int qlgpu_fullsave_read_latest(const char* path, const qlgpu_params* p, double* 
                 std::fclose(r.f);
                 return io_fail(QLGPU_ERR_ARG, "dataset Mean does not match the parameters");
             }
+            have_mean = true;
             if (mf)
                 for (size_t k = 0; k < nfl; ++k) mf[k] = (double)buf[k];
         } else if (name == "kx") {
@@ -384,6 +401,10 @@ int qlgpu_fullsave_read_latest(const char* path, const qlgpu_params* p, double* 
     }
     std::fclose(r.f);
     if (!r.ok) return io_fail(QLGPU_ERR_ARG, std::string("truncated file ") + path);
+    // every mode and the mean fields must be in the group (FullSave_Load.cpp:286-316 reads them all)
+    for (int j = 0; j < d.nxy; ++j)
+        if (!seen[j]) return io_fail(QLGPU_ERR_ARG, "group lacks dataset Ind " + std::to_string(j));
+    if (!have_mean) return io_fail(QLGPU_ERR_ARG, "group lacks dataset Mean");
     // no kx dataset: kx as initialised (FullSave_Load.cpp:322-324)
     if (!have_kx && kx0)
         for (int j = 0; j < d.nxy; ++j) kx0[j] = kx[j];

@@ -135,3 +135,51 @@ def test_fullsave_rejects_mismatch(tmp_path):
     assert "do not match" in str(ei.value)
     with pytest.raises(_capi.QLGPUError):
         io.load_solution(str(tmp_path / "missing.bin"), p)
+
+
+def _write_container(path, p, t, datasets):
+    """A FullSave container with one group holding the given (name, type, float32 payload) datasets."""
+    b = bytearray(b"QLFSAVE1")
+    b += struct.pack("<4i", 4, p.nz, p.nmf, p.nxy)
+    name = f"/t={t}".encode()
+    b += struct.pack("<I", len(name)) + name + struct.pack("<dI", t, len(datasets))
+    for dn, typ, payload in datasets:
+        dn = dn.encode()
+        cnt = payload.size // 2 if typ == 0 else payload.size
+        b += struct.pack("<I", len(dn)) + dn + struct.pack("<IQ", typ, cnt) + payload.astype(np.float32).tobytes()
+    open(path, "wb").write(bytes(b))
+
+
+def test_fullsave_rejects_corrupt_and_incomplete_groups(tmp_path):
+    p = mri_16x16_nz32(nx=4, ny=4, NZ=16)
+    kt = ktables(p)
+    lin, mf, kx0 = initial_state(p, 5, sigma=0.3)
+    good = [(f"Ind {j}: kx {kt['kx_index'][j]} ky {kt['ky_index'][j]}", 0,
+             lin[j].reshape(-1).view(np.float64)) for j in range(p.nxy)]
+    mean = ("Mean", 0, mf.reshape(-1).view(np.float64))
+    kxd = ("kx", 1, kx0 + p.q * 0.5 * kt["ky"])
+    path = str(tmp_path / "ok.bin")
+    _write_container(path, p, 0.5, good + [mean, kxd])
+    t, lo, mo, ko = io.load_solution(path, p)
+    assert t == 0.5 and np.abs(lo - lin).max() < 1e-6 * np.abs(lin).max()
+    # a mode dataset missing from the group
+    path = str(tmp_path / "missing_ind.bin")
+    _write_container(path, p, 0.5, good[:2] + good[3:] + [mean, kxd])
+    with pytest.raises(_capi.QLGPUError) as ei:
+        io.load_solution(path, p)
+    assert "Ind 2" in str(ei.value)
+    # no mean fields
+    path = str(tmp_path / "missing_mean.bin")
+    _write_container(path, p, 0.5, good + [kxd])
+    with pytest.raises(_capi.QLGPUError) as ei:
+        io.load_solution(path, p)
+    assert "Mean" in str(ei.value)
+    # the last dataset's count patched to an absurd size: an error, not an allocation failure
+    path = str(tmp_path / "corrupt.bin")
+    _write_container(path, p, 0.5, good + [mean, kxd])
+    raw = bytearray(open(path, "rb").read())
+    off = raw.rfind(b"kx") + 2 + 4  # name, then the type word; the count follows
+    struct.pack_into("<Q", raw, off, 1 << 61)
+    open(path, "wb").write(bytes(raw))
+    with pytest.raises(_capi.QLGPUError):
+        io.load_solution(path, p)
