@@ -54,6 +54,9 @@ SINGLE_WORKLOAD = ("QL MRI plain FP64 MHD_BQlin + RK3CN_Elin, 64x64 (kx,ky) mode
                    "(nz=85), Re=Rm=8000, dt=0.005, seed 1")
 NCASES = 48
 FALLBACK_HBM_GBS = 6650.0
+KERNEL_NAME = {"queue": "ens_kernel<MHD_BQlin,RK3CN_Elin> (chunk-queue engine, one launch of K steps)",
+               "items": "batch_kernel<MHD_BQlin,RK3CN_Elin> (work-item engine, one launch of K steps)"}
+KERNEL_PROFILE = {"queue": "ens_kernel_mri_ensemble48.md", "items": "batch_kernel_mri_ensemble48.md"}
 
 
 def single_params():
@@ -84,6 +87,13 @@ def reference_flops_per_step(p) -> float:
     step x (15 inverse + 7 forward) length-NZ transforms x 5 NZ log2 NZ, per mode column."""
     import math
     return p.nxy * 3 * (15 + 7) * 5 * p.NZ * math.log2(p.NZ)
+
+
+def own_transform_flops_per_step(p) -> float:
+    """FP64 flops of the transforms this build runs per mode-step: 3 stages x (9 inverse +
+    5 forward) length-NZ transforms x 5 NZ log2 NZ (qlgpu_ens.cuh)."""
+    import math
+    return p.nxy * 3 * 14 * 5 * p.NZ * math.log2(p.NZ)
 
 
 def fp64_peak(local) -> float:
@@ -396,6 +406,41 @@ def run_dns(args, local):
     return out
 
 
+def ensemble_parity(cases, sts, recs_e2e, outs_e2e, timed_out, args):
+    """Every case of the timed ensemble against the CPU oracle (strict FP64 build, OpenMP over
+    modes) from the same initial state: the end-to-end run's state and energy / stress /
+    dissipation series after K steps, and the device-timed run's state after W + K steps."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+
+    def rel(a, b):
+        nb = np.linalg.norm(b)
+        return float(np.linalg.norm(a - b) / nb) if nb > 0 else float(np.linalg.norm(a))
+
+    err_e2e = err_e2e_mf = err_series = err_timed = err_timed_mf = 0.0
+    for c, (p, (lin, mf, kx0)) in enumerate(zip(cases, sts)):
+        t1, l1, m1, k1, d1 = O.run(p, 0.0, lin, mf, kx0, args.steps, diag_every=1, kind="strict_omp",
+                                   nthreads=threads)
+        err_e2e = max(err_e2e, rel(outs_e2e[c][1], l1))
+        err_e2e_mf = max(err_e2e_mf, rel(outs_e2e[c][2], m1))
+        dg = np.vstack(recs_e2e[c])
+        for col in range(1, 13):
+            scale = np.abs(d1[:, col]).max()
+            if scale > 0:
+                err_series = max(err_series, float(np.abs(dg[:, col] - d1[:, col]).max() / scale))
+        t2, l2, m2, k2, _ = O.run(p, t1, l1, m1, k1, args.warmup, kind="strict_omp", nthreads=threads)
+        err_timed = max(err_timed, rel(timed_out[c][1], l2))
+        err_timed_mf = max(err_timed_mf, rel(timed_out[c][2], m2))
+    return {"against": "CPU oracle, strict FP64 build (-O2 -ffp-contract=off), OpenMP over modes",
+            "cases": len(cases), "tolerance": 1e-10,
+            "e2e_run": {"steps": args.steps, "max_rel_err_state": err_e2e, "max_rel_err_mean_field": err_e2e_mf,
+                        "max_rel_err_series": err_series},
+            "timed_run": {"steps": args.steps + args.warmup, "max_rel_err_state": err_timed,
+                          "max_rel_err_mean_field": err_timed_mf},
+            "oracle_s": time.perf_counter() - t0}
+
+
 def run_gpu(args):
     import torch
     ws, rank, local = dist_setup()
@@ -425,6 +470,9 @@ def run_gpu(args):
     assert ls == 0 and not any(st), (st, ls)
     mapping = batch.mapping()
     cost = batch.cost_model()
+    engine = batch.engine()
+    # the state after the W warm-up and K timed steps, for the parity check below
+    timed_out = [batch.get_state(c) for c in range(NCASES)]
 
     peak, peak_kind = hbm_peak()
     alg_step = sum(algorithmic_bytes_per_step(p) for p in cases)
@@ -432,6 +480,8 @@ def run_gpu(args):
     flops_step = sum(reference_flops_per_step(p) for p in cases)
     fp64_pk = fp64_peak(local)
     fp64_ach = flops_step * args.steps / (ms / 1e3) / 1e12
+    own_flops_step = sum(own_transform_flops_per_step(p) for p in cases)
+    own_ach = own_flops_step * args.steps / (ms / 1e3) / 1e12
 
     # end to end through the batch C ABI: H2D of every case's state from pinned
     # host memory, then per step one call that advances all cases and reads the
@@ -453,9 +503,12 @@ def run_gpu(args):
     for c, (lh, mh, kx0) in enumerate(pinned):
         batch.set_state(c, 0.0, lh, mh, kx0)
     ndiag = 0
+    recs_all = [[] for _ in range(NCASES)]
     for _ in range(args.steps):
         recs = batch.step(1, diag_every=1)
         ndiag += sum(len(r) for r in recs)
+        for c, r in enumerate(recs):
+            recs_all[c].append(r)
     outs = [batch.get_state(c) for c in range(NCASES)]
     ee1.record(ext)
     ee1.synchronize()
@@ -469,6 +522,7 @@ def run_gpu(args):
            "path": "QLBatch.set_state (pinned) x48, K x QLBatch.step(1, diag_every=1), QLBatch.get_state x48"}
     batch.close()
 
+    parity = ensemble_parity(cases, sts, recs_all, outs, timed_out, args) if rank == 0 else None
     plain = run_plain_per_case(cases, sts, local) if rank == 0 else None
     single = run_single(args, torch.cuda.ExternalStream, local) if rank == 0 else None
     dns = run_dns(args, local) if rank == 0 else None
@@ -485,15 +539,22 @@ def run_gpu(args):
                        "cost_model": cost},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": read_traffic("batch_kernel_mri_ensemble48.md"),
-                         "kernel": "batch_kernel<MHD_BQlin,RK3CN_Elin> (one launch of K steps)",
+                         "traffic": read_traffic(KERNEL_PROFILE[engine]),
+                         "kernel": KERNEL_NAME[engine], "engine": engine,
                          "algorithmic_bytes_per_step": alg_step, "avg_launch_ms": ms,
                          "fp64": {"achieved": fp64_ach, "peak": fp64_pk, "unit": "TFLOP/s", "frac": fp64_ach / fp64_pk,
                                   "flops_per_step": flops_step,
                                   "count": "reference formulation: 3 x (15 + 7) transforms x 5 NZ log2 NZ per "
                                            "mode-step; peak: measured FP64 FMA loop (qlgpu_fp64_peak)",
                                   "hbm_roofline_needs_fp64_frac": flops_step / (alg_step / (peak * 1e9)) / 1e12
-                                  / fp64_pk}},
+                                  / fp64_pk,
+                                  "actual": {"achieved": own_ach, "frac": own_ach / fp64_pk,
+                                             "flops_per_step": own_flops_step,
+                                             "count": "this kernel's transforms: 3 x 14 length-NZ transforms x "
+                                                      "5 NZ log2 NZ per mode-step (pointwise work not counted)",
+                                             "hbm_roofline_needs_fp64_frac":
+                                                 own_flops_step / (alg_step / (peak * 1e9)) / 1e12 / fp64_pk}}},
+            "parity": parity,
             "plain_per_case": plain,
             "speedup_vs_plain_per_case": value / plain["value"],
             "single_case": single,
@@ -509,6 +570,7 @@ def run_gpu(args):
     if rank == 0:
         if not args.no_cpu_baseline and ws == 1:
             out["cpu_baseline"] = cpu_baseline(budget_s=args.cpu_budget)
+            out["cpu_baseline_1thread"] = cpu_baseline(budget_s=min(args.cpu_budget, 10.0), threads=1)
         print(json.dumps(out), flush=True)
     return 0
 
@@ -516,7 +578,7 @@ def run_gpu(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

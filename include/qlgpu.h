@@ -260,7 +260,8 @@ int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms);
 int qlgpu_batch_cost_model(const qlgpu_batch_t* b, double* out7);
 
 /* Current mapping: info4 = {warps per CTA, CTAs launched, CTAs per SM,
- * dynamic shared bytes}; ncta[c] = CTAs that step case c (may be NULL). */
+ * dynamic shared bytes}; ncta[c] = CTAs that step case c (may be NULL);
+ * queue engine: ncta[c] = chunks of case c per stage. */
 int qlgpu_batch_mapping(const qlgpu_batch_t* b, int* info4, int* ncta);
 
 /* Fixed mapping: ncta[c] CTAs for case c at `warps` warps per CTA (1 up to
@@ -276,12 +277,42 @@ int qlgpu_batch_status(qlgpu_batch_t* b, int* case_status, int* launch_status);
 int qlgpu_batch_set_wait(qlgpu_batch_t* b, double seconds);
 
 /* Failure-detection test aid: removes the last work item of case c (a case
- * with two or more CTAs) from the current mapping, so that the case's other
- * CTAs wait for a stage that never completes.  The next step call must return
+ * with two or more CTAs) from the current mapping (queue engine: one chunk
+ * of case c, which needs two or more chunks, from every stage), so that the
+ * case's other CTAs wait for a stage that never completes.  The next step call must return
  * QLGPU_ERR_STATUS with QLGPU_STATUS_BATCH_TIMEOUT after the wait bound; the
  * batch stays usable after qlgpu_batch_set_mapping / qlgpu_batch_tune and
  * qlgpu_batch_set_state. */
 int qlgpu_batch_debug_drop_item(qlgpu_batch_t* b, int c);
+
+/* Engines.  QLGPU_BATCH_ENGINE_ITEMS: the work-item engine above (every model,
+ * integrator and NZ; CTAs own fixed work items and wait for their cases at
+ * each stage).  QLGPU_BATCH_ENGINE_QUEUE: MHD_BQlin batches with every NZ <=
+ * 128 -- CTAs take chunks of consecutive modes of one case and one stage from
+ * a global ticket counter; the CTA that completes a case's stage runs its
+ * mean-field stage, so no CTA waits at another case's stage boundary.  Chunk
+ * partial sums go to fixed slots summed in slot order: results do not depend
+ * on which CTA ran which chunk.  QLGPU_BATCH_ENGINE_AUTO picks the queue
+ * engine where it applies (the default at creation).  The per-case
+ * arithmetic of the two engines agrees to round-off (1e-12 relative), not
+ * bit for bit.  qlgpu_batch_set_mapping selects the work-item engine. */
+#define QLGPU_BATCH_ENGINE_AUTO 0
+#define QLGPU_BATCH_ENGINE_ITEMS 1
+#define QLGPU_BATCH_ENGINE_QUEUE 2
+int qlgpu_batch_set_engine(qlgpu_batch_t* b, int engine);
+int qlgpu_batch_engine(const qlgpu_batch_t* b, int* engine);
+
+/* Queue engine: CTA passes per chunk for the NZ classes 16, 32, 64, 128
+ * (passes4[i] >= 1; a pass steps 16 warps x 32/(NZ/4) modes).  Selects the
+ * queue engine.  qlgpu_batch_tune searches these when the queue engine is
+ * active. */
+int qlgpu_batch_set_chunks(qlgpu_batch_t* b, const int* passes4);
+
+/* Profiling aid of the queue engine (QLGPU_TRACE=1 in the environment at
+ * qlgpu_batch_create): per CTA of the last launch, averaged over CTAs, out4 =
+ * {us waiting for tickets and stages, us in chunks, us of that in mean-field
+ * stages, chunks}.  QLGPU_ERR_UNSUPPORTED when off. */
+int qlgpu_batch_queue_trace(qlgpu_batch_t* b, double* out4);
 
 int qlgpu_batch_stream(qlgpu_batch_t* b, void** stream);
 int qlgpu_batch_last_error(const qlgpu_batch_t* b, char* buf, int buflen);

@@ -38,7 +38,8 @@ _LIBS = {}
 
 
 def lib(kind: str = "strict"):
-    """kind: 'strict' (parity), 'fast' (portable timing build) or 'native'."""
+    """kind: 'strict' (parity), 'strict_omp' (parity, OpenMP over modes), 'fast' (portable timing
+    build) or 'native'."""
     if kind in _LIBS:
         return _LIBS[kind]
     if kind == "native":

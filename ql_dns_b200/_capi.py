@@ -29,7 +29,8 @@ EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "ql
            "qlgpu_batch_get_state", "qlgpu_batch_diagnostics", "qlgpu_batch_step", "qlgpu_batch_step_timed",
            "qlgpu_batch_tune", "qlgpu_batch_mapping", "qlgpu_batch_set_mapping", "qlgpu_batch_status",
            "qlgpu_batch_set_wait", "qlgpu_batch_debug_drop_item", "qlgpu_batch_stream",
-           "qlgpu_batch_last_error",
+           "qlgpu_batch_last_error", "qlgpu_batch_set_engine", "qlgpu_batch_engine", "qlgpu_batch_set_chunks",
+           "qlgpu_batch_queue_trace",
            "qlgpu_timevars_open", "qlgpu_timevars_save_data", "qlgpu_timevars_save_mean_fields",
            "qlgpu_timevars_close", "qlgpu_fullsave_write", "qlgpu_fullsave_read_latest", "qlgpu_fullsave_times",
            "qlgpu_io_last_error",
@@ -123,6 +124,10 @@ def load(path: str = LIB_PATH):
     L.qlgpu_batch_debug_drop_item.argtypes = [vp, ctypes.c_int]
     L.qlgpu_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.qlgpu_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    L.qlgpu_batch_set_engine.argtypes = [vp, ctypes.c_int]
+    L.qlgpu_batch_engine.argtypes = [vp, ip]
+    L.qlgpu_batch_set_chunks.argtypes = [vp, ip]
+    L.qlgpu_batch_queue_trace.argtypes = [vp, dp]
     L.qlgpu_timevars_open.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       ctypes.POINTER(vp)]
     L.qlgpu_timevars_save_data.argtypes = [vp, dp]

@@ -123,6 +123,28 @@ class QLBatch:
         k = (ctypes.c_int * len(ncta))(*ncta)
         _capi.check_batch(self.L.qlgpu_batch_set_mapping(self.b, int(warps), k), self.b)
 
+    ENGINES = {"auto": 0, "items": 1, "queue": 2}
+
+    def set_engine(self, engine: str):
+        """'queue' (chunk queue: MHD_BQlin, NZ <= 128), 'items' (work items: every case) or 'auto'."""
+        _capi.check_batch(self.L.qlgpu_batch_set_engine(self.b, self.ENGINES[engine]), self.b)
+
+    def engine(self) -> str:
+        e = ctypes.c_int()
+        _capi.check_batch(self.L.qlgpu_batch_engine(self.b, ctypes.byref(e)), self.b)
+        return {1: "items", 2: "queue"}[e.value]
+
+    def set_chunks(self, passes: list[int]):
+        """Queue engine: CTA passes per chunk for NZ = 16, 32, 64, 128."""
+        k = (ctypes.c_int * 4)(*passes)
+        _capi.check_batch(self.L.qlgpu_batch_set_chunks(self.b, k), self.b)
+
+    def queue_trace(self) -> dict:
+        """Queue engine, QLGPU_TRACE=1: per-CTA averages of the last launch."""
+        v = (ctypes.c_double * 4)()
+        _capi.check_batch(self.L.qlgpu_batch_queue_trace(self.b, v), self.b)
+        return {"wait_us": v[0], "chunk_us": v[1], "mean_field_us": v[2], "chunks": v[3]}
+
     def status(self):
         nc = len(self.cases)
         st = (ctypes.c_int * nc)()

@@ -708,11 +708,18 @@ namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[QLGPU_NOALLOC_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch, looked up once per device.  In host code
-// the symbol g_noalloc_scratch is only a host-side stand-in; handing it to a
-// kernel would read the wrong memory.
+// Per device, looked up once: the device address of g_noalloc_scratch (in host
+// code the symbol g_noalloc_scratch is only a host-side stand-in; handing it to
+// a kernel would read the wrong memory), the SM count and the opt-in shared
+// memory per CTA.  The cache lives for the process: after cudaDeviceReset the
+// context is new and the cached address is stale.
 std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[64] = {nullptr};
+struct NoallocDevice {
+    void* ptr = nullptr;
+    int sms = 0;
+    int smem_optin = 0;
+};
+NoallocDevice g_noalloc_dev[64];
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -815,30 +822,37 @@ extern "C" int qlgpu_rhs_noalloc(const qlgpu_params* pp, double t, double dt_lin
                     "(use qlgpu_create / qlgpu_rhs for larger grids)");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return fail(nullptr, QLGPU_ERR_NODEVICE, "no CUDA device");
-    void* base = nullptr;
+    NoallocDevice nd;
     {
-        // One-time set-up on this device: the device address of the scratch array.
+        // One-time set-up on this device: the device address of the scratch array and the
+        // two device attributes the launch geometry needs.
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_ptr[dev]) {
+        NoallocDevice& c = g_noalloc_dev[dev];
+        if (!c.ptr) {
             void* ptr = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
             if (e != cudaSuccess || !ptr)
                 return fail(nullptr, QLGPU_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            g_noalloc_ptr[dev] = ptr;
+            int sms = 0, optin = 0;
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+                cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+                return fail(nullptr, QLGPU_ERR_CUDA, "device attributes");
+            c.sms = sms;
+            c.smem_optin = optin;
+            c.ptr = ptr;
         }
-        base = g_noalloc_ptr[dev];
+        nd = c;
     }
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return fail(nullptr, QLGPU_ERR_CUDA, "device properties");
+    void* base = nd.ptr;
     // Launch geometry: as in qlgpu_create, at most one CTA per SM and one mode per pair of groups.
     int warps = 8;
-    while (warps > 1 && var.smem(warps) > (size_t)prop.sharedMemPerBlockOptin) warps >>= 1;
+    while (warps > 1 && var.smem(warps) > (size_t)nd.smem_optin) warps >>= 1;
     const size_t smem = var.smem(warps);
     if (ensure_smem_attr(var.kernel(), smem) != cudaSuccess)
         return fail(nullptr, QLGPU_ERR_CUDA, "shared memory request too large");
     const int modes_per_cta = warps * (32 / var.T) / 2;
     int grid = (nxy + modes_per_cta - 1) / modes_per_cta;
-    if (grid > prop.multiProcessorCount) grid = prop.multiProcessorCount;
+    if (grid > nd.sms) grid = nd.sms;
     if (grid > QLGPU_NOALLOC_MAX_GRID) grid = QLGPU_NOALLOC_MAX_GRID;
     const NoallocLayout L = noalloc_layout(p.NZ, nxy, nyh, nz, grid, var.PL);
     if (L.end > QLGPU_NOALLOC_SCRATCH_BYTES)

@@ -17,6 +17,13 @@
 // (%globaltimer stamps written by the kernel), fits alpha, beta and r[NZ] by
 // least squares, re-plans, and keeps the fastest measured mapping over two CTA
 // widths: the widest that fits the batch and half of it.
+//
+// Two engines step a batch.  The work-item engine above (qlgpu_batch.cuh) runs
+// every model, integrator and NZ.  The chunk-queue engine (qlgpu_ens.cuh) runs
+// MHD_BQlin batches with NZ <= 128: CTAs take chunks of a case's modes from a
+// global ticket counter, so no CTA waits at a stage boundary of another case.
+// Its tuning knob is the number of CTA passes per chunk of each NZ class; its
+// autotuner times probe launches over those and keeps the fastest.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,6 +39,7 @@
 
 #include "../../include/qlgpu.h"
 #include "qlgpu_batch_internal.h"
+#include "qlgpu_ens_host.h"
 #include "qlgpu_host.h"
 #include "qlgpu_kernel.cuh"
 
@@ -96,7 +104,9 @@ __global__ void batch_reset_kernel(const BatchCase* cases, int ncases, unsigned*
         ctl->abort = 0;
         ctl->fail_case = -1;
         ctl->fail_stage = -1;
+        ctl->fail_where = 0;
         ctl->t_start = 0;
+        ctl->next = 0u;
     }
     if (c >= ncases) return;
     DevClock* clk = cases[c].A[0].clk;
@@ -104,6 +114,7 @@ __global__ void batch_reset_kernel(const BatchCase* cases, int ncases, unsigned*
     if (threadIdx.x == 0) {
         clk->cnt_top = 0u;
         epoch[(size_t)c * BATCH_EPOCH_STRIDE] = 0u;
+        epoch[(size_t)c * BATCH_EPOCH_STRIDE + 1] = 0u;
         if (reset_ndiag) clk->ndiag = 0;
     }
 }
@@ -158,6 +169,20 @@ struct qlgpu_batch {
     bool descr_dirty = true;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     std::string err;
+    // chunk-queue engine (qlgpu_ens.cuh)
+    int engine = QLGPU_BATCH_ENGINE_ITEMS;
+    bool queue_ok = false;               // MHD_BQlin and every NZ <= 128
+    int qpasses[4] = {2, 2, 2, 2};       // CTA passes per chunk, NZ = 16, 32, 64, 128
+    std::vector<ens::EnsCase> ec;
+    std::vector<ens::RoundItem> round;
+    ens::EnsCase* d_ec = nullptr;
+    ens::RoundItem* d_round = nullptr;
+    cplx* d_tw8 = nullptr;               // 8-point twiddles of NZ = 16, 32, 64, 128 (240 cplx)
+    size_t qsmem = 0;
+    int qgrid = 0;
+    int drop_case = -1;                  // failure-detection aid: a chunk of this case is left out
+    bool qdirty = true;
+    unsigned long long* d_qtrace = nullptr;  // [grid][4] per-CTA time sums of the last queue launch (QLGPU_TRACE=1)
 };
 
 namespace {
@@ -392,6 +417,101 @@ int plan_and_apply(qlgpu_batch_t* b, int warps, const int* fixed_k) {
     return apply_mapping(b, warps, per_sm, smem, k, bins);
 }
 
+// ---------------------------------------------------------------------------
+// Chunk-queue engine
+// ---------------------------------------------------------------------------
+int ens_class(int NZ) { return NZ == 16 ? 0 : NZ == 32 ? 1 : NZ == 64 ? 2 : 3; }
+size_t tw8_offset(int NZ) { return NZ == 16 ? 0 : NZ == 32 ? 16 : NZ == 64 ? 48 : 112; }  // cplx
+
+bool queue_usable(const qlgpu_batch_t* b) {
+    if (!b->queue_ok || b->engine != QLGPU_BATCH_ENGINE_QUEUE) return false;
+    for (const CaseHost& h : b->cs)
+        if (h.rec_lin) return false;  // the stage-input record is a work-item engine feature
+    return true;
+}
+
+// Chunks per stage of every case (passes per chunk of its NZ class, raised until
+// the case's partial-sum slots hold every chunk) and the order of one round:
+// cases with the longest chunks first, each case's chunks consecutive.
+int queue_plan(qlgpu_batch_t* b) {
+    const int nc = b->ncases;
+    b->ec.assign(nc, ens::EnsCase());
+    std::vector<double> len(nc);
+    size_t smem = 0;
+    for (int c = 0; c < nc; ++c) {
+        const CaseHost& h = b->cs[c];
+        const int mpp = ens::modes_per_pass(h.NZ);
+        int passes = std::max(1, b->qpasses[ens_class(h.NZ)]);
+        int nch = 0, mpc = 0;
+        for (;;) {
+            mpc = passes * mpp;
+            nch = (h.nxy + mpc - 1) / mpc;
+            if (nch <= h.max_cta) break;
+            ++passes;
+        }
+        ens::EnsCase& e = b->ec[c];
+        std::memset(&e, 0, sizeof(e));
+        e.NZ = h.NZ;
+        e.nch = nch;
+        e.mpc = mpc;
+        e.tw8 = b->d_tw8 + tw8_offset(h.NZ);
+        len[c] = (double)passes * h.NZ;
+        smem = std::max(smem, ens::smem_bytes(h.NZ));
+    }
+    std::vector<int> ord(nc);
+    for (int c = 0; c < nc; ++c) ord[c] = c;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return len[x] > len[y]; });
+    b->round.clear();
+    for (int c : ord)
+        for (int j = 0; j < b->ec[c].nch; ++j) {
+            if (c == b->drop_case && j == b->ec[c].nch - 1) continue;
+            b->round.push_back(ens::RoundItem{c, j});
+        }
+    if (b->d_round) cudaFree(b->d_round);
+    b->d_round = nullptr;
+    QB_CK(cudaMalloc(&b->d_round, sizeof(ens::RoundItem) * std::max<size_t>(1, b->round.size())));
+    QB_CK(cudaMemcpyAsync(b->d_round, b->round.data(), sizeof(ens::RoundItem) * b->round.size(),
+                          cudaMemcpyHostToDevice, b->stream));
+    QB_CK(cudaMemcpyAsync(b->d_ec, b->ec.data(), sizeof(ens::EnsCase) * nc, cudaMemcpyHostToDevice, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    const void* k = ens::kernel(b->integ);
+    if (smem > b->smem_optin) return bfail(b, QLGPU_ERR_UNSUPPORTED, "queue engine: shared memory request too large");
+    QB_CK(ensure_smem_attr(k, smem));
+    int occ = 0;
+    QB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, ens::ENS_THREADS, smem));
+    if (occ < 1) return bfail(b, QLGPU_ERR_UNSUPPORTED, "queue engine: the CTA does not fit an SM");
+    b->qsmem = smem;
+    b->qgrid = b->sms;
+    b->qdirty = false;
+    drop_graphs(b);
+    return QLGPU_OK;
+}
+
+cudaError_t enqueue_queue(qlgpu_batch_t* b, int nsteps, int reset_ndiag) {
+    batch_reset_kernel<<<b->ncases, 64, 0, b->stream>>>(b->d_cases, b->ncases, b->d_epoch, b->d_ctl, reset_ndiag);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    ens::EnsLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.cases = b->d_cases;
+    L.ec = b->d_ec;
+    L.round = b->d_round;
+    L.epoch = b->d_epoch;
+    L.ctl = b->d_ctl;
+    L.next = &b->d_ctl->next;
+    L.case_end = b->d_case_end;
+    L.R = (int)b->round.size();
+    L.nrounds = 3 * nsteps;
+    L.parity = b->cur;
+    L.wait_ns = b->wait_ns;
+    L.trace = b->d_qtrace;
+    if (b->d_qtrace) {
+        e = cudaMemsetAsync(b->d_qtrace, 0, sizeof(unsigned long long) * 4 * b->qgrid, b->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return ens::launch(b->integ, L, b->qgrid, b->qsmem, b->stream);
+}
+
 BatchLaunch launch_args(qlgpu_batch_t* b, int nsteps) {
     BatchLaunch L;
     std::memset(&L, 0, sizeof(L));
@@ -420,16 +540,23 @@ int run_launch(qlgpu_batch_t* b, int nsteps, int reset_ndiag) {
         if (rc) return rc;
     }
     if (nsteps == 0) return QLGPU_OK;
+    const bool q = queue_usable(b);
+    if (q && b->qdirty) {
+        int rc = queue_plan(b);
+        if (rc) return rc;
+    }
     // the dynamic shared memory attribute belongs to the kernel, not to this batch
-    QB_CK(ensure_smem_attr(b->bk.kernel(), b->smem));
+    if (q) QB_CK(ensure_smem_attr(ens::kernel(b->integ), b->qsmem));
+    else QB_CK(ensure_smem_attr(b->bk.kernel(), b->smem));
+    auto enqueue = [&]() { return q ? enqueue_queue(b, nsteps, reset_ndiag) : enqueue_launch(b, nsteps, reset_ndiag); };
     if (b->use_graph) {
-        const auto key = std::make_tuple(nsteps, b->cur, reset_ndiag);
+        const auto key = std::make_tuple(nsteps, b->cur + (q ? 2 : 0), reset_ndiag);
         auto itg = b->graphs.find(key);
         if (itg == b->graphs.end()) {
             if (b->graphs.size() >= 8) drop_graphs(b);
             cudaGraph_t g = nullptr;
             QB_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            const cudaError_t le = enqueue_launch(b, nsteps, reset_ndiag);
+            const cudaError_t le = enqueue();
             const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
             if (le != cudaSuccess || ce != cudaSuccess) {
                 if (g) cudaGraphDestroy(g);
@@ -445,7 +572,7 @@ int run_launch(qlgpu_batch_t* b, int nsteps, int reset_ndiag) {
         }
         QB_CK(cudaGraphLaunch(itg->second, b->stream));
     } else {
-        QB_CK(enqueue_launch(b, nsteps, reset_ndiag));
+        QB_CK(enqueue());
     }
     b->cur = (b->cur + nsteps) & 1;
     return QLGPU_OK;
@@ -458,9 +585,10 @@ int check_launch_status(qlgpu_batch_t* b) {
     if (ctl.status & QLGPU_STATUS_TIMEOUT) {
         char buf[200];
         std::snprintf(buf, sizeof(buf),
-                      "batch: a CTA gave up waiting for case %d at stage %d (wait bound %.3g s); the state of the "
+                      "batch: a CTA gave up waiting %s case %d at stage %d (wait bound %.3g s); the state of the "
                       "batch is undefined",
-                      ctl.fail_case, ctl.fail_stage, b->wait_ns * 1e-9);
+                      ctl.fail_where == 1 ? "for a staged copy of" : "for", ctl.fail_case, ctl.fail_stage,
+                      b->wait_ns * 1e-9);
         return bfail(b, QLGPU_ERR_STATUS, buf);
     }
     return QLGPU_OK;
@@ -490,8 +618,8 @@ int qlgpu_batch_destroy(qlgpu_batch_t* b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
-    void* bufs[] = {b->arena,     b->d_cases,   b->d_ctas,  b->d_epoch, b->d_ctl,
-                    b->d_case_end, b->d_collect, b->d_out15, b->d_diag};
+    void* bufs[] = {b->arena,   b->d_cases, b->d_ctas, b->d_epoch, b->d_ctl, b->d_case_end, b->d_collect,
+                    b->d_out15, b->d_diag,  b->d_ec,   b->d_round, b->d_tw8, b->d_qtrace};
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : b->ev)
@@ -660,7 +788,35 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
     QB_ALLOC(b->d_case_end, sizeof(unsigned long long) * ncases);
     QB_ALLOC(b->d_collect, sizeof(int) * (2 * ncases + 2));
     QB_ALLOC(b->d_out15, sizeof(double) * 15);
+    QB_ALLOC(b->d_ec, sizeof(ens::EnsCase) * ncases);
+    QB_ALLOC(b->d_tw8, sizeof(cplx) * 240);
 #undef QB_ALLOC
+    {
+        // 8-point twiddles of the queue engine, tw[q T + t] = exp(2 pi i q t / NZ), T = NZ / 8
+        std::vector<double> tw8(480, 0.0);
+        for (int NZ : {16, 32, 64, 128}) {
+            const std::vector<double> t = twiddles(NZ, NZ / 8);
+            std::copy(t.begin(), t.end(), tw8.begin() + 2 * tw8_offset(NZ));
+        }
+        if (cudaMemcpyAsync(b->d_tw8, tw8.data(), sizeof(double) * 480, cudaMemcpyHostToDevice, b->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(b->stream) != cudaSuccess) {
+            b->err = "twiddle upload failed";
+            return bail(QLGPU_ERR_CUDA);
+        }
+        b->queue_ok = b->model == MODEL_BQLIN;
+        for (int c = 0; c < ncases; ++c)
+            if (cases[c].NZ > 128) b->queue_ok = false;
+        const char* tr = std::getenv("QLGPU_TRACE");
+        if (tr && tr[0] == '1' &&
+            cudaMalloc(&b->d_qtrace, sizeof(unsigned long long) * 4 * (size_t)b->sms) != cudaSuccess) {
+            b->err = "trace buffer";
+            return bail(QLGPU_ERR_CUDA);
+        }
+        const char* e = std::getenv("QLGPU_BATCH_ENGINE");
+        const bool force_items = e && std::string(e) == "items";
+        b->engine = (b->queue_ok && !force_items) ? QLGPU_BATCH_ENGINE_QUEUE : QLGPU_BATCH_ENGINE_ITEMS;
+    }
     if (cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess) {
         b->err = "event create failed";
         return bail(QLGPU_ERR_CUDA);
@@ -844,6 +1000,59 @@ int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms) {
         int rc = upload_descriptors(b);
         if (rc) return rc;
     }
+    if (queue_usable(b)) {
+        // queue engine: coordinate search over the CTA passes per chunk of each NZ class present
+        if (b->qdirty) {
+            int rc = queue_plan(b);
+            if (rc) return rc;
+        }
+        auto qprobe = [&](double* ms) -> int {
+            QB_CK(ensure_smem_attr(ens::kernel(b->integ), b->qsmem));
+            double best_of = 1e300;
+            for (int rep = 0; rep < 2; ++rep) {  // the first launch of a plan is a warm-up
+                QB_CK(cudaEventRecord(b->ev[0], b->stream));
+                QB_CK(enqueue_queue(b, probe_steps, 0));
+                QB_CK(cudaEventRecord(b->ev[1], b->stream));
+                QB_CK(cudaEventSynchronize(b->ev[1]));
+                float f = 0;
+                QB_CK(cudaEventElapsedTime(&f, b->ev[0], b->ev[1]));
+                b->cur = (b->cur + probe_steps) & 1;
+                int rc = check_launch_status(b);
+                if (rc) return rc;
+                if (rep > 0) best_of = std::min(best_of, (double)f);
+            }
+            *ms = best_of;
+            return QLGPU_OK;
+        };
+        bool present[4] = {false, false, false, false};
+        for (const CaseHost& h : b->cs) present[ens_class(h.NZ)] = true;
+        double best = 0;
+        int rc = qprobe(&best);
+        if (rc) return rc;
+        for (int cls = 3; cls >= 0; --cls) {
+            if (!present[cls]) continue;
+            const int keep = b->qpasses[cls];
+            int bestp = keep;
+            for (int pp : {1, 2, 3, 4, 6, 8}) {
+                if (pp == keep) continue;
+                b->qpasses[cls] = pp;
+                rc = queue_plan(b);
+                if (rc) return rc;
+                double ms = 0;
+                rc = qprobe(&ms);
+                if (rc) return rc;
+                if (ms < best) {
+                    best = ms;
+                    bestp = pp;
+                }
+            }
+            b->qpasses[cls] = bestp;
+        }
+        rc = queue_plan(b);
+        if (rc) return rc;
+        if (best_ms) *best_ms = best;
+        return QLGPU_OK;
+    }
     struct Best {
         double ms = 1e300;
         int warps = 0, per_sm = 0;
@@ -995,6 +1204,21 @@ int qlgpu_batch_cost_model(const qlgpu_batch_t* b, double* out7) {
 
 int qlgpu_batch_mapping(const qlgpu_batch_t* b, int* info4, int* ncta) {
     if (!b) return QLGPU_ERR_ARG;
+    if (queue_usable(b)) {
+        if (b->qdirty) {
+            int rc = queue_plan(const_cast<qlgpu_batch_t*>(b));
+            if (rc) return rc;
+        }
+        if (info4) {
+            info4[0] = ens::ENS_THREADS / 32;
+            info4[1] = b->qgrid;
+            info4[2] = 1;
+            info4[3] = (int)b->qsmem;
+        }
+        if (ncta)
+            for (int c = 0; c < b->ncases; ++c) ncta[c] = b->ec[c].nch;
+        return QLGPU_OK;
+    }
     if (info4) {
         info4[0] = b->warps;
         info4[1] = b->grid;
@@ -1011,6 +1235,8 @@ int qlgpu_batch_set_mapping(qlgpu_batch_t* b, int warps, const int* ncta) {
     if (warps < 1 || warps > b->wide_warps)
         return bfail(b, QLGPU_ERR_ARG, "warps per CTA must be 1 ... " + std::to_string(b->wide_warps) + " for this batch");
     QB_CK(cudaSetDevice(b->device));
+    b->engine = QLGPU_BATCH_ENGINE_ITEMS;  // an explicit CTA mapping is a work-item mapping
+    drop_graphs(b);
     return plan_and_apply(b, warps, ncta);
 }
 
@@ -1044,6 +1270,17 @@ int qlgpu_batch_set_wait(qlgpu_batch_t* b, double seconds) {
 
 int qlgpu_batch_debug_drop_item(qlgpu_batch_t* b, int c) {
     if (!b) return QLGPU_ERR_ARG;
+    if (queue_usable(b)) {
+        QB_CK(cudaSetDevice(b->device));
+        if (b->qdirty) {
+            int rc = queue_plan(b);
+            if (rc) return rc;
+        }
+        if (c < 0 || c >= b->ncases || b->ec[c].nch < 2)
+            return bfail(b, QLGPU_ERR_ARG, "drop item: the case needs two or more chunks");
+        b->drop_case = c;
+        return queue_plan(b);
+    }
     if (c < 0 || c >= b->ncases || b->ncta[c] < 2)
         return bfail(b, QLGPU_ERR_ARG, "drop item: the case needs two or more CTAs");
     QB_CK(cudaSetDevice(b->device));
@@ -1062,6 +1299,59 @@ int qlgpu_batch_debug_drop_item(qlgpu_batch_t* b, int c) {
     QB_CK(cudaStreamSynchronize(b->stream));
     b->ctas = ctas;
     drop_graphs(b);
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_set_engine(qlgpu_batch_t* b, int engine) {
+    if (!b) return QLGPU_ERR_ARG;
+    if (engine == QLGPU_BATCH_ENGINE_AUTO) engine = b->queue_ok ? QLGPU_BATCH_ENGINE_QUEUE : QLGPU_BATCH_ENGINE_ITEMS;
+    if (engine != QLGPU_BATCH_ENGINE_ITEMS && engine != QLGPU_BATCH_ENGINE_QUEUE)
+        return bfail(b, QLGPU_ERR_ARG, "unknown batch engine");
+    if (engine == QLGPU_BATCH_ENGINE_QUEUE && !b->queue_ok)
+        return bfail(b, QLGPU_ERR_UNSUPPORTED, "queue engine: MHD_BQlin batches with every NZ <= 128 only");
+    QB_CK(cudaSetDevice(b->device));
+    b->engine = engine;
+    b->drop_case = -1;
+    b->qdirty = true;
+    drop_graphs(b);
+    if (engine == QLGPU_BATCH_ENGINE_ITEMS) {
+        // a mapping that a dropped work item changed is replaced by the cost model's
+        return plan_and_apply(b, b->warps, nullptr);
+    }
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_engine(const qlgpu_batch_t* b, int* engine) {
+    if (!b || !engine) return QLGPU_ERR_ARG;
+    *engine = queue_usable(b) ? QLGPU_BATCH_ENGINE_QUEUE : QLGPU_BATCH_ENGINE_ITEMS;
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_set_chunks(qlgpu_batch_t* b, const int* passes4) {
+    if (!b || !passes4) return QLGPU_ERR_ARG;
+    for (int i = 0; i < 4; ++i)
+        if (passes4[i] < 1 || passes4[i] > 256) return bfail(b, QLGPU_ERR_ARG, "passes per chunk must be 1 ... 256");
+    if (!b->queue_ok) return bfail(b, QLGPU_ERR_UNSUPPORTED, "queue engine: MHD_BQlin batches with every NZ <= 128 only");
+    QB_CK(cudaSetDevice(b->device));
+    for (int i = 0; i < 4; ++i) b->qpasses[i] = passes4[i];
+    b->engine = QLGPU_BATCH_ENGINE_QUEUE;
+    b->drop_case = -1;
+    b->qdirty = true;
+    drop_graphs(b);
+    return queue_plan(b);
+}
+
+int qlgpu_batch_queue_trace(qlgpu_batch_t* b, double* out4) {
+    if (!b || !out4) return QLGPU_ERR_ARG;
+    if (!b->d_qtrace) return bfail(b, QLGPU_ERR_UNSUPPORTED, "queue trace: set QLGPU_TRACE=1 before qlgpu_batch_create");
+    QB_CK(cudaSetDevice(b->device));
+    std::vector<unsigned long long> t(4 * (size_t)b->qgrid);
+    QB_CK(cudaMemcpy(t.data(), b->d_qtrace, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 4; ++k) out4[k] = 0.0;
+    for (int g = 0; g < b->qgrid; ++g)
+        for (int k = 0; k < 4; ++k) out4[k] += (double)t[4 * (size_t)g + k];
+    for (int k = 0; k < 3; ++k) out4[k] *= 1e-3 / b->qgrid;  // us per CTA
+    out4[3] /= b->qgrid;                                     // chunks per CTA
     return QLGPU_OK;
 }
 

@@ -1,0 +1,21 @@
+// qlgpu_ens_host.h -- host view of the chunk-queue engine (qlgpu_ens.cuh):
+// the launch wrapper and the sizes the batch host code needs.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "qlgpu_types.h"
+
+namespace qlgpu {
+namespace ens {
+
+constexpr int ENS_THREADS = 512;
+
+cudaError_t launch(int integ, const EnsLaunch& L, int grid, size_t smem, cudaStream_t st);
+const void* kernel(int integ);
+size_t smem_bytes(int NZ);   // dynamic shared memory of one NZ class (16, 32, 64, 128)
+int modes_per_pass(int NZ);  // modes a CTA steps at once
+
+}  // namespace ens
+}  // namespace qlgpu

@@ -134,6 +134,8 @@ struct BatchCtl {
     int fail_case;   // case and stage of the first wait that gave up
     int fail_stage;
     unsigned long long t_start;  // %globaltimer at the start of CTA 0
+    unsigned next;               // chunk-queue engine: next ticket
+    int fail_where;              // 0 a wait for other CTAs of the case, 1 a wait for a staged copy
 };
 
 struct BatchLaunch {
@@ -146,6 +148,40 @@ struct BatchLaunch {
     int parity;                    // 1: the first step starts from lin buffer 1
     long long wait_ns;             // bound on one wait for the other CTAs of a case
 };
+
+// ---------------------------------------------------------------------------
+// Chunk-queue engine of the batch (qlgpu_ens.cuh)
+// ---------------------------------------------------------------------------
+namespace ens {
+
+// One entry of a round: chunk j of case c.
+struct RoundItem {
+    int c, j;
+};
+
+// Per-case constants of the queue engine.
+struct EnsCase {
+    int NZ, nch, mpc, pad;  // NZ class, chunks per stage, modes per chunk
+    const cplx* tw8;        // [8][NZ/8] twiddles of the 8-point layout
+};
+
+struct EnsLaunch {
+    const BatchCase* cases;
+    const EnsCase* ec;
+    const RoundItem* round;  // [R] one stage of every case
+    unsigned* epoch;         // [ncases * BATCH_EPOCH_STRIDE]: +0 stages released, +1 chunks done
+    BatchCtl* ctl;
+    unsigned* next;          // ticket counter
+    unsigned long long* case_end;
+    int R;                   // items per round
+    int nrounds;             // 3 K
+    int parity;
+    int pad;
+    long long wait_ns;
+    unsigned long long* trace;  // optional [grid][4] %globaltimer sums: stage waits, chunks, mean-field stages, count
+};
+
+}  // namespace ens
 
 }  // namespace qlgpu
 

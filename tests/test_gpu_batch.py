@@ -45,10 +45,23 @@ def states(cases, sigma=0.2):
     return out
 
 
-def run_batch(cases, sts, n, diag_every=1, mapping=None, tune=0):
+def bq_cases(integ=0):
+    """MHD_BQlin cases of every NZ the chunk-queue engine takes (16 ... 128), uneven mode counts."""
+    specs = [(8, 6, 16, 1 / 700), (16, 16, 32, 1 / 2000), (8, 8, 64, 1 / 3000), (12, 10, 32, 1 / 1500),
+             (6, 8, 128, 1 / 5000), (20, 20, 64, 1 / 4000), (18, 14, 128, 1 / 6000), (34, 30, 32, 1 / 800)]
+    return [QLParams(integrator=integ, nx=nx, ny=ny, NZ=NZ, nu=eta * (1 + i % 3), eta=eta, dt=0.01)
+            for i, (nx, ny, NZ, eta) in enumerate(specs)]
+
+
+def run_batch(cases, sts, n, diag_every=1, mapping=None, tune=0, engine=None, chunks=None):
     require_gpu()
     res = []
     with QLBatch(cases) as b:
+        if engine is not None:
+            b.set_engine(engine)
+            assert b.engine() == engine
+        if chunks is not None:
+            b.set_chunks(chunks)
         if mapping is not None:
             b.set_mapping(*mapping)
         for c, (lin, mf, kx0) in enumerate(sts):
@@ -205,3 +218,97 @@ def test_batch_of_tiny_and_ragged_cases():
             assert np.array_equal(ko, ko2)
             assert (np.linalg.norm(lo2) == 0 and np.abs(lo).max() == 0) or rel(lo, lo2) < TOL
             assert rel(mo, mo2) < TOL and series_rel(d, d2) < TOL
+
+
+# ---------------------------------------------------------------------------
+# Chunk-queue engine (MHD_BQlin, NZ <= 128): the default for such batches
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("integ", [0, 1])
+def test_queue_engine_matches_oracle(integ):
+    cases = bq_cases(integ)
+    sts = states(cases)
+    n = 30
+    res, m = run_batch(cases, sts, n, engine="queue")
+    assert m["warps"] == 16
+    for p, (lin, mf, kx0), (t, lo, mo, ko, d) in zip(cases, sts, res):
+        t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, n, diag_every=1)
+        assert t == t2 and np.array_equal(ko, ko2)
+        assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL, (p, rel(lo, lo2), rel(mo, mo2))
+        assert d.shape == d2.shape and series_rel(d, d2) < TOL
+
+
+def test_queue_engine_is_the_default_and_chunking_independent():
+    # chunk sizes change only which CTA steps which modes and how many chunk sums there are
+    cases = bq_cases()
+    sts = states(cases)
+    with QLBatch(cases) as b:
+        assert b.engine() == "queue"
+    a, ma = run_batch(cases, sts, 20, diag_every=0, chunks=[1, 1, 1, 1])
+    c, mc = run_batch(cases, sts, 20, diag_every=0, chunks=[3, 2, 5, 1])
+    assert ma["ncta"] != mc["ncta"]
+    for x, y in zip(a, c):
+        assert rel(x[1], y[1]) < 1e-12 and rel(x[2], y[2]) < 1e-12
+    # the same chunking twice is bit for bit the same
+    c2, _ = run_batch(cases, sts, 20, diag_every=0, chunks=[3, 2, 5, 1])
+    for x, y in zip(c, c2):
+        assert np.array_equal(x[1], y[1]) and np.array_equal(x[2], y[2])
+
+
+def test_queue_engine_matches_item_engine():
+    cases = bq_cases()
+    sts = states(cases)
+    a, _ = run_batch(cases, sts, 25, diag_every=5, engine="queue")
+    b, _ = run_batch(cases, sts, 25, diag_every=5, engine="items")
+    for x, y in zip(a, b):
+        assert np.array_equal(x[3], y[3])
+        assert rel(x[1], y[1]) < 1e-12 and rel(x[2], y[2]) < 1e-12 and series_rel(x[4], y[4]) < 1e-12
+
+
+def test_queue_engine_tune_keeps_state_and_parity():
+    cases = bq_cases()
+    sts = states(cases)
+    require_gpu()
+    with QLBatch(cases) as b:
+        for c, (lin, mf, kx0) in enumerate(sts):
+            b.set_state(c, 0.0, lin, mf, kx0)
+        assert b.tune(2) > 0 and b.engine() == "queue"
+        for c, (lin, mf, kx0) in enumerate(sts):
+            t, lo, mo, ko = b.get_state(c)
+            assert t == 0.0 and np.array_equal(lo, lin) and np.array_equal(mo, mf)
+        b.step(5)
+        b.step(4)
+        for p, (lin, mf, kx0), c in zip(cases, sts, range(len(cases))):
+            t, lo, mo, ko = b.get_state(c)
+            t2, lo2, mo2, ko2, _ = O.run(p, 0.0, lin, mf, kx0, 9)
+            assert abs(t - t2) < 1e-15 and rel(lo, lo2) < TOL and rel(mo, mo2) < TOL
+
+
+def test_queue_engine_wait_bound_reports_timeout():
+    # one chunk of case 1 is left out of every stage: the case's next stage never
+    # becomes ready, the bounded wait ends the launch with a status, and the batch
+    # is usable again after set_engine and set_state
+    from ql_dns_b200._capi import QLGPUError
+    cases = bq_cases()[:4]
+    sts = states(cases)
+    require_gpu()
+    with QLBatch(cases) as b:
+        b.set_chunks([1, 1, 1, 1])
+        for c, (lin, mf, kx0) in enumerate(sts):
+            b.set_state(c, 0.0, lin, mf, kx0)
+        b.set_wait(0.2)
+        b.debug_drop_item(1)
+        with pytest.raises(QLGPUError) as ei:
+            b.step(2)
+        assert ei.value.code == 4 and "waiting" in str(ei.value)
+        st, ls = b.status()
+        assert ls & 8
+        b.set_engine("queue")
+        for c, (lin, mf, kx0) in enumerate(sts):
+            b.set_state(c, 0.0, lin, mf, kx0)
+        b.step(4)
+        st, ls = b.status()
+        assert ls == 0
+        for p, (lin, mf, kx0), c in zip(cases, sts, range(4)):
+            t, lo, mo, ko = b.get_state(c)
+            t2, lo2, mo2, ko2, _ = O.run(p, 0.0, lin, mf, kx0, 4)
+            assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL

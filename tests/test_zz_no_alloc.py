@@ -68,3 +68,45 @@ def test_rhs_noalloc_rejects_oversized_case():
     buf = ctypes.create_string_buffer(256)
     L.qlgpu_last_error(None, buf, 256)
     assert b"8192" in buf.value
+
+
+def test_rhs_noalloc_large_grid_matches_oracle_and_changes_grid():
+    # Three calls in a row on different grids: 64x64 modes at NZ = 128 (126 CTAs, so the
+    # two-level reduction over CTA groups runs), then 16x16 at NZ = 32 with kx0 = NULL (the
+    # library's own kx table) on the legacy default stream, then the large grid again.  A
+    # table left over from the previous call would fail the next comparison.  Each result is
+    # checked against the CPU oracle and against qlgpu_rhs.
+    require_gpu()
+    import torch
+    from oracle import oracle as O
+    L = _capi.load()
+    big = mri_16x16_nz32(nx=64, ny=64, NZ=128)
+    small = mri_16x16_nz32(nx=16, ny=16, NZ=32)
+    for call, (p, seed, t, dtl, own_kx) in enumerate([(big, 41, 0.61, 0.0013, True), (small, 42, 0.29, 0.004, False),
+                                                      (big, 43, 1.37, 0.0009, True)]):
+        cp = _capi.to_c(p)
+        lin, mf, kx0 = initial_state(p, seed, sigma=0.3)
+        if own_kx:
+            kx0 = kx0 + 0.25 * (2 * np.pi / p.L[0])  # a sheared wavenumber set, not the default table
+        Fo, Fmo, Lo = O.rhs(p, t, dtl, lin, mf, kx0 if own_kx else None)
+        with QLSolver(p) as s:
+            s.set_state(0.0, lin, mf, kx0 if own_kx else None)
+            F, Fm, Lop = s.rhs(t, dtl, lin, mf)
+        d_lin, d_mf = _dev(lin), _dev(mf)
+        d_kx0 = _dev(kx0) if own_kx else None
+        d_F = torch.empty_like(d_lin)
+        d_Fm = torch.empty_like(d_mf)
+        d_L = torch.empty(lin.shape, dtype=torch.float64, device="cuda")
+        if own_kx:
+            stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        else:
+            torch.cuda.synchronize()
+            stream = None  # legacy default stream
+        rc = L.qlgpu_rhs_noalloc(ctypes.byref(cp), t, dtl, d_lin.data_ptr(), d_mf.data_ptr(),
+                                 d_kx0.data_ptr() if own_kx else None, d_F.data_ptr(), d_Fm.data_ptr(),
+                                 d_L.data_ptr(), stream)
+        _capi.check(rc, None)
+        torch.cuda.synchronize()
+        F2, Fm2, L2 = d_F.cpu().numpy(), d_Fm.cpu().numpy(), d_L.cpu().numpy()
+        assert rel(F2, Fo) < 1e-11 and rel(Fm2, Fmo) < 1e-10 and rel(L2, Lo) < 1e-14, (call, rel(F2, Fo), rel(Fm2, Fmo))
+        assert rel(F2, F) < 1e-12 and rel(Fm2, Fm) < 1e-11 and rel(L2, Lop) < 1e-15, call
