@@ -425,6 +425,7 @@ def ensemble_parity(cases, sts, recs_e2e, outs_e2e, timed_out, args):
         err_e2e = max(err_e2e, rel(outs_e2e[c][1], l1))
         err_e2e_mf = max(err_e2e_mf, rel(outs_e2e[c][2], m1))
         dg = np.vstack(recs_e2e[c])
+        d1 = d1[1:]  # the oracle's series starts with the initial record
         for col in range(1, 13):
             scale = np.abs(d1[:, col]).max()
             if scale > 0:

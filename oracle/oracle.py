@@ -148,8 +148,8 @@ def philox(ctr, key, kind: str = "strict"):
 
 
 def tlm_maxwell(p, t0, lin, mf, kx0, dlin, dmf=None, nsteps: int = 1, kind: str = "strict"):
-    """Tangent-linear run (MHD_BQlin / RK3CN_Elin): (J, dJ) with J the mean over the
-    steps of the fluctuation Maxwell stress and dJ its derivative along (dlin, dmf)."""
+    """Tangent-linear run (MHD_BQlin with RK3CN_Elin or RK3CN): (J, dJ) with J the mean
+    over the steps of the fluctuation Maxwell stress and dJ its derivative along (dlin, dmf)."""
     lin = np.ascontiguousarray(lin, dtype=np.complex128)
     mf = np.ascontiguousarray(mf, dtype=np.complex128)
     dlin = np.ascontiguousarray(dlin, dtype=np.complex128)
@@ -161,5 +161,5 @@ def tlm_maxwell(p, t0, lin, mf, kx0, dlin, dmf=None, nsteps: int = 1, kind: str 
     rc = lib(kind).oracle_tlm_maxwell(ctypes.byref(pp), t0, _dp(lin), _dp(mf), k, _dp(dlin), dm, nsteps,
                                       _dp(J), _dp(dJ))
     if rc:
-        raise ValueError("the tangent-linear oracle covers MHD_BQlin with RK3CN_Elin")
+        raise ValueError("the tangent-linear oracle covers MHD_BQlin")
     return float(J[0]), float(dJ[0])

@@ -870,8 +870,10 @@ struct Integrator {
             }
     }
 
-    // Crank-Nicolson update of stage s (RK3CN.cpp:102-115)
-    void update_cn(State& sol, const State& F, const State* Fp, double linC, double n1, double n2) {
+    // Crank-Nicolson update of stage s (RK3CN.cpp:102-115).  advance_old = false leaves the
+    // old operator in place (the tangent of the same stage is updated first with it).
+    void update_cn(State& sol, const State& F, const State* Fp, double linC, double n1, double n2,
+                   bool advance_old = true) {
         const int nz = M.d.nz;
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static) num_threads(M.nthreads)
@@ -900,7 +902,7 @@ struct Integrator {
                 else
                     u[k] = n1 * denom * F.pMF(mm)[k] + (1 + linC * Lm) * denom * u[k];
             }
-        linOpOld = linOp;  // RK3CN.cpp:119-122
+        if (advance_old) linOpOld = linOp;  // RK3CN.cpp:119-122
     }
 
     double step(double t, double dt, State& sol, const std::vector<double>& kx0) {
@@ -1089,18 +1091,20 @@ int oracle_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
     return 0;
 }
 
-// Tangent-linear run for MHD_BQlin / RK3CN_Elin (the checker of the adjoint).
-// J = (1/N) sum_{n=1..N} AM_b after each step (main.cpp:108-133, AM_b of
-// MHD_BQlin.cpp:392,424) and its derivative dJ in the direction (dlin, dmf)
+// Tangent-linear run for MHD_BQlin with RK3CN_Elin or RK3CN (the checker of the
+// adjoint).  J = (1/N) sum_{n=1..N} AM_b after each step (main.cpp:108-133, AM_b
+// of MHD_BQlin.cpp:392,424) and its derivative dJ in the direction (dlin, dmf)
 // of the initial state.  The state is propagated with the tangent alongside:
-// the stage update is linear (RK3CN_Elin.cpp:102-104) and is applied to both;
+// the stage update is linear (RK3CN_Elin.cpp:102-104; RK3CN.cpp:105-107 with
+// the operators of the stage and of the previous stage) and is applied to both;
 // the remap zeroes the same modes in both; the derivative of the rhs and of
 // AM_b, both polynomials of degree two in the state, is taken exactly by the
 // polarization identity D f(x) d = (f(x + h d) - f(x - h d)) / (2 h).
 int oracle_tlm_maxwell(const OracleParams* p, double t0, const double* lin_in, const double* mf_in,
                        const double* kx0_in, const double* dlin_in, const double* dmf_in, int nsteps, double* J,
                        double* dJ) {
-    if (p->model != 0 || p->integrator != 0) return 1;
+    if (p->model != 0) return 1;
+    const bool cn = p->integrator == 1;
     Model M(*p);
     State s, ds;
     s.init(M.d);
@@ -1147,21 +1151,31 @@ int oracle_tlm_maxwell(const OracleParams* p, double t0, const double* lin_in, c
     };
     const double dt = p->dt;
     const double a0 = I.a0, a1 = I.a1, a2 = I.a2, b1 = I.b1, b2 = I.b2, p1 = I.p1, p2 = I.p2;
+    const double lf = cn ? dt / 2 : dt;  // RK3CN.cpp:86 (dt/2) or RK3CN_Elin.cpp:89 (dt)
+    // one stage update of the tangent, then of the state (the CN old operator advances after both)
+    auto update2 = [&](const State& F, const State* Fp, const State& dF, const State* dFp, double linC, double n1,
+                       double n2) {
+        if (cn) {
+            I.update_cn(ds, dF, dFp, linC, n1, n2, false);
+            I.update_cn(s, F, Fp, linC, n1, n2, true);
+        } else {
+            I.update_exp(ds, dF, dFp, linC, n1, n2);
+            I.update_exp(s, F, Fp, linC, n1, n2);
+        }
+    };
     double sJ = 0, sdJ = 0;
     for (int n = 0; n < nsteps; ++n) {
-        // RK3CN_Elin::Step (RK3CN_Elin.cpp:86-177) on the state and the tangent
+        // RK3CN_Elin::Step (RK3CN_Elin.cpp:86-177) / RK3CN::Step (RK3CN.cpp:77-202) on the
+        // state and the tangent
         M.rhs(t, dt * p1, s, F1, kx0, I.linOp);
         tangent_rhs(t, dt * p1, s, ds, dF1);
-        I.update_exp(s, F1, nullptr, dt * a0, a0 * dt, 0);
-        I.update_exp(ds, dF1, nullptr, dt * a0, a0 * dt, 0);
+        update2(F1, nullptr, dF1, nullptr, lf * a0, a0 * dt, 0);
         M.rhs(t + dt * p1, dt * (p2 - p1), s, F2, kx0, I.linOp);
         tangent_rhs(t + dt * p1, dt * (p2 - p1), s, ds, dF2);
-        I.update_exp(s, F2, &F1, dt * (a1 + b1), a1 * dt, b1 * dt);
-        I.update_exp(ds, dF2, &dF1, dt * (a1 + b1), a1 * dt, b1 * dt);
+        update2(F2, &F1, dF2, &dF1, lf * (a1 + b1), a1 * dt, b1 * dt);
         M.rhs(t + dt * p2, dt * (1.0 - p2), s, F1, kx0, I.linOp);
         tangent_rhs(t + dt * p2, dt * (1.0 - p2), s, ds, dF1);
-        I.update_exp(s, F1, &F2, dt * (a2 + b2), a2 * dt, b2 * dt);
-        I.update_exp(ds, dF1, &dF2, dt * (a2 + b2), a2 * dt, b2 * dt);
+        update2(F1, &F2, dF1, &dF2, lf * (a2 + b2), a2 * dt, b2 * dt);
         t += dt;
         if (p->remap) {
             std::vector<double> k2 = kx0;

@@ -1,11 +1,12 @@
 // qlgpu_adjoint.cu -- gradient of the time-averaged Maxwell stress with
-// respect to the initial fluctuation field: the forward MHD_BQlin /
-// RK3CN_Elin run with checkpoints, then the discrete adjoint of every step in
+// respect to the initial fluctuation field: the forward MHD_BQlin run
+// (RK3CN_Elin or RK3CN) with checkpoints, then the discrete adjoint of every step in
 // reverse, with the stages of each checkpoint window recomputed
 // (qlgpu_adjoint_maxwell in include/qlgpu.h; kernels in qlgpu_adjoint.cuh).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -103,6 +104,13 @@ int afail(qlgpu_t* h, int code, const std::string& msg) {
     return code;
 }
 
+int adj_integ(const qlgpu_t* h) { return h->p.integrator == QLGPU_INTEG_RK3CN ? INTEG_CN : INTEG_EXP; }
+
+// the stage-start record of RK3CN copies the clock's bytes from t_old (CnRec's layout)
+static_assert(offsetof(DevClock, dtlin_old) == offsetof(DevClock, t_old) + 8 &&
+                  offsetof(DevClock, old_init) == offsetof(DevClock, t_old) + 16 && sizeof(CnRec) == 24,
+              "CnRec mirrors DevClock from t_old");
+
 #define QA_CK(call)                                                                                \
     do {                                                                                           \
         cudaError_t e_ = (call);                                                                   \
@@ -150,6 +158,7 @@ struct AdjJob {
     DevClock cend{};
     cplx *stU = nullptr, *stB = nullptr, *postU = nullptr;
     double *kx_pre = nullptr, *kx_post = nullptr, *t_pre = nullptr;
+    CnRec* cn_pre = nullptr;  // RK3CN: the old-operator clock fields at every stage start of the window
     cplx *lamU[2] = {nullptr, nullptr}, *lamB[2] = {nullptr, nullptr};
     cplx *lamF[2] = {nullptr, nullptr}, *lamG[2] = {nullptr, nullptr};
     double *prof = nullptr, *bpart = nullptr, *bsum = nullptr;
@@ -168,8 +177,8 @@ int adj_begin(AdjJob& j, qlgpu_t* h, double t0, const double* lin0, const double
     j.h = h;
     if (!lin0 || !mf0 || nsteps < 1 || checkpoint_every < 1)
         return afail(h, QLGPU_ERR_ARG, "null argument, nsteps < 1 or checkpoint_every < 1");
-    if (h->p.model != QLGPU_MODEL_MHD_BQLIN || h->p.integrator != QLGPU_INTEG_RK3CN_ELIN)
-        return afail(h, QLGPU_ERR_UNSUPPORTED, "the adjoint covers MHD_BQlin with RK3CN_Elin");
+    if (h->p.model != QLGPU_MODEL_MHD_BQLIN)
+        return afail(h, QLGPU_ERR_UNSUPPORTED, "the adjoint covers MHD_BQlin (RK3CN_Elin or RK3CN)");
     if (h->noise_f != 0.0 || h->cfl > 0) return afail(h, QLGPU_ERR_UNSUPPORTED, "the adjoint runs at fixed dt, no noise");
     if (!pick_ops(h->NZ, &j.ops)) return afail(h, QLGPU_ERR_UNSUPPORTED, "unsupported NZ");
     QA_CK(cudaSetDevice(h->device));
@@ -258,6 +267,7 @@ int adj_alloc_backward(AdjJob& j) {
     QA_CK(j.pool.get(&j.kx_pre, (size_t)j.C * j.nxy));
     QA_CK(j.pool.get(&j.kx_post, j.nxy));
     QA_CK(j.pool.get(&j.t_pre, (size_t)j.C + 1));
+    QA_CK(j.pool.get(&j.cn_pre, (size_t)j.C * 3));
     for (int i = 0; i < 2; ++i) {
         QA_CK(j.pool.get(&j.lamU[i], j.nlin));
         QA_CK(j.pool.get(&j.lamB[i], j.nmfe));
@@ -299,7 +309,10 @@ int adj_recompute_step(AdjJob& j, int n) {
                                                j.nlin * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
         const cudaError_t e2 = cudaMemcpyAsync(j.stB + ((size_t)n * 3 + s) * j.nmfe, h->d_mf, j.nmfe * sizeof(cplx),
                                                cudaMemcpyDeviceToDevice, st);
-        if (herr == cudaSuccess) herr = e1 != cudaSuccess ? e1 : e2;
+        // t_old, dtlin_old, old_init of the clock (the layout of CnRec)
+        const cudaError_t e3 = cudaMemcpyAsync(j.cn_pre + (size_t)n * 3 + s, &h->d_clk->t_old, sizeof(CnRec),
+                                               cudaMemcpyDeviceToDevice, st);
+        if (herr == cudaSuccess) herr = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
     });
     QA_CK(herr);
     return QLGPU_OK;
@@ -337,6 +350,7 @@ int adj_backward_step(AdjJob& j, int steps, int n) {
         M.prof = j.prof;
         M.tw = h->d_tw;
         M.sc = S;
+        M.integ = adj_integ(h);
         j.ops.mf_pre(M, h->dp, st);
         AdjStageArgs A;
         std::memset(&A, 0, sizeof(A));
@@ -354,6 +368,8 @@ int adj_backward_step(AdjJob& j, int steps, int n) {
         A.prof = j.prof;
         A.bpart = j.bpart;
         A.t_dev = j.t_pre + n;
+        A.cn = j.cn_pre + (size_t)n * 3 + s;
+        A.integ = adj_integ(h);
         A.sc = S;
         j.ops.modes(A, h->dp, h->nxy, st);
         const int nout = 3 * h->NZ;
@@ -403,6 +419,7 @@ int adj_backward_step_seeds(SeedReverse& R, cudaStream_t st, int steps, int n) {
         std::memset(&M, 0, sizeof(M));
         M.tw = h->d_tw;
         M.sc = h->sc[s];
+        M.integ = adj_integ(h);
         R.ops.mf_pre_s(M, h->dp, X, ns, st);
         AdjStageArgs A;
         std::memset(&A, 0, sizeof(A));
@@ -411,6 +428,7 @@ int adj_backward_step_seeds(SeedReverse& R, cudaStream_t st, int steps, int n) {
         A.kyi = h->d_kyi;
         A.ilap2 = h->d_ilap2;
         A.tw = h->d_tw;
+        A.integ = adj_integ(h);
         A.sc = h->sc[s];
         R.ops.modes_s(A, h->dp, X, h->nxy, ns, st);
         const int nout = 3 * h->NZ;
@@ -551,6 +569,7 @@ int run_jobs_persistent(std::vector<AdjJob>& jobs, double t0, const double* lin0
         for (int q = 0; q < nj; ++q) {
             const AdjJob& j = jobs[q];
             AdjSeedBufs& e = hb[q];
+            e.cn_pre = adj_integ(j.h) == INTEG_CN ? j.cn_pre : nullptr;
             e.stU = j.stU;
             e.stB = j.stB;
             e.postU = j.postU;
@@ -612,7 +631,7 @@ int run_jobs_persistent(std::vector<AdjJob>& jobs, double t0, const double* lin0
             QA_CK(cudaMemcpyAsync(d.clk, j.ck_clk + w, sizeof(DevClock), cudaMemcpyDeviceToDevice, bs));
             // the mean-field profile cache holds a later mean field: recompute it in the first stage
             QA_CK(cudaMemcpyAsync(&d.clk->mfr_valid, &zero, sizeof(int), cudaMemcpyHostToDevice, bs));
-            qlgpu_batch_set_record(b, q, j.stU, j.stB, j.kx_pre, j.t_pre);
+            qlgpu_batch_set_record(b, q, j.stU, j.stB, j.kx_pre, j.t_pre, j.cn_pre);
         }
         rc = qlgpu_batch_step(b, steps, 0, nullptr, 0, nullptr);
         if (rc) {

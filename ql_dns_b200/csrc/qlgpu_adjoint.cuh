@@ -1,5 +1,5 @@
-// qlgpu_adjoint.cuh -- discrete adjoint of one RK3CN_Elin stage of MHD_BQlin
-// (sm_100a kernels).  No counterpart in the reference.
+// qlgpu_adjoint.cuh -- discrete adjoint of one RK3CN_Elin or RK3CN stage of
+// MHD_BQlin (sm_100a kernels).  No counterpart in the reference.
 //
 // Forward stage (QL_DNS/Integrators/RK3CN_Elin.cpp:86-177 with
 // QL_DNS/Models/MHD_BQlin.cpp:117-284), per mode, with R_f = P(fac f) the
@@ -8,7 +8,10 @@
 //   F_zeta= T(-i a dBy R_b + ddBy R_bz + i b By R_eta) + (q - 2 Omega) i c u
 //   F_eta = T(-i a dBy R_u + i b By R_zeta - 2 dBy R_{i c uz} - ddBy R_uz) - q i c b
 //   F_u   = T(i b By R_b) + ilapF (T(2 a b dBy R_bz) + 2 a b q u + 2 Omega i c zeta)
-//   u' = E (n1 F + n2 Fprev + u),   E = exp(linC L)
+//   u' = E (n1 F + n2 Fprev + u),   E = exp(linC L)            (RK3CN_Elin.cpp:102-104)
+//   u' = D (n1 F + n2 Fprev) + C u,  D = 1/(1 - linC L), C = (1 + linC Lold) D
+//                                                              (RK3CN.cpp:105-107, Lold the
+//                                                               previous stage's operator)
 // and for the mean field G_Bx = EMF_x, G_By = -q Bx + EMF_y with the real
 // stress profiles  Ex = sum_modes mult (Re(R_bz R_u*) - Re(R_uz R_b*)),
 // Ey = sum_modes mult (Re(R_bz R_uy*) - Re(R_uz R_by*)), EMF = rs_fac i kz T(E)
@@ -18,7 +21,8 @@
 // (lamU, lamB, lamFprev, lamGprev) with the real inner product
 // <x, y> = Re sum conj(x) y:  mu = E lamU', lamF = n1 mu + lamF_out,
 // lamU = mu + (dR/dU)^H lamF + (dEMF/dU)^H lamG, lamFprev = n2 mu, and the
-// mean-field part likewise.  One CTA per mode: 14 inverse transforms (the nine
+// mean-field part likewise (Crank-Nicolson: mu = D lamU' and the direct term
+// C lamU' in place of mu).  One CTA per mode: 14 inverse transforms (the nine
 // forward real-space fields and five back-propagated rhs fields W = P(lamF)),
 // a pointwise pass giving the nine real-space adjoints and the mode's
 // contribution to the adjoint of the mean-field profiles, nine forward
@@ -44,6 +48,9 @@ struct AdjStageArgs {
     double* bpart;         // [3][NZ][nxy] per-mode adjoint of the mean-field profiles
     double t_s;            // stage time (when t_dev is null)
     const double* t_dev;   // the step's start time on the device: stage time = *t_dev + sc.t_off
+    const CnRec* cn;       // RK3CN: the old-operator fields at the stage start
+    int integ;             // INTEG_EXP or INTEG_CN
+    int pad;
     StageConst sc;
 };
 
@@ -63,10 +70,13 @@ struct AdjGeom {
     static_assert(sizeof(double) * 4 * G::nz <= sizeof(cplx) * 2 * G::XSIZE, "E table fits two exchange buffers");
 };
 
-// E = exp(linC L_f) of field f at stored index s (RK3CN_Elin.cpp:102-104), L at the stage end.
+// E = exp(linC L_f) of field f at stored index s (RK3CN_Elin.cpp:102-104), L at the stage
+// end; for RK3CN D = 1/(1 - linC L_f) (RK3CN.cpp:105).
 __device__ __forceinline__ double adj_efac(const DevParams& P, const StageConst& S, double kxe, double ky, double kz2,
-                                           int f) {
-    return exp(__dmul_rn(S.linC, linop_f<MODEL_BQLIN>(P, lap_end<MODEL_BQLIN>(P, kxe, ky, kz2), f)));
+                                           int f, int integ) {
+    const double L = linop_f<MODEL_BQLIN>(P, lap_end<MODEL_BQLIN>(P, kxe, ky, kz2), f);
+    if (integ == INTEG_CN) return __drcp_rn(__dsub_rn(1.0, __dmul_rn(S.linC, L)));
+    return exp(__dmul_rn(S.linC, L));
 }
 
 // The stage adjoint of one mode (one CTA).  A may live in parameter space (one
@@ -108,7 +118,17 @@ __device__ __forceinline__ void adj_modes_body(const AdjStageArgs& A, const DevP
     for (int i = tid; i < 4 * nz; i += blockDim.x) {
         const int f = i / nz, s = i % nz;
         const int kzi = s <= G::H ? s : s - nz;
-        etab[i] = adj_efac(P, S, kxe, ky, kz2val(kzval(kzi, P.kzL)), f);
+        etab[i] = adj_efac(P, S, kxe, ky, kz2val(kzval(kzi, P.kzL)), f, A.integ);
+    }
+    // RK3CN: kx where the previous stage's operator was evaluated (RK3CN.cpp:119-122;
+    // the init form at the run's start, RK3CN.cpp:57), as the forward stage computes it
+    double kxo = 0.0;
+    int old_init = 0;
+    if (A.integ == INTEG_CN) {
+        const double tclock = A.t_dev ? *A.t_dev : __dsub_rn(A.t_s, S.t_off);
+        old_init = A.cn->old_init;
+        if (old_init) kxo = kx_at(kx0, P.q, tclock, ky);
+        else kxo = __dadd_rn(kx_at(kx0, P.q, A.cn->t_old, ky), __dmul_rn(__dmul_rn(P.q, A.cn->dtlin_old), ky));
     }
     __syncthreads();
 
@@ -256,6 +276,13 @@ __device__ __forceinline__ void adj_modes_body(const AdjStageArgs& A, const DevP
         const double il2 = il2row[s];
         const cplx mu = cscale(lo[f * nz + s], etab[idx]);
         cplx r = mu;
+        if (A.integ == INTEG_CN) {
+            // the direct term (1 + linC Lold) D lamU' (RK3CN.cpp:107)
+            const double lo_lap = old_init ? lap_init<MODEL_BQLIN>(P, kxo, lap2val(ky, kz2, z0))
+                                           : lap_end<MODEL_BQLIN>(P, kxo, ky, kz2);
+            const double Lold = linop_f<MODEL_BQLIN>(P, lo_lap, f);
+            r = cscale(mu, __dadd_rn(1.0, __dmul_rn(S.linC, Lold)));
+        }
         if (f == 0 || f == 1) {
             // uz = (a c u - i b zeta) il2, i c uz, uy = (a b u + i c zeta) il2
             const cplx luz = cscale(csub(RW[4 * NZ + s], imul(RW[6 * NZ + s], c)), fac);
@@ -308,6 +335,7 @@ __global__ void __launch_bounds__(AdjGeom<NZ>::THREADS, 6)
 // The per-seed buffers are read from a device table; the position in the sweep
 // (step n of a window of `steps`, stage s, buffer parity) is a launch argument.
 struct AdjSeedBufs {
+    const CnRec* cn_pre;   // [C][3] RK3CN old-operator fields at every stage start (null: RK3CN_Elin)
     const cplx* stU;       // [C][3] recorded stage inputs
     const cplx* stB;       // [C][3] recorded stage mean fields
     const cplx* postU;     // the window's end state
@@ -357,6 +385,7 @@ __global__ void __launch_bounds__(AdjGeom<NZ>::THREADS, 6)
         sA.prof = B.prof;
         sA.bpart = B.bpart;
         sA.t_dev = B.t_pre + X.n;
+        sA.cn = B.cn_pre ? B.cn_pre + (size_t)X.n * 3 + X.s : nullptr;
     }
     __syncthreads();
     adj_modes_body<NZ>(sA, P, blockIdx.x);
@@ -377,6 +406,8 @@ struct AdjMfArgs {
     cplx* lamGp;           // n2 muB (null: first stage)
     double* prof;          // [5][NZ] out
     const cplx* tw;
+    int integ;             // INTEG_EXP or INTEG_CN
+    int pad;
     StageConst sc;
 };
 
@@ -395,13 +426,16 @@ __device__ __forceinline__ void adj_mf_pre_body(const AdjMfArgs& A, const DevPar
         const int kzi = s <= G::H ? s : s - nz;
         const double kz2 = kz2val(kzval(kzi, P.kzL));
         const double Lm = P.ql ? __dmul_rn(P.eta, kz2) : 0.0;
-        const double e = exp(__dmul_rn(S.linC, Lm));
+        // exp(linC Lm), or D = 1/(1 - linC Lm) and the direct term (1 + linC Lm) D for RK3CN
+        const double e = A.integ == INTEG_CN ? __drcp_rn(__dsub_rn(1.0, __dmul_rn(S.linC, Lm)))
+                                             : exp(__dmul_rn(S.linC, Lm));
         const cplx muB = cscale(A.lamB_out[m * nz + s], e);
         cplx lg = cscale(muB, S.n1);
         if (A.lamG_out) lg = cadd(lg, A.lamG_out[m * nz + s]);
         lamG[m][s] = lg;
         if (A.lamGp) A.lamGp[m * nz + s] = cscale(muB, S.n2);
-        A.lamB_in[m * nz + s] = muB;
+        A.lamB_in[m * nz + s] =
+            A.integ == INTEG_CN ? cscale(muB, __dadd_rn(1.0, __dmul_rn(S.linC, Lm))) : muB;
     }
     __syncthreads();
     if (tid < 2 * nz && P.ql) {

@@ -100,6 +100,7 @@ __device__ __noinline__ bool batch_item_stage(const BatchCase* cs, int s, int sw
             sA.rec_mf = cs->rec_mf + ((size_t)n * 3 + s) * nmfe;
             sA.rec_kx = s == 0 ? cs->rec_kx + (size_t)n * sP.nxy : nullptr;
             sA.rec_t = s == 0 ? cs->rec_t + n : nullptr;
+            sA.rec_cn = cs->rec_cn ? cs->rec_cn + (size_t)n * 3 + s : nullptr;
         }
     }
     __syncthreads();

@@ -265,6 +265,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned ph) {
 struct ChunkHdr {
     DevParams P;
     StageArgs A;
+    // constants of the chunk's stage from the case's clock (thread 0, after the header)
+    double tclock, t_new, qt, ts, Om2, cn_t_old, cn_dtlin_old;
+    int cn_old_init, diag_due, has_prev, pad2;
     int c, r, ok, top;
     unsigned tk;
     int pad[3];
@@ -405,23 +408,36 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
     const StageArgs& A = hd.A;
     const StageConst& S = A.sc;
     const int nzd = E::nz;
-    const double tclock = __ldcg(&A.clk->t);
-    CnOld cn;
-    cn.t_old = __ldcg(&A.clk->t_old);
-    cn.dtlin_old = __ldcg(&A.clk->dtlin_old);
-    cn.old_init = __ldcg(&A.clk->old_init);
-    const double t_new = __dadd_rn(tclock, P.dt);
-    const bool last = S.last != 0;
-    bool diag_due = false;
-    if (last && P.tv_interval > 0.0) {
-        const double tv = __dadd_rn(__ldcg(&A.clk->timevar), P.dt);
-        diag_due = __dsub_rn(tv, P.tv_interval) > -1e-8;
+    if (tid == 0) {
+        const double tc = __ldcg(&A.clk->t);
+        hd.tclock = tc;
+        hd.cn_t_old = __ldcg(&A.clk->t_old);
+        hd.cn_dtlin_old = __ldcg(&A.clk->dtlin_old);
+        hd.cn_old_init = __ldcg(&A.clk->old_init);
+        const double tn = __dadd_rn(tc, P.dt);
+        hd.t_new = tn;
+        int dd = 0;
+        if (S.last && P.tv_interval > 0.0) {
+            const double tv = __dadd_rn(__ldcg(&A.clk->timevar), P.dt);
+            dd = __dsub_rn(tv, P.tv_interval) > -1e-8;
+        }
+        hd.diag_due = dd;
+        hd.qt = __dmul_rn(P.q, tn);
+        hd.ts = __dadd_rn(tc, S.t_off);
+        hd.Om2 = __dmul_rn(2.0, P.Omega);
+        hd.has_prev = (S.has_prev && A.Fprev) ? 1 : 0;
     }
-    const double qt = __dmul_rn(P.q, t_new);
-    const double ts = __dadd_rn(tclock, S.t_off);
-    const double fac = P.fac;
-    const double Om2 = __dmul_rn(2.0, P.Omega);
-    const bool has_prev = S.has_prev && A.Fprev;
+    __syncthreads();
+    // read from shared memory where used, so that they do not hold registers across the mode loop
+    const double& tclock = hd.tclock;
+    const double& t_new = hd.t_new;
+    const double& qt = hd.qt;
+    const double& ts = hd.ts;
+    const double& Om2 = hd.Om2;
+    const double& fac = P.fac;
+    const bool last = S.last != 0;
+    const bool diag_due = hd.diag_due != 0;
+    const bool has_prev = hd.has_prev != 0;
     const double* By = prof;
     const double* dBy = prof + NZ;
     const double* ddBy = prof + 2 * NZ;
@@ -476,8 +492,8 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
             em_u = exp(S.linC * P.nu * hxy);
             em_b = exp(S.linC * P.cb * hxy);
         } else {
-            if (cn.old_init) kxo = kx_at(kx0, P.q, tclock, ky);
-            else kxo = __dadd_rn(kx_at(kx0, P.q, cn.t_old, ky), __dmul_rn(__dmul_rn(P.q, cn.dtlin_old), ky));
+            if (hd.cn_old_init) kxo = kx_at(kx0, P.q, tclock, ky);
+            else kxo = __dadd_rn(kx_at(kx0, P.q, hd.cn_t_old, ky), __dmul_rn(__dmul_rn(P.q, hd.cn_dtlin_old), ky));
         }
         // remap after the step (main.cpp:122-123, MHD_BQlin.cpp:319-329): the mode's new
         // state is zero and kx0 moves by one box wavenumber period
@@ -526,8 +542,8 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
                 const double kz2 = kz2val(kzc[k]);
                 const bool z0 = (kyi == 0 && sx == 0);
                 const double L = linop_f<MODEL_BQLIN>(P, lap_end<MODEL_BQLIN>(P, kxe, ky, kz2), f);
-                const double lo = cn.old_init ? lap_init<MODEL_BQLIN>(P, kxo, lap2val(ky, kz2, z0))
-                                              : lap_end<MODEL_BQLIN>(P, kxo, ky, kz2);
+                const double lo = hd.cn_old_init ? lap_init<MODEL_BQLIN>(P, kxo, lap2val(ky, kz2, z0))
+                                                 : lap_end<MODEL_BQLIN>(P, kxo, ky, kz2);
                 nv = rk_update<INTEG_CN>(S, L, linop_f<MODEL_BQLIN>(P, lo, f), F[rr], fp, uin, fpm != nullptr);
             }
             if (fo) stc(fo + f * nzd + sx, F[rr]);

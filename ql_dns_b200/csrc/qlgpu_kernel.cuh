@@ -404,6 +404,11 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
         if (A.rec_kx)
             for (int i = threadIdx.x; i < P.nxy; i += blockDim.x) A.rec_kx[i] = __ldcg(A.kx0 + i);
         if (A.rec_t && threadIdx.x == 0) A.rec_t[0] = __ldcg(&A.clk->t);
+        if (A.rec_cn && threadIdx.x == 0) {
+            A.rec_cn->t_old = __ldcg(&A.clk->t_old);
+            A.rec_cn->dtlin_old = __ldcg(&A.clk->dtlin_old);
+            A.rec_cn->old_init = __ldcg(&A.clk->old_init);
+        }
     }
     // ---- mode loop: one mode per pair of groups, warp-uniform trip count (TMEM access is warp-wide)
     constexpr int PW = SW / 2;  // pairs per warp

@@ -48,6 +48,13 @@ struct DevClock {
     unsigned cnt_group[64];
 };
 
+// The Crank-Nicolson old-operator fields of a DevClock at a stage's start (the
+// record the adjoint of RK3CN reads): the same byte layout as DevClock from t_old.
+struct CnRec {
+    double t_old, dtlin_old;
+    int old_init, pad;
+};
+
 // Coefficients of one stage (RK3CN_Elin.cpp:89-91,122-125,155-158;
 // RK3CN.cpp:92-94,...).
 struct StageConst {
@@ -91,6 +98,7 @@ struct StageArgs {
     cplx* rec_mf;
     double* rec_kx;
     double* rec_t;
+    CnRec* rec_cn;          // the CN old-operator fields at the stage start (null: off)
     StageConst sc;
 };
 
@@ -112,6 +120,7 @@ struct BatchCase {
     cplx* rec_mf;
     double* rec_kx;
     double* rec_t;
+    CnRec* rec_cn;   // [3 n + s]
 };
 
 // One work item: CTA number `cta` of the `ncta` CTAs that step case `c`.

@@ -1,6 +1,6 @@
-"""Discrete adjoint of the MHD_BQlin / RK3CN_Elin step on the GPU
-(qlgpu_adjoint_maxwell) against the oracle's tangent-linear model and central
-finite differences of the GPU forward run.
+"""Discrete adjoint of the MHD_BQlin step with RK3CN_Elin and with RK3CN
+(Crank-Nicolson) on the GPU (qlgpu_adjoint_maxwell) against the oracle's
+tangent-linear model and central finite differences of the GPU forward run.
 
 J = mean over N steps of the fluctuation Maxwell stress.  Bars: the adjoint
 directional derivative Re <grad, d> agrees with the tangent-linear dJ to 1e-8
@@ -36,10 +36,10 @@ def gpu_J(p, lin, mf, kx0, n):
     return d[:, 8].mean()
 
 
-@pytest.mark.parametrize("NZ", [16, 32, 64, 128])
-def test_adjoint_matches_tangent_linear(NZ):
+@pytest.mark.parametrize("integ,NZ", [(0, 16), (0, 32), (0, 64), (0, 128), (1, 16), (1, 32), (1, 64), (1, 128)])
+def test_adjoint_matches_tangent_linear(integ, NZ):
     require_gpu()
-    p = mri_16x16_nz32(nx=8, ny=8, NZ=NZ)
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=NZ, integrator=integ)
     lin, mf, kx0 = initial_state(p, 7, sigma=0.2)
     n = 24
     with QLSolver(p) as s:
@@ -61,10 +61,11 @@ def test_adjoint_matches_tangent_linear(NZ):
     assert abs(float(np.real(np.vdot(gm, dm))) - dJm) <= 1e-8 * abs(dJm)
 
 
-def test_adjoint_through_remaps_vs_tangent_linear():
+@pytest.mark.parametrize("integ", [0, 1])
+def test_adjoint_through_remaps_vs_tangent_linear(integ):
     # high-ky modes shear past the remap threshold during the run
     require_gpu()
-    p = QLParams(nx=8, ny=12, NZ=32, dt=0.02)
+    p = QLParams(nx=8, ny=12, NZ=32, dt=0.02, integrator=integ)
     lin, mf, kx0 = initial_state(p, 11, sigma=0.3)
     n = 60
     t, lo, mo, ko, _ = O.run(p, 0.0, lin, mf, kx0, n)
@@ -76,9 +77,10 @@ def test_adjoint_through_remaps_vs_tangent_linear():
         assert abs(float(np.real(np.vdot(g, d))) - dJ) <= 1e-8 * abs(dJ)
 
 
-def test_adjoint_matches_central_differences():
+@pytest.mark.parametrize("integ", [0, 1])
+def test_adjoint_matches_central_differences(integ):
     require_gpu()
-    p = mri_16x16_nz32(nx=16, ny=16, NZ=32)
+    p = mri_16x16_nz32(nx=16, ny=16, NZ=32, integrator=integ)
     lin, mf, kx0 = initial_state(p, 3, sigma=0.05)
     n = 40
     with QLSolver(p) as s:
@@ -247,3 +249,25 @@ def test_seeds_with_different_parameters_reverse_per_seed():
         with QLSolver(pk) as s:
             J1, g1, m1 = s.adjoint_maxwell(0.0, *sts[k], 12, 4)
         assert abs(J[k] - J1) <= 1e-12 * abs(J1) and rel(gl[k], g1) < 1e-10 and rel(gm[k], m1) < 1e-10
+
+
+def test_crank_nicolson_batch_of_seeds_against_tangent_linear():
+    # RK3CN through the persistent path: the window recompute records every stage's
+    # old-operator clock fields, which the stage adjoint of the seeds' reverse sweep reads
+    require_gpu()
+    p = mri_16x16_nz32(nx=8, ny=8, NZ=64, integrator=1)
+    sts = [initial_state(p, 60 + k, sigma=0.2) for k in range(2)]
+    n, ck = 17, 5
+    solvers = [QLSolver(p) for _ in sts]
+    try:
+        J, gl, gm = QLSolver.adjoint_maxwell_batch(solvers, 0.0, [s[0] for s in sts], [s[1] for s in sts],
+                                                   [s[2] for s in sts], n, ck)
+    finally:
+        for s_ in solvers:
+            s_.close()
+    for k in range(2):
+        Jo, _ = O.tlm_maxwell(p, 0.0, *sts[k], np.zeros_like(sts[k][0]), None, n)
+        assert abs(J[k] - Jo) <= 1e-10 * abs(Jo)
+        for d in directions(sts[k][0].shape, 2, 70 + k, np.linalg.norm(sts[k][0])):
+            _, dJ = O.tlm_maxwell(p, 0.0, *sts[k], d, None, n)
+            assert abs(float(np.real(np.vdot(gl[k], d))) - dJ) <= 1e-8 * abs(dJ)
