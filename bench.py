@@ -131,14 +131,44 @@ def read_traffic(name: str):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed region: NVML read
+    every ~2 ms in a thread (read-only queries), else nvidia-smi every 200 ms."""
+
+    HW_SLOWDOWN, SW_POWER_CAP, SW_THERMAL, HW_THERMAL = 0x8, 0x4, 0x20, 0x40
 
     def __init__(self, index: int):
-        self.index = index
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        self.index = int(ids[index]) if index < len(ids) and ids[index].isdigit() else index
+        self.samples = []  # (sm_mhz, max_mhz, reasons bitmask)
         self.proc = None
-        self.lines = []
+        self.nvml = None
+        self.stop = threading.Event()
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def loop():
+                while not self.stop.is_set():
+                    try:
+                        self.samples.append((float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)),
+                                             float(smax), int(get_reasons(h))))
+                    except Exception:
+                        pass
+                    time.sleep(0.002)
+
+            self.nvml = pynvml
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -146,43 +176,44 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread = threading.Thread(target=self._read_smi, daemon=True)
             self.thread.start()
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _read_smi(self):
+        names = [self.HW_SLOWDOWN, self.HW_THERMAL, self.SW_THERMAL, self.SW_POWER_CAP]
+        for ln in self.proc.stdout:
+            f = [x.strip() for x in ln.strip().split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                bits = sum(b for b, v in zip(names, f[5:9]) if v.lower().startswith("active"))
+                self.samples.append((float(f[1]), float(f[2]), bits))
+            except ValueError:
+                continue
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        elif self.nvml:
+            self.thread.join(timeout=1)
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        names = {self.HW_SLOWDOWN: "hw_slowdown", self.HW_THERMAL: "hw_thermal_slowdown",
+                 self.SW_THERMAL: "sw_thermal_slowdown", self.SW_POWER_CAP: "sw_power_cap"}
+        reasons = sorted({n for b, n in names.items() for s in self.samples if s[2] & b})
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples), "sm_max_mhz": self.samples[-1][1],
+                "reasons": reasons, "samples": len(self.samples),
+                "source": "NVML, ~2 ms period" if self.nvml else "nvidia-smi, 200 ms period"}
 
 
 def dist_setup(backend: str = "nccl", timeout_s: float = 120.0):
@@ -488,39 +519,62 @@ def run_gpu(args):
     # host memory, then per step one call that advances all cases and reads the
     # 48 diagnostic records (energy / stress / dissipation) back to the host,
     # then D2H of every case's state
-    pinned = []
+    def pinned_like(a):
+        return torch.empty(a.shape, dtype=torch.float64 if a.dtype == np.float64 else torch.complex128,
+                           pin_memory=True).numpy()
+
+    pin_in, pin_out = [], []
     for lin, mf, kx0 in sts:
-        lh = torch.empty(lin.shape, dtype=torch.complex128, pin_memory=True).numpy()
-        mh = torch.empty(mf.shape, dtype=torch.complex128, pin_memory=True).numpy()
-        lh[...] = lin
-        mh[...] = mf
-        pinned.append((lh, mh, kx0))
+        lh, mh, kh = pinned_like(lin), pinned_like(mf), pinned_like(kx0)
+        lh[...], mh[...], kh[...] = lin, mf, kx0
+        pin_in.append((lh, mh, kh))
+        pin_out.append((pinned_like(lin), pinned_like(mf), pinned_like(kx0)))
     ext = torch.cuda.ExternalStream(batch.stream())
-    torch.cuda.synchronize()
-    barrier(ws)
-    ee0 = torch.cuda.Event(enable_timing=True)
-    ee1 = torch.cuda.Event(enable_timing=True)
-    ee0.record(ext)
-    for c, (lh, mh, kx0) in enumerate(pinned):
-        batch.set_state(c, 0.0, lh, mh, kx0)
-    ndiag = 0
-    recs_all = [[] for _ in range(NCASES)]
-    for _ in range(args.steps):
-        recs = batch.step(1, diag_every=1)
-        ndiag += sum(len(r) for r in recs)
-        for c, r in enumerate(recs):
-            recs_all[c].append(r)
-    outs = [batch.get_state(c) for c in range(NCASES)]
-    ee1.record(ext)
-    ee1.synchronize()
-    e2e_ms = max_over_ranks(ws, ee0.elapsed_time(ee1))
-    assert ndiag == NCASES * args.steps
-    assert all(np.isfinite(o[1]).all() and np.isfinite(o[2]).all() for o in outs)
+
+    def e2e_run(per_step: bool):
+        """State of all cases in from pinned host memory, K steps with the energy / stress /
+        dissipation record of every step read back, state of all cases out."""
+        torch.cuda.synchronize()
+        barrier(ws)
+        ee0 = torch.cuda.Event(enable_timing=True)
+        ee1 = torch.cuda.Event(enable_timing=True)
+        ee0.record(ext)
+        h0 = time.perf_counter()
+        batch.set_states(0.0, pin_in)
+        h1 = time.perf_counter()
+        recs_all = [[] for _ in range(NCASES)]
+        if per_step:
+            for _ in range(args.steps):
+                for c, r in enumerate(batch.step(1, diag_every=1)):
+                    recs_all[c].append(r)
+        else:
+            for c, r in enumerate(batch.step(args.steps, diag_every=1)):
+                recs_all[c].append(r)
+        h2 = time.perf_counter()
+        outs = batch.get_states(pin_out)
+        ee1.record(ext)
+        ee1.synchronize()
+        h3 = time.perf_counter()
+        ms = max_over_ranks(ws, ee0.elapsed_time(ee1))
+        assert sum(len(r) for rr in recs_all for r in rr) == NCASES * args.steps
+        assert all(np.isfinite(o[1]).all() and np.isfinite(o[2]).all() for o in outs)
+        outs = [(o[0], o[1].copy(), o[2].copy(), o[3].copy()) for o in outs]
+        return ms, recs_all, outs, {"set_states_ms": 1e3 * (h1 - h0), "steps_ms": 1e3 * (h2 - h1),
+                                    "get_states_ms": 1e3 * (h3 - h2)}
+
+    e2e_run(True)  # warm-up of the one-step graph
+    e2e_ms, recs_all, outs, phases = e2e_run(True)
+    one_ms, _, _, one_phases = e2e_run(False)
     state_bytes = sum(lin.nbytes + mf.nbytes + kx0.nbytes for lin, mf, kx0 in sts)
     e2e = {"value": job_modes * args.steps / (e2e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": state_bytes / args.steps,
            "d2h_bytes_per_step": NCASES * 15 * 8 + state_bytes / args.steps,
-           "path": "QLBatch.set_state (pinned) x48, K x QLBatch.step(1, diag_every=1), QLBatch.get_state x48"}
+           "path": "QLBatch.set_states (pinned, all 48 cases), K x QLBatch.step(1, diag_every=1) (one launch and "
+                   "the 48 records read back per step), QLBatch.get_states (pinned)",
+           "phases_host_ms": phases,
+           "one_call": {"value": job_modes * args.steps / (one_ms / 1e3), "unit": UNIT,
+                        "path": "as above with one QLBatch.step(K, diag_every=1): one launch, every step's 48 "
+                                "records read back after it", "phases_host_ms": one_phases}}
     batch.close()
 
     parity = ensemble_parity(cases, sts, recs_all, outs, timed_out, args) if rank == 0 else None

@@ -236,6 +236,13 @@ int qlgpu_batch_dims(const qlgpu_batch_t* b, int c, int* nxy, int* nz, int* nmf)
 int qlgpu_batch_set_state(qlgpu_batch_t* b, int c, double t, const double* lin, const double* mf, const double* kx0);
 int qlgpu_batch_get_state(qlgpu_batch_t* b, int c, double* t, double* lin, double* mf, double* kx0);
 
+/* Every case at once, one synchronisation: lin[c], mf[c] (and kx0[c], which
+ * may be NULL, as may kx0 itself) are case c's host buffers, pinned for
+ * asynchronous copies; get: t[ncases] (may be NULL) and any non-NULL buffer. */
+int qlgpu_batch_set_states(qlgpu_batch_t* b, double t, const double* const* lin, const double* const* mf,
+                           const double* const* kx0);
+int qlgpu_batch_get_states(qlgpu_batch_t* b, double* t, double* const* lin, double* const* mf, double* const* kx0);
+
 /* Initial diagnostic record of case c (15 doubles, as qlgpu_diagnostics). */
 int qlgpu_batch_diagnostics(qlgpu_batch_t* b, int c, double* out15);
 
@@ -307,6 +314,8 @@ int qlgpu_batch_engine(const qlgpu_batch_t* b, int* engine);
  * queue engine.  qlgpu_batch_tune searches these when the queue engine is
  * active. */
 int qlgpu_batch_set_chunks(qlgpu_batch_t* b, const int* passes4);
+/* The current passes per chunk of the four NZ classes (after qlgpu_batch_tune: the tuned ones). */
+int qlgpu_batch_chunks(const qlgpu_batch_t* b, int* passes4);
 
 /* Profiling aid of the queue engine (QLGPU_TRACE=1 in the environment at
  * qlgpu_batch_create): per CTA of the last launch, averaged over CTAs, out4 =

@@ -31,6 +31,7 @@ EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "ql
            "qlgpu_batch_set_wait", "qlgpu_batch_debug_drop_item", "qlgpu_batch_stream",
            "qlgpu_batch_last_error", "qlgpu_batch_set_engine", "qlgpu_batch_engine", "qlgpu_batch_set_chunks",
            "qlgpu_batch_queue_trace",
+           "qlgpu_batch_set_states", "qlgpu_batch_get_states", "qlgpu_batch_chunks",
            "qlgpu_timevars_open", "qlgpu_timevars_save_data", "qlgpu_timevars_save_mean_fields",
            "qlgpu_timevars_close", "qlgpu_fullsave_write", "qlgpu_fullsave_read_latest", "qlgpu_fullsave_times",
            "qlgpu_io_last_error",
@@ -127,7 +128,11 @@ def load(path: str = LIB_PATH):
     L.qlgpu_batch_set_engine.argtypes = [vp, ctypes.c_int]
     L.qlgpu_batch_engine.argtypes = [vp, ip]
     L.qlgpu_batch_set_chunks.argtypes = [vp, ip]
+    L.qlgpu_batch_chunks.argtypes = [vp, ip]
     L.qlgpu_batch_queue_trace.argtypes = [vp, dp]
+    dpp = ctypes.POINTER(dp)
+    L.qlgpu_batch_set_states.argtypes = [vp, ctypes.c_double, dpp, dpp, dpp]
+    L.qlgpu_batch_get_states.argtypes = [vp, dp, dpp, dpp, dpp]
     L.qlgpu_timevars_open.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       ctypes.POINTER(vp)]
     L.qlgpu_timevars_save_data.argtypes = [vp, dp]

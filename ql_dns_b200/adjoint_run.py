@@ -1,13 +1,17 @@
 """Adjoint run of the QL MRI at 32x32 modes x NZ=64 (Re=Rm=4000, dt=0.01).
 
     python -m ql_dns_b200.adjoint_run [--seeds 16] [--steps 2000] [--checkpoint 100] [--fd-dirs 8] [--reps 2]
+                                      [--integrator 0|1]
 
 All seeds run together: J = the fluctuation Maxwell stress averaged over the
 steps and dJ/d lin0 come from one qlgpu_adjoint_maxwell_batch call (one handle
 and stream per seed, checkpoints every --checkpoint steps, stages recomputed
 per window).  The forward cost it is compared with is the same seeds' forward
 run with a record every step through the batched ensemble (one persistent
-launch for all seeds, QLBatch).  Gradients are checked along --fd-dirs random
+launch for all seeds, QLBatch), with the batch's default engine (the chunk
+queue, which the adjoint's forward sweep also uses) and with the work-item
+engine (which its window recompute uses: that engine records the stage inputs).
+--integrator 1 runs RK3CN (Crank-Nicolson) instead of RK3CN_Elin.  Gradients are checked along --fd-dirs random
 directions per seed (scaled to |lin0|, so eps is a relative perturbation)
 against central finite differences of the batched forward run with step eps
 and eps/2.  Per direction: the relative error |adj - fd| / |fd| and the error
@@ -45,11 +49,13 @@ def main(argv=None):
     ap.add_argument("--fd-dirs", type=int, default=8)
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--reps", type=int, default=2, help="timed repetitions; the minimum is reported")
+    ap.add_argument("--integrator", type=int, default=0, choices=[0, 1])
     a = ap.parse_args(argv)
-    p = adjoint_32x32_nz64()
+    p = adjoint_32x32_nz64(integrator=a.integrator)
     S = a.seeds
     states = [initial_state(p, seed, sigma=1e-3) for seed in range(S)]
-    out = {"workload": f"MHD_BQlin + RK3CN_Elin, {p.nx}x{p.ny} modes x NZ={p.NZ}, Re=Rm={1 / p.nu:.0f}, "
+    integ = "RK3CN_Elin" if a.integrator == 0 else "RK3CN"
+    out = {"workload": f"MHD_BQlin + {integ}, {p.nx}x{p.ny} modes x NZ={p.NZ}, Re=Rm={1 / p.nu:.0f}, "
                        f"dt={p.dt}, {a.steps} steps, checkpoint every {a.checkpoint}, {S} seeds together",
            "eps": a.eps}
     with QLBatch([p] * S) as b:
@@ -60,6 +66,16 @@ def main(argv=None):
             Jf = batch_J(b, states, a.steps)
             t_fwds.append(time.perf_counter() - t0)
         t_fwd = min(t_fwds)
+        engine = b.engine()
+        b.set_engine("items")
+        batch_J(b, states, 3)
+        t_items = []
+        for _ in range(a.reps):
+            t0 = time.perf_counter()
+            batch_J(b, states, a.steps)
+            t_items.append(time.perf_counter() - t0)
+        t_fwd_items = min(t_items)
+        b.set_engine("auto")
         solvers = [QLSolver(p) for _ in range(S)]
         try:
             QLSolver.adjoint_maxwell_batch(solvers, 0.0, [s[0] for s in states], [s[1] for s in states],
@@ -103,7 +119,8 @@ def main(argv=None):
                 "J_rel_diff_max": float(np.max(np.abs(Ja - Jf) / np.abs(Jf))),
                 "forward_batch_s": t_fwd, "adjoint_batch_s": t_adj,
                 "forward_batch_s_all": t_fwds, "adjoint_batch_s_all": t_adjs,
-                "adjoint_over_forward": t_adj / t_fwd,
+                "adjoint_over_forward": t_adj / t_fwd, "forward_engine": engine,
+                "forward_batch_items_s": t_fwd_items, "adjoint_over_forward_items": t_adj / t_fwd_items,
                 "single_seed": {"forward_s": t_fwd1, "adjoint_s": t_adj1, "adjoint_over_forward": t_adj1 / t_fwd1},
                 "batch_speedup_vs_sequential_adjoint": S * t_adj1 / t_adj})
     if dirs:

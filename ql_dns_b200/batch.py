@@ -75,6 +75,41 @@ class QLBatch:
                                                        _capi.dptr(kx0)), self.b)
         return t.value, lin, mf, kx0
 
+    def set_states(self, t: float, states):
+        """Every case's (lin, mf, kx0) at once (kx0 may be None); one synchronisation.  Pinned
+        host arrays (e.g. from torch pin_memory) copy asynchronously."""
+        nc = len(self.cases)
+        arrs = []
+        P = ctypes.POINTER(ctypes.c_double)
+        lp, mp, kp = (P * nc)(), (P * nc)(), (P * nc)()
+        for c, (lin, mf, kx0) in enumerate(states):
+            nxy, nz, nmf = self.dims[c]
+            lin = np.ascontiguousarray(lin, dtype=np.complex128)
+            mf = np.ascontiguousarray(mf, dtype=np.complex128)
+            assert lin.shape == (nxy, 4, nz) and mf.shape == (nmf, nz)
+            arrs += [lin, mf]
+            lp[c], mp[c] = _capi.dptr(lin), _capi.dptr(mf)
+            if kx0 is not None:
+                kx0 = np.ascontiguousarray(kx0, dtype=np.float64)
+                arrs.append(kx0)
+                kp[c] = _capi.dptr(kx0)
+        _capi.check_batch(self.L.qlgpu_batch_set_states(self.b, float(t), lp, mp, kp), self.b)
+
+    def get_states(self, out=None):
+        """Every case's (t, lin, mf, kx0); `out` = per-case (lin, mf, kx0) host arrays to fill
+        (pinned for asynchronous copies), else new arrays."""
+        nc = len(self.cases)
+        if out is None:
+            out = [(np.empty((d[0], 4, d[1]), dtype=np.complex128), np.empty((d[2], d[1]), dtype=np.complex128),
+                    np.empty(d[0])) for d in self.dims]
+        P = ctypes.POINTER(ctypes.c_double)
+        lp, mp, kp = (P * nc)(), (P * nc)(), (P * nc)()
+        for c, (lin, mf, kx0) in enumerate(out):
+            lp[c], mp[c], kp[c] = _capi.dptr(lin), _capi.dptr(mf), _capi.dptr(kx0)
+        t = np.zeros(nc)
+        _capi.check_batch(self.L.qlgpu_batch_get_states(self.b, _capi.dptr(t), lp, mp, kp), self.b)
+        return [(t[c], lin, mf, kx0) for c, (lin, mf, kx0) in enumerate(out)]
+
     def diagnostics(self, c: int) -> np.ndarray:
         out = np.zeros(15)
         _capi.check_batch(self.L.qlgpu_batch_diagnostics(self.b, c, _capi.dptr(out)), self.b)
@@ -106,11 +141,18 @@ class QLBatch:
         return best.value
 
     def mapping(self) -> dict:
+        """CTA width, grid, CTAs per SM, shared memory and per case its CTAs (work-item engine) or
+        chunks per stage (queue engine, with the passes per chunk of NZ = 16, 32, 64, 128)."""
         info = (ctypes.c_int * 4)()
         nc = len(self.cases)
         k = (ctypes.c_int * nc)()
         _capi.check_batch(self.L.qlgpu_batch_mapping(self.b, info, k), self.b)
-        return {"warps": info[0], "grid": info[1], "ctas_per_sm": info[2], "smem": info[3], "ncta": list(k)}
+        out = {"warps": info[0], "grid": info[1], "ctas_per_sm": info[2], "smem": info[3], "ncta": list(k)}
+        if self.engine() == "queue":
+            p4 = (ctypes.c_int * 4)()
+            _capi.check_batch(self.L.qlgpu_batch_chunks(self.b, p4), self.b)
+            out["chunk_passes"] = dict(zip([16, 32, 64, 128], list(p4)))
+        return out
 
     def cost_model(self) -> dict:
         """The planner's cost model (fitted by tune()): alpha = us per stage per launch,

@@ -70,7 +70,7 @@ struct CaseHost {
     cplx* lin[2] = {nullptr, nullptr};
     cplx *F1 = nullptr, *F2 = nullptr, *mf = nullptr, *Fmf1 = nullptr, *Fmf2 = nullptr, *tw = nullptr;
     double *kx0 = nullptr, *ky = nullptr, *il2 = nullptr, *partials = nullptr, *gpartials = nullptr;
-    double *mfr = nullptr, *ekz = nullptr;
+    double *mfr = nullptr, *ekz = nullptr, *kx_init = nullptr;
     int *kxi = nullptr, *kyi = nullptr;
     DevClock* clk = nullptr;
     double* diag = nullptr;
@@ -135,6 +135,31 @@ __global__ void batch_collect_kernel(const BatchCase* cases, int ncases, const B
     }
 }
 
+// set_states: case c's clock starts at t (reset_case_clock for every case at once) and,
+// where kx_default[c], its kx0 is the unsheared table.  One block per case.
+__global__ void batch_set_clocks_kernel(const BatchCase* cases, int ncases, double t, const int* kx_default) {
+    const int c = blockIdx.x;
+    if (c >= ncases) return;
+    DevClock* k = cases[c].A[0].clk;
+    unsigned* w = reinterpret_cast<unsigned*>(k);
+    for (int i = threadIdx.x; i < (int)(sizeof(DevClock) / sizeof(unsigned)); i += blockDim.x) w[i] = 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        k->t = t;
+        k->old_init = 1;
+    }
+    if (kx_default[c]) {
+        const int nxy = cases[c].P.nxy;
+        for (int i = threadIdx.x; i < nxy; i += blockDim.x) cases[c].A[0].kx0[i] = cases[c].kx_init[i];
+    }
+}
+
+// get_states: every case's clock time into one array.
+__global__ void batch_gather_t_kernel(const BatchCase* cases, int ncases, double* out) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncases; c += gridDim.x * blockDim.x)
+        out[c] = cases[c].A[0].clk->t;
+}
+
 }  // namespace
 
 struct qlgpu_batch {
@@ -184,6 +209,8 @@ struct qlgpu_batch {
     int drop_case = -1;                  // failure-detection aid: a chunk of this case is left out
     bool qdirty = true;
     unsigned long long* d_qtrace = nullptr;  // [grid][4] per-CTA time sums of the last queue launch (QLGPU_TRACE=1)
+    int* d_flags = nullptr;                  // [ncases] per-case flags of set_states
+    double* d_tvec = nullptr;                // [ncases] clock times of get_states
 };
 
 namespace {
@@ -356,6 +383,7 @@ int upload_descriptors(qlgpu_batch_t* b) {
             A.ekz_tab = h.ekz + (size_t)s * 2 * h.nz;
             A.sc = h.sc[s];
         }
+        d.kx_init = h.kx_init;
         d.rec_lin = h.rec_lin;
         d.rec_mf = h.rec_mf;
         d.rec_kx = h.rec_kx;
@@ -629,7 +657,7 @@ int qlgpu_batch_destroy(qlgpu_batch_t* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
     void* bufs[] = {b->arena,   b->d_cases, b->d_ctas, b->d_epoch, b->d_ctl, b->d_case_end, b->d_collect,
-                    b->d_out15, b->d_diag,  b->d_ec,   b->d_round, b->d_tw8, b->d_qtrace};
+                    b->d_out15, b->d_diag,  b->d_ec,   b->d_round, b->d_tw8, b->d_qtrace, b->d_flags, b->d_tvec};
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : b->ev)
@@ -720,7 +748,7 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
         off[c] = o;
         o += 4 * al256(nlin * sizeof(cplx));                       // lin[2], F1, F2
         o += 3 * al256(nmfe * sizeof(cplx));                       // mf, Fmf1, Fmf2
-        o += 2 * al256(h.nxy * sizeof(double));                    // kx0, ky
+        o += 3 * al256(h.nxy * sizeof(double));                    // kx0, ky, kx_init
         o += 2 * al256(h.nxy * sizeof(int));                       // kxi, kyi
         o += al256(h.NZ * sizeof(cplx));                           // twiddles
         o += al256((size_t)(h.p.ny / 2) * h.nz * sizeof(double));  // 1/lap2
@@ -753,6 +781,7 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
         h.Fmf1 = reinterpret_cast<cplx*>(take(nmfe * sizeof(cplx)));
         h.Fmf2 = reinterpret_cast<cplx*>(take(nmfe * sizeof(cplx)));
         h.kx0 = reinterpret_cast<double*>(take(h.nxy * sizeof(double)));
+        h.kx_init = reinterpret_cast<double*>(take(h.nxy * sizeof(double)));
         h.ky = reinterpret_cast<double*>(take(h.nxy * sizeof(double)));
         h.kxi = reinterpret_cast<int*>(take(h.nxy * sizeof(int)));
         h.kyi = reinterpret_cast<int*>(take(h.nxy * sizeof(int)));
@@ -772,6 +801,7 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
         const std::vector<double> il2 = ilap2_table(h.p, h.nz);
         const std::vector<double> ekz = ekz_table(h.p, h.dp);
         cudaMemcpyAsync(h.kx0, h.kx_tab.data(), h.nxy * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+        cudaMemcpyAsync(h.kx_init, h.kx_tab.data(), h.nxy * sizeof(double), cudaMemcpyHostToDevice, b->stream);
         cudaMemcpyAsync(h.ky, ky.data(), h.nxy * sizeof(double), cudaMemcpyHostToDevice, b->stream);
         cudaMemcpyAsync(h.kxi, kxi.data(), h.nxy * sizeof(int), cudaMemcpyHostToDevice, b->stream);
         cudaMemcpyAsync(h.kyi, kyi.data(), h.nxy * sizeof(int), cudaMemcpyHostToDevice, b->stream);
@@ -799,6 +829,8 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
     QB_ALLOC(b->d_collect, sizeof(int) * (2 * ncases + 2));
     QB_ALLOC(b->d_out15, sizeof(double) * 15);
     QB_ALLOC(b->d_ec, sizeof(ens::EnsCase) * ncases);
+    QB_ALLOC(b->d_flags, sizeof(int) * ncases);
+    QB_ALLOC(b->d_tvec, sizeof(double) * ncases);
     QB_ALLOC(b->d_tw8, sizeof(cplx) * 240);
 #undef QB_ALLOC
     {
@@ -891,6 +923,63 @@ int qlgpu_batch_get_state(qlgpu_batch_t* b, int c, double* t, double* lin, doubl
     QB_CK(cudaMemcpyAsync(&tt, &h.clk->t, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
     QB_CK(cudaStreamSynchronize(b->stream));
     if (t) *t = tt;
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_set_states(qlgpu_batch_t* b, double t, const double* const* lin, const double* const* mf,
+                           const double* const* kx0) {
+    if (!b || !lin || !mf) return QLGPU_ERR_ARG;
+    for (int c = 0; c < b->ncases; ++c)
+        if (!lin[c] || !mf[c]) return bfail(b, QLGPU_ERR_ARG, "null state of case " + std::to_string(c));
+    QB_CK(cudaSetDevice(b->device));
+    if (b->descr_dirty) {
+        int rc = upload_descriptors(b);
+        if (rc) return rc;
+    }
+    std::vector<int> dflt(b->ncases, 1);
+    for (int c = 0; c < b->ncases; ++c) {
+        CaseHost& h = b->cs[c];
+        const size_t nlin = (size_t)h.nxy * 4 * h.nz, nmfe = (size_t)h.nmf * h.nz;
+        QB_CK(cudaMemcpyAsync(h.lin[b->cur], lin[c], nlin * sizeof(cplx), cudaMemcpyHostToDevice, b->stream));
+        QB_CK(cudaMemcpyAsync(h.mf, mf[c], nmfe * sizeof(cplx), cudaMemcpyHostToDevice, b->stream));
+        if (kx0 && kx0[c]) {
+            dflt[c] = 0;
+            QB_CK(cudaMemcpyAsync(h.kx0, kx0[c], h.nxy * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+        }
+    }
+    // the clocks (and the default kx0) of every case in one launch, after the copies above
+    QB_CK(cudaMemcpyAsync(b->d_flags, dflt.data(), sizeof(int) * b->ncases, cudaMemcpyHostToDevice, b->stream));
+    batch_set_clocks_kernel<<<b->ncases, 128, 0, b->stream>>>(b->d_cases, b->ncases, t, b->d_flags);
+    QB_CK(cudaGetLastError());
+    QB_CK(cudaStreamSynchronize(b->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_get_states(qlgpu_batch_t* b, double* t, double* const* lin, double* const* mf, double* const* kx0) {
+    if (!b) return QLGPU_ERR_ARG;
+    QB_CK(cudaSetDevice(b->device));
+    if (b->descr_dirty) {
+        int rc = upload_descriptors(b);
+        if (rc) return rc;
+    }
+    for (int c = 0; c < b->ncases; ++c) {
+        CaseHost& h = b->cs[c];
+        const size_t nlin = (size_t)h.nxy * 4 * h.nz, nmfe = (size_t)h.nmf * h.nz;
+        if (lin && lin[c])
+            QB_CK(cudaMemcpyAsync(lin[c], h.lin[b->cur], nlin * sizeof(cplx), cudaMemcpyDeviceToHost, b->stream));
+        if (mf && mf[c]) QB_CK(cudaMemcpyAsync(mf[c], h.mf, nmfe * sizeof(cplx), cudaMemcpyDeviceToHost, b->stream));
+        if (kx0 && kx0[c])
+            QB_CK(cudaMemcpyAsync(kx0[c], h.kx0, h.nxy * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    }
+    std::vector<double> tt(b->ncases, 0.0);
+    if (t) {
+        batch_gather_t_kernel<<<1, 128, 0, b->stream>>>(b->d_cases, b->ncases, b->d_tvec);
+        QB_CK(cudaGetLastError());
+        QB_CK(cudaMemcpyAsync(tt.data(), b->d_tvec, sizeof(double) * b->ncases, cudaMemcpyDeviceToHost, b->stream));
+    }
+    QB_CK(cudaStreamSynchronize(b->stream));
+    if (t)
+        for (int c = 0; c < b->ncases; ++c) t[c] = tt[c];
     return QLGPU_OK;
 }
 
@@ -1348,6 +1437,12 @@ int qlgpu_batch_set_chunks(qlgpu_batch_t* b, const int* passes4) {
     b->qdirty = true;
     drop_graphs(b);
     return queue_plan(b);
+}
+
+int qlgpu_batch_chunks(const qlgpu_batch_t* b, int* passes4) {
+    if (!b || !passes4) return QLGPU_ERR_ARG;
+    for (int i = 0; i < 4; ++i) passes4[i] = b->qpasses[i];
+    return QLGPU_OK;
 }
 
 int qlgpu_batch_queue_trace(qlgpu_batch_t* b, double* out4) {

@@ -367,48 +367,51 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
     const int s = r % 3, n = r / 3;
     const int swap = (n + L.parity) & 1;
 
-    // ---- header and tables (skipped when this CTA ran the same case and stage last)
+    // ---- header (skipped when this CTA ran the same case and stage last)
     __syncthreads();
     const bool fresh = !(hd.ok && hd.c == c && hd.r == r);
     if (fresh) {
         cta_copy8(&hd.P, &cs->P, (int)sizeof(DevParams));
         cta_copy8(&hd.A, &cs->A[s], (int)sizeof(StageArgs));
-        __syncthreads();
-        if (tid == 0) {
-            if (swap) {
-                const cplx* in = hd.A.lin_in;
-                hd.A.lin_in = hd.A.lin_out;
-                hd.A.lin_out = const_cast<cplx*>(in);
-            }
-            hd.c = c;
-            hd.r = r;
-            hd.ok = 1;
-        }
-        for (int i = tid; i < NZ; i += THREADS) {
-            tw[i] = ldc(ec.tw8 + i);
-            const int kzi = i <= E::H ? i : i - NZ;
-            kzc[i] = kzval(kzi, hd.P.kzL);
-        }
-        if (INTEG == INTEG_EXP)
-            for (int i = tid; i < E::nz; i += THREADS) {
-                ekz[i] = __ldg(hd.A.ekz_tab + i);
-                ekz[E::NZE + i] = __ldg(hd.A.ekz_tab + E::nz + i);
-            }
-        __syncthreads();
-        const bool cached = __ldcg(&hd.A.clk->mfr_valid) != 0;
-        if (cached) {
-            for (int i = tid; i < 3 * NZ; i += THREADS) prof[i] = __ldcg(hd.A.mfr_cache + i);
-        } else {
-            // real-space By, dz By, dz^2 By of the stage input (MHD_BQlin.cpp:122-127)
-            profiles_of<NZ>(hd, prof, reinterpret_cast<cplx*>(smem_raw + E::o_warp));
-        }
-        __syncthreads();
     }
+    __syncthreads();
     const DevParams& P = hd.P;
     const StageArgs& A = hd.A;
     const StageConst& S = A.sc;
     const int nzd = E::nz;
+    // steps that start from buffer 1 read lin_out and write lin_in of the descriptor
+    const cplx* lin_in = swap ? A.lin_out : A.lin_in;
+    cplx* lin_out = const_cast<cplx*>(swap ? A.lin_in : A.lin_out);
+    // ---- the chunk's modes: pass p, pair (warp, pi) -> mode base + p W PPW + warp PPW + pi.  The
+    // first mode's staged copy and wavenumbers are requested before the tables are loaded.
+    const int mbeg = j * ec.mpc;
+    const int mend = min(P.nxy, mbeg + ec.mpc);
+    constexpr int MPP = WARPS * E::PPW;  // modes per pass
+    const int first = mbeg + warp * E::PPW;
+    const unsigned fbytes = 64u * (unsigned)nzd;
+    // the pair's barrier was initialised at kernel start; bar_ph holds the parity of its next phase
+    unsigned phase = bar_ph[warp * MAX_PAIRS_PER_WARP + pi];
+    // pair leader (role U, t = 0) issues the copies of its pair; every pair waits once per pass, so
+    // a pair past the chunk's end stages the chunk's last mode (finite values; its stores and sums
+    // are switched off)
+    const bool leader = (role == 0 && t == 0);
+    if (leader && first < mend) bulk_load(stg, lin_in + (size_t)min(first + pi, mend - 1) * 4 * nzd, fbytes, bar);
+    // the mode's wavenumbers are loaded one mode ahead (their latency overlaps the previous mode)
+    double nky = 0.0, nkx0 = 0.0;
+    int nkyi = 0, nkxi = 0;
+    if (first < mend) {
+        const int m0 = min(first + pi, mend - 1);
+        nky = __ldg(A.ky + m0);
+        nkx0 = __ldcg(A.kx0 + m0);
+        nkyi = __ldg(A.kyi + m0);
+        nkxi = __ldg(A.kxi + m0);
+    }
     if (tid == 0) {
+        if (fresh) {
+            hd.c = c;
+            hd.r = r;
+            hd.ok = 1;
+        }
         const double tc = __ldcg(&A.clk->t);
         hd.tclock = tc;
         hd.cn_t_old = __ldcg(&A.clk->t_old);
@@ -426,6 +429,29 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         hd.ts = __dadd_rn(tc, S.t_off);
         hd.Om2 = __dmul_rn(2.0, P.Omega);
         hd.has_prev = (S.has_prev && A.Fprev) ? 1 : 0;
+    }
+    // ---- tables of the case and stage
+    if (fresh) {
+        for (int i = tid; i < NZ; i += THREADS) {
+            tw[i] = ldc(ec.tw8 + i);
+            const int kzi = i <= E::H ? i : i - NZ;
+            kzc[i] = kzval(kzi, P.kzL);
+        }
+        if (INTEG == INTEG_EXP)
+            for (int i = tid; i < E::nz; i += THREADS) {
+                ekz[i] = __ldg(A.ekz_tab + i);
+                ekz[E::NZE + i] = __ldg(A.ekz_tab + E::nz + i);
+            }
+        const bool cached = __ldcg(&A.clk->mfr_valid) != 0;
+        if (cached) {
+            for (int i = tid; i < 3 * NZ; i += THREADS) prof[i] = __ldcg(A.mfr_cache + i);
+        } else {
+            // real-space By, dz By, dz^2 By of the stage input (MHD_BQlin.cpp:122-127); scratch:
+            // warp 0's exchange buffers and warp 1's K buffers, which no staged copy writes
+            __syncthreads();
+            profiles_of<NZ>(hd, prof,
+                            reinterpret_cast<cplx*>(smem_raw + E::o_warp) + E::K_CPLX + E::STG_CPLX);
+        }
     }
     __syncthreads();
     // read from shared memory where used, so that they do not hold registers across the mode loop
@@ -454,33 +480,28 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
     }
     double dacc[3] = {0.0, 0.0, 0.0};  // U: eb, AM_b, diss_b; B: eu, AM_u, diss_u
 
-    // ---- modes of the chunk: pass p, pair (warp, pi) -> mode base + p W PPW + warp PPW + pi
-    const int mbeg = j * ec.mpc;
-    const int mend = min(P.nxy, mbeg + ec.mpc);
-    constexpr int MPP = WARPS * E::PPW;  // modes per pass
-    const int first = mbeg + warp * E::PPW;
-    const unsigned fbytes = 64u * (unsigned)nzd;
-    // the pair's barrier was initialised at kernel start; bar_ph holds the parity of its next phase
-    unsigned phase = bar_ph[warp * MAX_PAIRS_PER_WARP + pi];
-    // pair leader (role U, t = 0) issues the copies of its pair
-    const bool leader = (role == 0 && t == 0);
-    // every pair waits once per pass, so a pair past the chunk's end stages the chunk's last
-    // mode (finite values; its stores and sums are switched off)
-    if (leader && first < mend) bulk_load(stg, A.lin_in + (size_t)min(first + pi, mend - 1) * 4 * nzd, fbytes, bar);
     int m;
     bool ok = true;
+    const int lp = role * T + t;  // lane within the pair
     for (int wb = first; wb < mend; wb += MPP) {  // warp-uniform
         const int mraw = wb + pi;
         const bool valid = mraw < mend;
         m = valid ? mraw : mend - 1;
         // L2 prefetch of the pair's next mode (fields and previous right-hand side)
         if (leader && mraw + MPP < mend) {
-            l2_prefetch(A.lin_in + (size_t)(mraw + MPP) * 4 * nzd, fbytes);
+            l2_prefetch(lin_in + (size_t)(mraw + MPP) * 4 * nzd, fbytes);
             if (has_prev) l2_prefetch(A.Fprev + (size_t)(mraw + MPP) * 4 * nzd, fbytes);
         }
-        const double ky = __ldg(A.ky + m);
-        double kx0 = __ldcg(A.kx0 + m);
-        const int kyi = __ldg(A.kyi + m), kxi = __ldg(A.kxi + m);
+        const double ky = nky;
+        double kx0 = nkx0;
+        const int kyi = nkyi, kxi = nkxi;
+        if (wb + MPP < mend) {
+            const int mn = min(wb + MPP + pi, mend - 1);
+            nky = __ldg(A.ky + mn);
+            nkx0 = __ldcg(A.kx0 + mn);
+            nkyi = __ldg(A.kyi + mn);
+            nkxi = __ldg(A.kxi + mn);
+        }
         const double a = kx_at(kx0, P.q, ts, ky);
         const double b = ky;
         const double ab = __dmul_rn(a, b);
@@ -503,7 +524,7 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
             kx0 = __dsub_rn(kx0, P.remap_shift);
         }
         const double* __restrict__ il2row = A.ilap2 + (size_t)kyi * nzd;
-        cplx* __restrict__ uo = A.lin_out + (size_t)m * 4 * nzd;
+        cplx* __restrict__ uo = lin_out + (size_t)m * 4 * nzd;
         cplx* __restrict__ fo = A.Fout ? A.Fout + (size_t)m * 4 * nzd : nullptr;
         const cplx* __restrict__ fpm = has_prev ? A.Fprev + (size_t)m * 4 * nzd : nullptr;
         cplx* KU = Kw + (size_t)pi * 2 * NZ;
@@ -768,10 +789,15 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         }
         // ---- after the mode: remap bookkeeping, next mode's copy, diagnostics
         if (zero && valid && role == 0 && t == 0) A.kx0[m] = kx0;
+        // the next mode's 1/lap2 row into L1 (a read-only table): its loads in slots 1, 5, 7 hit L1
+        if (wb + MPP < mend && lp * 16 < nzd) {
+            const double* row = A.ilap2 + (size_t)nkyi * nzd + 16 * lp;
+            asm volatile("prefetch.global.L1 [%0];\n" ::"l"(row));
+        }
         __syncwarp();  // every lane is done with the staging buffer and K
         {
             const int wn = wb + MPP;
-            if (leader && wn < mend) bulk_load(stg, A.lin_in + (size_t)min(wn + pi, mend - 1) * 4 * nzd, fbytes, bar);
+            if (leader && wn < mend) bulk_load(stg, lin_in + (size_t)min(wn + pi, mend - 1) * 4 * nzd, fbytes, bar);
         }
         if (diag_due && valid && !zero) {
             // Calc_Energy_AM_Diss per mode at t_new (MHD_BQlin.cpp:365-407): U sums the magnetic

@@ -114,6 +114,7 @@ constexpr int BATCH_EPOCH_STRIDE = 32;  // words between the per-case stage coun
 struct BatchCase {
     DevParams P;
     StageArgs A[3];
+    const double* kx_init;  // the unsheared wavenumber table (Kdata::kx) on the device
     // optional record of every stage input of a launch (null: off): step n, stage s at
     // rec_lin + (3 n + s) nxy 4 nz, rec_mf + (3 n + s) nmf nz, rec_kx + n nxy, rec_t + n
     cplx* rec_lin;

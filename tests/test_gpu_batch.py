@@ -312,3 +312,29 @@ def test_queue_engine_wait_bound_reports_timeout():
             t, lo, mo, ko = b.get_state(c)
             t2, lo2, mo2, ko2, _ = O.run(p, 0.0, lin, mf, kx0, 4)
             assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL
+
+
+@pytest.mark.parametrize("engine", ["queue", "items"])
+def test_set_states_get_states_match_per_case_calls(engine):
+    # every case in one call (some with their own kx0, some with the default table) and out
+    # again in one call, against the per-case entry points
+    cases = bq_cases()
+    base = states(cases)  # kx0 of initial_state is the default table
+    sts = [(lin, mf, kx0 + 0.5 * (2 * np.pi / p.L[0]) if c % 2 else None)
+           for c, (p, (lin, mf, kx0)) in enumerate(zip(cases, base))]
+    require_gpu()
+    with QLBatch(cases) as b:
+        b.set_engine(engine)
+        b.set_states(0.25, sts)
+        b.step(6)
+        a = b.get_states()
+        for c, (lin, mf, kx0) in enumerate(sts):
+            b.set_state(c, 0.25, lin, mf, kx0)
+        b.step(6)
+        for c in range(len(cases)):
+            t, lo, mo, ko = b.get_state(c)
+            assert a[c][0] == t and np.array_equal(a[c][1], lo) and np.array_equal(a[c][2], mo)
+            assert np.array_equal(a[c][3], ko)
+    for p, (lin, mf, kx0), (_, _, k_default), (t, lo, mo, ko) in zip(cases, sts, base, a):
+        t2, lo2, mo2, ko2, _ = O.run(p, 0.25, lin, mf, k_default if kx0 is None else kx0, 6)
+        assert abs(t - t2) < 1e-15 and rel(lo, lo2) < TOL and np.array_equal(ko, ko2)
