@@ -166,6 +166,12 @@ class ClockSampler:
             self.nvml = pynvml
             self.thread = threading.Thread(target=loop, daemon=True)
             self.thread.start()
+            # the thread is sampling before the timed region starts; only the samples taken
+            # from here on (inside the region) are kept
+            t_end = time.time() + 0.5
+            while not self.samples and time.time() < t_end:
+                time.sleep(0.0005)
+            self.samples.clear()
             return self
         except Exception:
             self.nvml = None

@@ -157,18 +157,37 @@ int qlgpu_stream(qlgpu_t* h, void** stream);
  * when h is NULL).  Returns the message length. */
 int qlgpu_last_error(const qlgpu_t* h, char* buf, int buflen);
 
+/* 1 in the debug build (libqlgpu_debug.so, compiled with -DQLGPU_DEBUG: device
+ * index checks and canary guard zones after every device buffer, checked after
+ * each call that launches kernels), else 0. */
+int qlgpu_debug_build(void);
+
+/* Debug build: overwrites the first byte of guard zone `zone` of the handle's
+ * buffers from the host, so that the next call that launches kernels returns
+ * QLGPU_ERR_STATUS with QLGPU_STATUS_CANARY (the test of the check itself).
+ * QLGPU_ERR_UNSUPPORTED in a release build; QLGPU_ERR_ARG for a bad zone. */
+int qlgpu_debug_guard_poke(qlgpu_t* h, int zone);
+
 /* Library version string. */
 const char* qlgpu_version(void);
 
 /* Driving noise after every step (Model::DrivingNoise, QL_DNS/Models/
- * MHD_BQlin.cpp:558-618, called by main.cpp:112-113 when f_noise != 0):
- * modes with ky != 0 and k_low < |k| < k_high get complex normal increments
- * of standard deviation f_noise/sqrt(2) per part, scaled as the reference.
- * The reference's clock-seeded mt19937 (MHD_BQlin.cpp:22) is replaced by one
+ * MHD_BQlin.cpp:558-618 and MHD_FullQlin.cpp:786-1045, called by
+ * main.cpp:112-113 when f_noise != 0): modes with k_low < |k| < k_high get
+ * complex normal increments of standard deviation f_noise/sqrt(2) per part,
+ * scaled as the reference.  MHD_BQlin drives ky != 0 modes only; MHD_FullQlin
+ * also drives ky = 0, kz != 0 in conjugate pairs, so that the field stays real
+ * (kx < 0 draws, its kx > 0 partner adds the conjugate at -kz).  The
+ * reference's clock-seeded mt19937 (MHD_BQlin.cpp:22) is replaced by one
  * Philox4x32-10 counter per (step since set_state, mode, kz, field) under
- * `seed`.  f_noise = 0 turns it off.  MHD_BQlin only (QLGPU_ERR_UNSUPPORTED
- * otherwise). */
+ * `seed`.  f_noise = 0 turns it off. */
 int qlgpu_set_noise(qlgpu_t* h, double f_noise, double k_low, double k_high, unsigned long long seed);
+
+/* MHD_FullQlin's drive_only_velocityQ / drive_only_magneticQ inputs
+ * (MHD_FullQlin.cpp:21-22): nonzero drive_only_velocity leaves b and eta
+ * undriven, nonzero drive_only_magnetic leaves u and zeta undriven.  Both 0 by
+ * default; MHD_BQlin has no such switches (QLGPU_ERR_UNSUPPORTED when set). */
+int qlgpu_set_noise_fields(qlgpu_t* h, int drive_only_velocity, int drive_only_magnetic);
 
 /* Variable time step (RK3CN_Elin.cpp:76-80; RK3CN.cpp alike): cfl > 0 makes
  * every step dt = cfl / Calculate_CFL (MHD_BQlin.cpp:540-552,
@@ -225,6 +244,11 @@ int qlgpu_adjoint_maxwell_batch(qlgpu_t* const* handles, int nseeds, double t0, 
 typedef struct qlgpu_batch qlgpu_batch_t;
 
 #define QLGPU_STATUS_BATCH_TIMEOUT 8 /* a CTA gave up waiting for the others of its case */
+/* Debug build only (libqlgpu_debug.so, -DQLGPU_DEBUG): a device index check
+ * failed (the access was redirected in bounds), or a guard zone after a device
+ * buffer was overwritten.  Either makes the call return QLGPU_ERR_STATUS. */
+#define QLGPU_STATUS_BOUNDS 16
+#define QLGPU_STATUS_CANARY 32
 
 /* Creates the batch (device memory, wavenumber tables, an initial CTA
  * mapping from the cost model).  All cases zero; t = 0. */
@@ -242,6 +266,16 @@ int qlgpu_batch_get_state(qlgpu_batch_t* b, int c, double* t, double* lin, doubl
 int qlgpu_batch_set_states(qlgpu_batch_t* b, double t, const double* const* lin, const double* const* mf,
                            const double* const* kx0);
 int qlgpu_batch_get_states(qlgpu_batch_t* b, double* t, double* const* lin, double* const* mf, double* const* kx0);
+
+/* Driving noise of case c after every step, as qlgpu_set_noise and
+ * qlgpu_set_noise_fields of a single handle with the case's fixed dt: the
+ * Philox counter's step word counts the steps since the case's state was set.
+ * f_noise = 0 turns it off (the default). */
+int qlgpu_batch_set_noise(qlgpu_batch_t* b, int c, double f_noise, double k_low, double k_high,
+                          unsigned long long seed, int drive_only_velocity, int drive_only_magnetic);
+
+/* Debug build: as qlgpu_debug_guard_poke for the batch's buffers. */
+int qlgpu_batch_debug_guard_poke(qlgpu_batch_t* b, int zone);
 
 /* Initial diagnostic record of case c (15 doubles, as qlgpu_diagnostics). */
 int qlgpu_batch_diagnostics(qlgpu_batch_t* b, int c, double* out15);

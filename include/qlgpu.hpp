@@ -56,6 +56,8 @@ struct Inputs {
     // driving noise (Input_parameters.cpp:107-109); the generator's seed replaces the clock
     double f_noise = 0.0, noise_range_low = 0.0, noise_range_high = 1e16;
     unsigned long long noise_seed = 0;
+    // MHD_FullQlin only (Input_parameters.cpp:110-111, MHD_FullQlin.cpp:21-22)
+    bool drive_only_velocityQ = false, drive_only_magneticQ = false;
 };
 
 class Model;
@@ -178,8 +180,11 @@ public:
         check(qlgpu_create(&p_, -1, &h_), nullptr);
         variable_dt_ = sp.dt < 0;
         if (variable_dt_) check(qlgpu_set_cfl(h_, sp.CFL, -sp.dt), h_);
-        if (sp.f_noise != 0.0)
+        if (sp.f_noise != 0.0) {
             check(qlgpu_set_noise(h_, sp.f_noise, sp.noise_range_low, sp.noise_range_high, sp.noise_seed), h_);
+            if (sp.drive_only_velocityQ || sp.drive_only_magneticQ)
+                check(qlgpu_set_noise_fields(h_, sp.drive_only_velocityQ, sp.drive_only_magneticQ), h_);
+        }
     }
     virtual ~Integrator() {
         if (h_) qlgpu_destroy(h_);

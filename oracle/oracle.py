@@ -61,6 +61,7 @@ def lib(kind: str = "strict"):
     L.oracle_run_forced.argtypes = [ctypes.POINTER(OracleParams), dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, dp,
                                     ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double, ctypes.c_ulonglong, dp]
+    L.oracle_run_forced_fields.argtypes = L.oracle_run_forced.argtypes[:-1] + [ctypes.c_int, ctypes.c_int, dp]
     u32p = ctypes.POINTER(ctypes.c_uint32)
     L.oracle_philox.argtypes = [u32p, u32p, u32p]
     _LIBS[kind] = L
@@ -121,9 +122,11 @@ def run(p, t0, lin, mf, kx0, nsteps, diag_every=0, kind: str = "strict", nthread
 
 
 def run_forced(p, t0, lin, mf, kx0, nsteps, diag_every=0, cfl=0.0, dt_max=0.0, f_noise=0.0, k_lo=0.0,
-               k_hi=0.0, seed=0, kind: str = "strict"):
+               k_hi=0.0, seed=0, kind: str = "strict", drive_only_velocity=False, drive_only_magnetic=False):
     """main.cpp loop with variable dt (cfl > 0) and driving noise (f_noise != 0); a
-    record after every diag_every-th step -> (t, lin, mf, kx0, diag[nrec, 15], dt_mean)."""
+    record after every diag_every-th step -> (t, lin, mf, kx0, diag[nrec, 15], dt_mean).
+    drive_only_velocity / drive_only_magnetic: the MHD_FullQlin switches
+    (MHD_FullQlin.cpp:21-22)."""
     lin = np.ascontiguousarray(lin, dtype=np.complex128).copy()
     mf = np.ascontiguousarray(mf, dtype=np.complex128).copy()
     kx0 = np.ascontiguousarray(kx0, dtype=np.float64).copy()
@@ -132,8 +135,9 @@ def run_forced(p, t0, lin, mf, kx0, nsteps, diag_every=0, cfl=0.0, dt_max=0.0, f
     diag = np.zeros((maxd, 15))
     dtm = np.zeros(1)
     pp = _params(p)
-    n = lib(kind).oracle_run_forced(ctypes.byref(pp), _dp(t), _dp(lin), _dp(mf), _dp(kx0), nsteps, diag_every,
-                                    _dp(diag), maxd, cfl, dt_max, f_noise, k_lo, k_hi, seed, _dp(dtm))
+    n = lib(kind).oracle_run_forced_fields(ctypes.byref(pp), _dp(t), _dp(lin), _dp(mf), _dp(kx0), nsteps,
+                                           diag_every, _dp(diag), maxd, cfl, dt_max, f_noise, k_lo, k_hi, seed,
+                                           int(bool(drive_only_velocity)), int(bool(drive_only_magnetic)), _dp(dtm))
     return float(t[0]), lin, mf, kx0, diag[:n], float(dtm[0])
 
 

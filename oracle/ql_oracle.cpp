@@ -343,16 +343,31 @@ struct Model {
     }
 
     // DrivingNoise of MHD_BQlin (MHD_BQlin.cpp:558-618; ky = 0 modes are not
-    // driven, dont_drive_ky0_modes_ = 1 at :18).  The reference draws from a
-    // clock-seeded mt19937 (:22-23); here every (step, mode, kz, field) has its
-    // own Philox4x32-10 counter and Box-Muller pair, so runs are reproducible
-    // and the GPU draws the same numbers.
+    // driven, dont_drive_ky0_modes_ = 1 at :18) and of MHD_FullQlin
+    // (MHD_FullQlin.cpp:786-1045: the same on ky != 0 modes, :795-848, with the
+    // drive_only_velocity / drive_only_magnetic switches of :21-22, and ky = 0
+    // driven, dont_drive_ky0_modes_ = 0 at :19).  For ky = 0 every kx < 0 mode
+    // (Kdata.cpp:124-146: its kx > 0 partner has the same |kx|) draws noise at kz
+    // indices 1..nz-1 (:969-1023) and the partner adds the reversed conjugate
+    // buffer to indices 1..nz-1 (:1028-1040), pos[nz - k] += conj(noise_neg[k]).
+    // The reference draws from a clock-seeded mt19937 (MHD_BQlin.cpp:22-23);
+    // here every (step, mode, kz, field) has its own Philox4x32-10 counter and
+    // Box-Muller pair, so runs are reproducible and the GPU draws the same numbers.
     void driving_noise(double t, double dt, State& sol, const std::vector<double>& kx0, double f_noise,
-                       double k_lo, double k_hi, unsigned long long seed, unsigned long long step) {
+                       double k_lo, double k_hi, unsigned long long seed, unsigned long long step,
+                       bool only_velocity = false, bool only_magnetic = false) {
         const double lo2 = k_lo * k_lo, hi2 = k_hi * k_hi;
         const double mult_noise_fac = (1.0 / (16 * 32 * 32)) * (1.0 / (16 * 32 * 32));  // :35-36
         const double multfac = dt * (double)totalN2 * mult_noise_fac;
         const double sd = f_noise / std::sqrt(2.0);
+        const bool full = p.model == 1;
+        const bool drive_v[4] = {!(full && only_magnetic), !(full && only_magnetic), !(full && only_velocity),
+                                 !(full && only_velocity)};
+        auto draw = [&](int i, int k, int v, double mult) {
+            double z1, z2;
+            philox_normal_pair(seed, step, (unsigned)i, (unsigned)(4 * k + v), &z1, &z2);
+            return mult * cd(z1 * sd, z2 * sd);
+        };
         for (int i = 0; i < d.nxy; ++i) {
             if (K.ky_index[i] == 0) continue;
             ModeK m;
@@ -363,10 +378,28 @@ struct Model {
                 const double mu = std::sqrt(multfac * lap2 / lapF);
                 const double mz = std::sqrt(-multfac * lap2);
                 for (int v = 0; v < 4; ++v) {
-                    double z1, z2;
-                    philox_normal_pair(seed, step, (unsigned)i, (unsigned)(4 * k + v), &z1, &z2);
-                    const double mult = (v == 0 || v == 2) ? mu : mz;
-                    sol.pLin(i, v)[k] += mult * cd(z1 * sd, z2 * sd);
+                    if (!drive_v[v]) continue;
+                    sol.pLin(i, v)[k] += draw(i, k, v, (v == 0 || v == 2) ? mu : mz);
+                }
+            }
+        }
+        if (!full) return;
+        const int nx = d.Nx / 2, ny = d.Ny / 2;
+        for (int a = 1; a < nx; ++a) {
+            const int ipos = a * ny;                 // kx index a (Kdata.cpp:30-37)
+            const int ineg = (2 * nx - a - 1) * ny;  // kx index -a (Kdata.cpp:39-46)
+            ModeK m;
+            assign_laplacians(p, d, K, kx0, ineg, t, false, m);
+            for (int k = 1; k < d.nz; ++k) {
+                const double lapF = m.lapF[k], lap2 = m.lap2[k];
+                if (!(lapF > -hi2 && lapF < -lo2)) continue;
+                const double mu = std::sqrt(multfac * lap2 / lapF);
+                const double mz = std::sqrt(-multfac * lap2);
+                for (int v = 0; v < 4; ++v) {
+                    if (!drive_v[v]) continue;
+                    const cd n = draw(ineg, k, v, (v == 0 || v == 2) ? mu : mz);
+                    sol.pLin(ineg, v)[k] += n;
+                    sol.pLin(ipos, v)[d.nz - k] += std::conj(n);
                 }
             }
         }
@@ -1041,9 +1074,10 @@ int oracle_run(const OracleParams* p, double* t_io, double* lin_io, double* mf_i
 // driving noise after every step (main.cpp:112-113), then t += dt and the
 // remap.  A diagnostic record after every diag_every-th step (and the initial
 // one).  Returns the record count; *dt_mean_out = Integrator::mean_time_step.
-int oracle_run_forced(const OracleParams* p, double* t_io, double* lin_io, double* mf_io, double* kx0_io,
-                      int nsteps, int diag_every, double* diag_out, int max_diag, double cfl, double dt_max,
-                      double f_noise, double k_lo, double k_hi, unsigned long long seed, double* dt_mean_out) {
+int oracle_run_forced_fields(const OracleParams* p, double* t_io, double* lin_io, double* mf_io, double* kx0_io,
+                             int nsteps, int diag_every, double* diag_out, int max_diag, double cfl, double dt_max,
+                             double f_noise, double k_lo, double k_hi, unsigned long long seed, int only_velocity,
+                             int only_magnetic, double* dt_mean_out) {
     Model M(*p);
     State s;
     s.init(M.d);
@@ -1070,7 +1104,9 @@ int oracle_run_forced(const OracleParams* p, double* t_io, double* lin_io, doubl
         }
         I.step(t, dt, s, kx0);
         dt_sum += dt;
-        if (f_noise != 0.0) M.driving_noise(t, dt, s, kx0, f_noise, k_lo, k_hi, seed, (unsigned long long)n);
+        if (f_noise != 0.0)
+            M.driving_noise(t, dt, s, kx0, f_noise, k_lo, k_hi, seed, (unsigned long long)n, only_velocity != 0,
+                            only_magnetic != 0);
         t += dt;
         if (p->remap) M.remap(p->q * t, s, kx0);
         if (diag_every > 0 && (n + 1) % diag_every == 0) record(t);
@@ -1081,6 +1117,13 @@ int oracle_run_forced(const OracleParams* p, double* t_io, double* lin_io, doubl
     std::memcpy(mf_io, s.mf.data(), s.mf.size() * sizeof(cd));
     std::memcpy(kx0_io, kx0.data(), kx0.size() * sizeof(double));
     return nrec;
+}
+
+int oracle_run_forced(const OracleParams* p, double* t_io, double* lin_io, double* mf_io, double* kx0_io,
+                      int nsteps, int diag_every, double* diag_out, int max_diag, double cfl, double dt_max,
+                      double f_noise, double k_lo, double k_hi, unsigned long long seed, double* dt_mean_out) {
+    return oracle_run_forced_fields(p, t_io, lin_io, mf_io, kx0_io, nsteps, diag_every, diag_out, max_diag, cfl,
+                                    dt_max, f_noise, k_lo, k_hi, seed, 0, 0, dt_mean_out);
 }
 
 // Philox4x32-10 of one counter (known-answer tests of the generator).

@@ -12,6 +12,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libqlgpu.so")
+# QLGPU_DEBUG=1: the -DQLGPU_DEBUG build (device bounds checks, canary-guarded buffers)
+DEBUG_LIB_PATH = os.path.join(HERE, "_lib", "libqlgpu_debug.so")
 
 QLGPU_OK = 0
 ERRORS = {1: "QLGPU_ERR_ARG", 2: "QLGPU_ERR_UNSUPPORTED", 3: "QLGPU_ERR_CUDA", 4: "QLGPU_ERR_STATUS",
@@ -39,7 +41,8 @@ EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "ql
            "qlgpu_dns_step", "qlgpu_dns_diagnostics", "qlgpu_dns_rhs", "qlgpu_dns_status", "qlgpu_dns_last_error",
            "qlgpu_dns_step_timed", "qlgpu_dns_stream", "qlgpu_fp64_peak",
            "qlgpu_set_noise", "qlgpu_set_cfl", "qlgpu_mean_time_step", "qlgpu_adjoint_maxwell_batch",
-           "qlgpu_batch_cost_model"]
+           "qlgpu_batch_cost_model", "qlgpu_set_noise_fields", "qlgpu_batch_set_noise", "qlgpu_debug_build",
+           "qlgpu_debug_guard_poke", "qlgpu_batch_debug_guard_poke"]
 
 
 class qlgpu_params(ctypes.Structure):
@@ -76,11 +79,14 @@ class QLGPUError(RuntimeError):
 _lib = None
 
 
-def load(path: str = LIB_PATH):
-    """Load libqlgpu.so (raises if it is missing; there is no fallback)."""
+def load(path: str | None = None):
+    """Load libqlgpu.so, or libqlgpu_debug.so when QLGPU_DEBUG=1 (raises if it is
+    missing; there is no fallback)."""
     global _lib
     if _lib is not None:
         return _lib
+    if path is None:
+        path = DEBUG_LIB_PATH if os.environ.get("QLGPU_DEBUG") == "1" else LIB_PATH
     if not os.path.exists(path):
         raise QLGPUError(5, f"{path} not built (python -m ql_dns_b200.build)")
     L = ctypes.CDLL(path)
@@ -157,6 +163,12 @@ def load(path: str = LIB_PATH):
     L.qlgpu_dns_stream.restype = vp
     L.qlgpu_fp64_peak.argtypes = [ctypes.c_int, dp]
     L.qlgpu_set_noise.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong]
+    L.qlgpu_set_noise_fields.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.qlgpu_debug_build.argtypes = []
+    L.qlgpu_debug_guard_poke.argtypes = [vp, ctypes.c_int]
+    L.qlgpu_batch_debug_guard_poke.argtypes = [vp, ctypes.c_int]
+    L.qlgpu_batch_set_noise.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int]
     L.qlgpu_set_cfl.argtypes = [vp, ctypes.c_double, ctypes.c_double]
     L.qlgpu_mean_time_step.argtypes = [vp, dp]
     L.qlgpu_batch_cost_model.argtypes = [vp, dp]

@@ -165,6 +165,13 @@ class QLBatch:
         k = (ctypes.c_int * len(ncta))(*ncta)
         _capi.check_batch(self.L.qlgpu_batch_set_mapping(self.b, int(warps), k), self.b)
 
+    def set_noise(self, c: int, f_noise: float, k_low: float, k_high: float, seed: int = 0,
+                  drive_only_velocity: bool = False, drive_only_magnetic: bool = False):
+        """Driving noise of case c after every step (as QLSolver.set_noise); f_noise = 0: off."""
+        _capi.check_batch(self.L.qlgpu_batch_set_noise(self.b, int(c), float(f_noise), float(k_low), float(k_high),
+                                                       int(seed), int(bool(drive_only_velocity)),
+                                                       int(bool(drive_only_magnetic))), self.b)
+
     ENGINES = {"auto": 0, "items": 1, "queue": 2}
 
     def set_engine(self, engine: str):

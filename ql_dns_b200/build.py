@@ -1,6 +1,12 @@
 """Build the sm_100a shared library ql_dns_b200/_lib/libqlgpu.so in-tree.
 
-Usage: python -m ql_dns_b200.build [--force] [--verbose]
+Usage: python -m ql_dns_b200.build [--force] [--verbose] [--debug]
+
+--debug builds ql_dns_b200/_lib/libqlgpu_debug.so with -DQLGPU_DEBUG: device
+bounds checks on the index math of every kernel family (a failed check sets a
+status bit and the access is redirected in bounds, no trap) and canary-guarded
+device buffers checked after every launch.  QLGPU_DEBUG=1 in the environment
+makes the Python binding load it.
 """
 from __future__ import annotations
 
@@ -16,6 +22,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libqlgpu.so")
+DEBUG_LIB = os.path.join(OUT_DIR, "libqlgpu_debug.so")
 MAIN = os.path.join(OUT_DIR, "ql_main")
 
 NVCC_FLAGS = [
@@ -25,6 +32,7 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr",
 ]
 OBJ_DIR = os.path.join(OUT_DIR, "obj")
+DEBUG_OBJ_DIR = os.path.join(OUT_DIR, "obj_debug")
 
 
 def sources():
@@ -37,10 +45,10 @@ def deps():
             glob.glob(os.path.join(ROOT, "include", "*")))
 
 
-def stale() -> bool:
-    if not os.path.exists(LIB):
+def stale(lib: str = LIB) -> bool:
+    if not os.path.exists(lib):
         return True
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     return any(os.path.getmtime(d) > t for d in deps())
 
 
@@ -49,20 +57,24 @@ def _headers_mtime() -> float:
     return max(os.path.getmtime(h) for h in hs) if hs else 0.0
 
 
-def build(force: bool = False, verbose: bool = False, extra=None, jobs: int | None = None) -> str:
-    if not force and not stale():
-        return LIB
-    os.makedirs(OBJ_DIR, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, extra=None, jobs: int | None = None,
+          debug: bool = False) -> str:
+    lib = DEBUG_LIB if debug else LIB
+    obj_dir = DEBUG_OBJ_DIR if debug else OBJ_DIR
+    if not force and not stale(lib):
+        return lib
+    os.makedirs(obj_dir, exist_ok=True)
+    flags = NVCC_FLAGS + (["-DQLGPU_DEBUG"] if debug else [])
     nvcc = os.environ.get("NVCC", "nvcc")
     hdr_t = _headers_mtime()
     inc = ["-I" + os.path.join(ROOT, "include")]
 
     def compile_one(src):
-        obj = os.path.join(OBJ_DIR, os.path.splitext(os.path.basename(src))[0] + ".o")
+        obj = os.path.join(obj_dir, os.path.splitext(os.path.basename(src))[0] + ".o")
         if (not force and extra is None and os.path.exists(obj) and os.path.getmtime(obj) > os.path.getmtime(src)
                 and os.path.getmtime(obj) > hdr_t):
             return obj
-        cmd = [nvcc] + NVCC_FLAGS + (extra or []) + inc + ["-c", "-o", obj + ".tmp.o", src]
+        cmd = [nvcc] + flags + (extra or []) + inc + ["-c", "-o", obj + ".tmp.o", src]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -80,13 +92,14 @@ def build(force: bool = False, verbose: bool = False, extra=None, jobs: int | No
     with concurrent.futures.ThreadPoolExecutor(max_workers=n) as ex:
         objs = list(ex.map(compile_one, srcs))
     cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC", "-o",
-           LIB + ".tmp"] + objs
+           lib + ".tmp"] + objs
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
-    os.replace(LIB + ".tmp", LIB)
-    build_main(verbose)
-    return LIB
+    os.replace(lib + ".tmp", lib)
+    if not debug:
+        build_main(verbose)
+    return lib
 
 
 def build_main(verbose: bool = False) -> str:
@@ -106,7 +119,8 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas-v", action="store_true")
+    ap.add_argument("--debug", action="store_true")
     a = ap.parse_args()
-    build(force=a.force or a.ptxas_v, verbose=a.verbose, extra=(["-Xptxas", "-v"] if a.ptxas_v else None))
-    print(LIB)
+    print(build(force=a.force or a.ptxas_v, verbose=a.verbose, extra=(["-Xptxas", "-v"] if a.ptxas_v else None),
+                debug=a.debug))
     sys.exit(0)

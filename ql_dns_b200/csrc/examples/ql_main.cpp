@@ -59,6 +59,8 @@ int main(int argc, char** argv) {
     SP.noise_range_low = read_key<double>(full, "noise_range_low_", 0.0);
     SP.noise_range_high = read_key<double>(full, "noise_range_high_", 1e16);
     SP.noise_seed = (unsigned long long)read_key<double>(full, "noise_seed_", 0.0);
+    SP.drive_only_velocityQ = read_key<int>(full, "drive_only_velocity?", 0) != 0;
+    SP.drive_only_magneticQ = read_key<int>(full, "drive_only_magnetic?", 0) != 0;
     const double tv_save = read_key<double>(full, "tv_save_", SP.dt < 0 ? -SP.dt : SP.dt);
     const int integ = read_key<int>(full, "integrator_", 0);  // 0 RK3CN_Elin (main.cpp:95), 1 RK3CN
     const int nsteps = std::atoi(argv[3]);

@@ -126,6 +126,28 @@ int check_launch(qlgpu_t* h) {
 
 }  // namespace
 
+// Debug build: after a call's launches, the device index checks' status bits (the clock's
+// and the adjoint kernels') and the guard zones after every buffer.  A release build
+// returns at once.
+int qlgpu_debug_verify(qlgpu_t* h) {
+#ifdef QLGPU_DEBUG
+    int st = 0, sa = 0, g = 0;
+    QLGPU_CK(cudaMemcpyAsync(&st, &h->d_clk->status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(cudaMemcpyAsync(&sa, h->d_dbg, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    QLGPU_CK(guard_check(h->guards, h->stream, &g));
+    st = ((st | sa) & QLGPU_STATUS_BOUNDS) | g;
+    if (st) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "debug build: device status 0x%x (%s)", st,
+                      (st & QLGPU_STATUS_BOUNDS) ? "an index check failed" : "a guard zone was overwritten");
+        return fail(h, QLGPU_ERR_STATUS, buf);
+    }
+#else
+    (void)h;
+#endif
+    return QLGPU_OK;
+}
+
 extern "C" {
 
 const char* qlgpu_version(void) { return "qlgpu 0.1 (sm_100a, FP64)"; }
@@ -253,11 +275,12 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
         return bail(QLGPU_ERR_CUDA);
     }
     const size_t nlin = (size_t)h->nxy * 4 * h->nz, nmfe = (size_t)h->nmf * h->nz;
-#define QLGPU_ALLOC(ptr, bytes)                                        \
-    if (cudaMalloc(&(ptr), (bytes)) != cudaSuccess) {                  \
-        h->err = "cudaMalloc failed for " #ptr;                        \
-        return bail(QLGPU_ERR_CUDA);                                   \
-    }                                                                  \
+#define QLGPU_ALLOC(ptr, bytes)                                                      \
+    if (cudaMalloc(&(ptr), (bytes) + QLGPU_GUARD_BYTES) != cudaSuccess) {             \
+        h->err = "cudaMalloc failed for " #ptr;                                      \
+        return bail(QLGPU_ERR_CUDA);                                                 \
+    }                                                                                \
+    guard_add(h->guards, (ptr), (bytes));                                            \
     cudaMemsetAsync((ptr), 0, (bytes), h->stream);
     QLGPU_ALLOC(h->d_lin[0], nlin * sizeof(cplx));
     QLGPU_ALLOC(h->d_lin[1], nlin * sizeof(cplx));
@@ -278,6 +301,7 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
     QLGPU_ALLOC(h->d_ilap2, (size_t)(p.ny / 2) * h->nz * sizeof(double));
     QLGPU_ALLOC(h->d_mfr, (size_t)8 * h->NZ * sizeof(double));
     QLGPU_ALLOC(h->d_ekz, (size_t)6 * h->nz * sizeof(double));
+    QLGPU_ALLOC(h->d_dbg, sizeof(int));
     const std::vector<double> tw = twiddles(h->NZ, var.T);
     cudaMemcpyAsync(h->d_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream);
     h->il2_tab = ilap2_table(p, h->nz);
@@ -297,6 +321,10 @@ int qlgpu_create(const qlgpu_params* pp, int device, qlgpu_t** out) {
         }
     }
 #undef QLGPU_ALLOC
+    if (guard_arm(h->guards, h->stream) != cudaSuccess) {
+        h->err = "guard zones";
+        return bail(QLGPU_ERR_CUDA);
+    }
     rc = reset_clock(h, 0.0);
     if (rc) return bail(rc);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
@@ -314,11 +342,12 @@ int qlgpu_destroy(qlgpu_t* h) {
     void* bufs[] = {h->d_lin[0], h->d_lin[1], h->d_F1, h->d_F2, h->d_mf, h->d_Fmf1, h->d_Fmf2,
                     h->d_kx0, h->d_ky, h->d_kxi, h->d_kyi, h->d_tw, h->d_partials, h->d_gpartials,
                     h->d_clk, h->d_diag, h->d_out15, h->d_linop, h->d_ilap2, h->d_trace,
-                    h->d_mfr, h->d_ekz, h->d_forcing, h->d_kx0_prev};
+                    h->d_mfr, h->d_ekz, h->d_forcing, h->d_kx0_prev, h->d_dbg};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : h->ev)
         if (e) cudaEventDestroy(e);
+    guard_release(h->guards);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return QLGPU_OK;
@@ -407,8 +436,6 @@ static int step_forced(qlgpu_t* h, int nsteps, int diag_every, double* diag_out,
     const double tv_saved = h->dp.tv_interval;
     h->dp.tv_interval = 0.0;  // records come from diag_kernel here
     h->ekz_dynamic = h->cfl > 0;
-    const long tot = (long)h->p.nx * ((h->p.ny / 2) * 2) * h->NZ;
-    const double mult_noise_fac = (1.0 / (16 * 32 * 32)) * (1.0 / (16 * 32 * 32));  // MHD_BQlin.cpp:35-36
     int nd = 0, rc = QLGPU_OK;
     for (int n = 0; n < nsteps && rc == QLGPU_OK; ++n) {
         double dt = h->p.dt;
@@ -442,18 +469,16 @@ static int step_forced(qlgpu_t* h, int nsteps, int diag_every, double* diag_out,
             a.kx0_prev = h->d_kx0_prev;
             a.kx0_now = h->d_kx0;
             a.ky = h->d_ky;
+            a.kxi = h->d_kxi;
             a.kyi = h->d_kyi;
             a.nxy = h->nxy;
             a.nz = h->nz;
             a.q = h->p.q;
             a.t = t;
             a.kzL = 2 * kPI / h->p.L[2];
-            a.lo2 = h->noise_klo * h->noise_klo;
-            a.hi2 = h->noise_khi * h->noise_khi;
-            a.multfac = dt * (double)tot * (double)tot * mult_noise_fac;
-            a.sd = h->noise_f / std::sqrt(2.0);
-            a.seed = h->noise_seed;
             a.step = h->steps_taken;
+            a.ns = noise_spec(h->p, h->NZ, dt, h->noise_f, h->noise_klo, h->noise_khi, h->noise_seed,
+                              h->noise_only_vel, h->noise_only_mag);
             const int n_el = h->nxy * h->nz;
             noise_kernel<<<(n_el + 255) / 256, 256, 0, h->stream>>>(a);
         }
@@ -479,19 +504,38 @@ static int step_forced(qlgpu_t* h, int nsteps, int diag_every, double* diag_out,
     if (ndiag) *ndiag = nd;
     if (c.status & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE))
         return fail(h, QLGPU_ERR_STATUS, "device status set: non-finite or unstable solution");
-    return QLGPU_OK;
+    return qlgpu_debug_verify(h);
 }
 
 int qlgpu_set_noise(qlgpu_t* h, double f_noise, double k_low, double k_high, unsigned long long seed) {
     if (!h) return QLGPU_ERR_ARG;
     if (!std::isfinite(f_noise) || !(k_low >= 0) || !(k_high >= k_low))
         return fail(h, QLGPU_ERR_ARG, "noise: finite f_noise, 0 <= k_low <= k_high");
-    if (f_noise != 0.0 && h->p.model != QLGPU_MODEL_MHD_BQLIN)
-        return fail(h, QLGPU_ERR_UNSUPPORTED, "driving noise is built for MHD_BQlin");
     h->noise_f = f_noise;
     h->noise_klo = k_low;
     h->noise_khi = k_high;
     h->noise_seed = seed;
+    return QLGPU_OK;
+}
+
+int qlgpu_debug_build(void) { return QLGPU_DEBUG_BUILD; }
+
+int qlgpu_debug_guard_poke(qlgpu_t* h, int zone) {
+    if (!h) return QLGPU_ERR_ARG;
+    if (!QLGPU_DEBUG_BUILD) return fail(h, QLGPU_ERR_UNSUPPORTED, "guard zones exist in the debug build only");
+    if (zone < 0 || zone >= (int)h->guards.zones.size()) return fail(h, QLGPU_ERR_ARG, "no such guard zone");
+    QLGPU_CK(cudaSetDevice(h->device));
+    QLGPU_CK(guard_poke(h->guards, zone, h->stream));
+    QLGPU_CK(cudaStreamSynchronize(h->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_set_noise_fields(qlgpu_t* h, int drive_only_velocity, int drive_only_magnetic) {
+    if (!h) return QLGPU_ERR_ARG;
+    if ((drive_only_velocity || drive_only_magnetic) && h->p.model != QLGPU_MODEL_MHD_FULLQLIN)
+        return fail(h, QLGPU_ERR_UNSUPPORTED, "drive_only_velocity / drive_only_magnetic are MHD_FullQlin inputs");
+    h->noise_only_vel = drive_only_velocity != 0;
+    h->noise_only_mag = drive_only_magnetic != 0;
     return QLGPU_OK;
 }
 
@@ -553,7 +597,7 @@ int qlgpu_step(qlgpu_t* h, int nsteps, int diag_every, double* diag_out, int max
                                                            : "diagnostic records dropped (max_diag too small)");
         return fail(h, QLGPU_ERR_STATUS, buf);
     }
-    return QLGPU_OK;
+    return qlgpu_debug_verify(h);
 }
 
 int qlgpu_step_timed(qlgpu_t* h, float* stage_ms) {
@@ -570,7 +614,7 @@ int qlgpu_step_timed(qlgpu_t* h, float* stage_ms) {
     int st = 0;
     QLGPU_CK(cudaMemcpy(&st, &h->d_clk->status, sizeof(int), cudaMemcpyDeviceToHost));
     if (st & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE)) return fail(h, QLGPU_ERR_STATUS, "device status set");
-    return QLGPU_OK;
+    return qlgpu_debug_verify(h);
 }
 
 int qlgpu_diagnostics(qlgpu_t* h, double* out15) {
@@ -584,7 +628,7 @@ int qlgpu_diagnostics(qlgpu_t* h, double* out15) {
     if (rc) return rc;
     QLGPU_CK(cudaMemcpyAsync(out15, h->d_out15, 15 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     QLGPU_CK(cudaStreamSynchronize(h->stream));
-    return QLGPU_OK;
+    return qlgpu_debug_verify(h);
 }
 
 int qlgpu_rhs(qlgpu_t* h, double t, double dt_lin, const double* lin_in, const double* mf_in, double* lin_rhs,
@@ -615,7 +659,7 @@ int qlgpu_rhs(qlgpu_t* h, double t, double dt_lin, const double* lin_in, const d
     if (linop) QLGPU_CK(cudaMemcpyAsync(linop, h->d_linop, nlin * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     QLGPU_CK(cudaMemcpyAsync(h->d_mf, h->d_Fmf2, nmfe * sizeof(cplx), cudaMemcpyDeviceToDevice, h->stream));
     QLGPU_CK(cudaStreamSynchronize(h->stream));
-    return QLGPU_OK;
+    return qlgpu_debug_verify(h);
 }
 
 int qlgpu_status(qlgpu_t* h, int* status) {

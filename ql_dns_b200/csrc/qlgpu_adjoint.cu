@@ -354,6 +354,7 @@ int adj_backward_step(AdjJob& j, int steps, int n) {
         j.ops.mf_pre(M, h->dp, st);
         AdjStageArgs A;
         std::memset(&A, 0, sizeof(A));
+        A.status = h->d_dbg;
         A.U = j.stU + ((size_t)n * 3 + s) * j.nlin;
         A.lamU_out = j.lamU[j.iu];
         A.lamF_out = (s == 2) ? nullptr : j.lamF[0];
@@ -423,6 +424,7 @@ int adj_backward_step_seeds(SeedReverse& R, cudaStream_t st, int steps, int n) {
         R.ops.mf_pre_s(M, h->dp, X, ns, st);
         AdjStageArgs A;
         std::memset(&A, 0, sizeof(A));
+        A.status = h->d_dbg;
         A.ky = h->d_ky;
         A.kxi = h->d_kxi;
         A.kyi = h->d_kyi;
@@ -821,7 +823,8 @@ extern "C" int qlgpu_adjoint_maxwell(qlgpu_t* h, double t0, const double* lin0, 
     if (rc) return rc;
     double* gl[1] = {grad_lin};
     double* gm[1] = {grad_mf};
-    return run_jobs(jobs, J, gl, grad_mf ? gm : nullptr);
+    rc = run_jobs(jobs, J, gl, grad_mf ? gm : nullptr);
+    return rc ? rc : qlgpu_debug_verify(h);
 }
 
 extern "C" int qlgpu_adjoint_maxwell_batch(qlgpu_t* const* handles, int nseeds, double t0, const double* lin0,
@@ -858,6 +861,7 @@ extern "C" int qlgpu_adjoint_maxwell_batch(qlgpu_t* const* handles, int nseeds, 
     const bool streams = mode && std::string(mode) == "streams";
     int rc = streams ? run_jobs(jobs, J, gl.data(), grad_mf ? gm.data() : nullptr)
                      : run_jobs_persistent(jobs, t0, lin0, mf0, kx0, J, gl.data(), grad_mf ? gm.data() : nullptr);
+    for (int q = 0; q < nseeds && !rc; ++q) rc = qlgpu_debug_verify(handles[q]);
     if (rc) {
         for (int q = 0; q < nseeds; ++q)
             if (!handles[q]->err.empty() && handles[q] != h0) h0->err = handles[q]->err;

@@ -28,6 +28,7 @@
 // contribution to the adjoint of the mean-field profiles, nine forward
 // transforms, and the spectral chain back to (u, zeta, b, eta).
 #pragma once
+#include "qlgpu_debug.cuh"
 #include "qlgpu_stage.cuh"
 
 namespace qlgpu {
@@ -51,6 +52,7 @@ struct AdjStageArgs {
     const CnRec* cn;       // RK3CN: the old-operator fields at the stage start
     int integ;             // INTEG_EXP or INTEG_CN
     int pad;
+    int* status;           // the handle's status word (debug-build index checks)
     StageConst sc;
 };
 
@@ -82,7 +84,8 @@ __device__ __forceinline__ double adj_efac(const DevParams& P, const StageConst&
 // The stage adjoint of one mode (one CTA).  A may live in parameter space (one
 // seed per launch) or in shared memory (a launch over many seeds).
 template <int NZ>
-__device__ __forceinline__ void adj_modes_body(const AdjStageArgs& A, const DevParams& P, const int mode) {
+__device__ __forceinline__ void adj_modes_body(const AdjStageArgs& A, const DevParams& P, int mode) {
+    mode = QLGPU_CHECK_INDEX(mode, P.nxy, A.status);
     using G = Geom<NZ>;
     using AG = AdjGeom<NZ>;
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(BatchOcc<MAXNZ>::MAX_THREADS, 1) batch_kernel(
             // all items of this CTA publish stage k before the CTA waits for any of them
             for (int i = 0; i < nitems; ++i) {
                 const BatchSlot it = s_items[i];
-                const BatchCase* cs = L.cases + it.c;
+                const BatchCase* cs = L.cases + QLGPU_CHECK_INDEX(it.c, L.ncases, &L.ctl->status);
                 bool top = false;
                 if (it.NZ == 16) {
                     top = batch_item_stage<16, MODEL, INTEG, MAXNZ>(cs, s, swap, it.cta, it.ncta, tmem, n);

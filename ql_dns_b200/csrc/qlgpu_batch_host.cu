@@ -40,6 +40,7 @@
 #include "../../include/qlgpu.h"
 #include "qlgpu_batch_internal.h"
 #include "qlgpu_ens_host.h"
+#include "qlgpu_guard.h"
 #include "qlgpu_host.h"
 #include "qlgpu_kernel.cuh"
 
@@ -80,6 +81,7 @@ struct CaseHost {
     cplx *rec_lin = nullptr, *rec_mf = nullptr;
     double *rec_kx = nullptr, *rec_t = nullptr;
     CnRec* rec_cn = nullptr;
+    bool noise_on = false;  // driving noise after every step (qlgpu_batch_set_noise)
 };
 
 // One work item of the planner: CTA number i of the k given to case c.
@@ -211,6 +213,8 @@ struct qlgpu_batch {
     unsigned long long* d_qtrace = nullptr;  // [grid][4] per-CTA time sums of the last queue launch (QLGPU_TRACE=1)
     int* d_flags = nullptr;                  // [ncases] per-case flags of set_states
     double* d_tvec = nullptr;                // [ncases] clock times of get_states
+    NoiseSpec* d_noise = nullptr;            // [ncases] driving-noise constants
+    GuardList guards;                        // debug build: canary zones after the device buffers
 };
 
 namespace {
@@ -229,6 +233,8 @@ int bfail(qlgpu_batch_t* b, int code, const std::string& msg) {
     } while (0)
 
 size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+// one arena slot: the buffer and, in the debug build, its guard zone
+size_t gslot(size_t x) { return al256(x + QLGPU_GUARD_BYTES); }
 
 int modes_per_cta(int warps, int T) { return warps * (32 / T) / 2; }
 
@@ -381,6 +387,7 @@ int upload_descriptors(qlgpu_batch_t* b) {
             A.diag_cap = h.diag_cap;
             A.mfr_cache = h.mfr;
             A.ekz_tab = h.ekz + (size_t)s * 2 * h.nz;
+            A.noise = (s == 2 && h.noise_on) ? b->d_noise + c : nullptr;
             A.sc = h.sc[s];
         }
         d.kx_init = h.kx_init;
@@ -533,6 +540,7 @@ cudaError_t enqueue_queue(qlgpu_batch_t* b, int nsteps, int reset_ndiag) {
     L.R = (int)b->round.size();
     L.nrounds = 3 * nsteps;
     L.parity = b->cur;
+    L.ncases = b->ncases;
     L.wait_ns = b->wait_ns;
     L.trace = b->d_qtrace;
     if (b->d_qtrace) {
@@ -553,6 +561,7 @@ BatchLaunch launch_args(qlgpu_batch_t* b, int nsteps) {
     L.nsteps = nsteps;
     L.parity = b->cur;
     L.wait_ns = b->wait_ns;
+    L.ncases = b->ncases;
     return L;
 }
 
@@ -616,6 +625,31 @@ int run_launch(qlgpu_batch_t* b, int nsteps, int reset_ndiag, cudaEvent_t ev_bef
     return QLGPU_OK;
 }
 
+// Debug build: after a launch, the index checks' bit in the launch status and in every case's
+// status word, and the guard zones after every buffer.  A release build returns at once.
+int debug_verify(qlgpu_batch_t* b) {
+#ifdef QLGPU_DEBUG
+    const int nc = b->ncases;
+    std::vector<int> col(2 * (size_t)nc + 2);
+    batch_collect_kernel<<<(nc + 127) / 128, 128, 0, b->stream>>>(b->d_cases, nc, b->d_ctl, b->d_collect);
+    QB_CK(cudaGetLastError());
+    QB_CK(cudaMemcpyAsync(col.data(), b->d_collect, col.size() * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    int g = 0;
+    QB_CK(guard_check(b->guards, b->stream, &g));
+    int st = g | (col[2 * nc] & QLGPU_STATUS_BOUNDS);
+    for (int c = 0; c < nc; ++c) st |= col[2 * c] & QLGPU_STATUS_BOUNDS;
+    if (st) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "debug build: device status 0x%x (%s)", st,
+                      (st & QLGPU_STATUS_BOUNDS) ? "an index check failed" : "a guard zone was overwritten");
+        return bfail(b, QLGPU_ERR_STATUS, buf);
+    }
+#else
+    (void)b;
+#endif
+    return QLGPU_OK;
+}
+
 int check_launch_status(qlgpu_batch_t* b) {
     BatchCtl ctl;
     QB_CK(cudaMemcpyAsync(&ctl, b->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, b->stream));
@@ -629,7 +663,7 @@ int check_launch_status(qlgpu_batch_t* b) {
                       b->wait_ns * 1e-9);
         return bfail(b, QLGPU_ERR_STATUS, buf);
     }
-    return QLGPU_OK;
+    return debug_verify(b);
 }
 
 int reset_case_clock(qlgpu_batch_t* b, int c, double t) {
@@ -657,11 +691,13 @@ int qlgpu_batch_destroy(qlgpu_batch_t* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
     void* bufs[] = {b->arena,   b->d_cases, b->d_ctas, b->d_epoch, b->d_ctl, b->d_case_end, b->d_collect,
-                    b->d_out15, b->d_diag,  b->d_ec,   b->d_round, b->d_tw8, b->d_qtrace, b->d_flags, b->d_tvec};
+                    b->d_out15, b->d_diag,  b->d_ec,   b->d_round, b->d_tw8, b->d_qtrace, b->d_flags, b->d_tvec,
+                    b->d_noise};
     for (void* p : bufs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : b->ev)
         if (e) cudaEventDestroy(e);
+    guard_release(b->guards);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return QLGPU_OK;
@@ -746,17 +782,17 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
         }
         const size_t nlin = (size_t)h.nxy * 4 * h.nz, nmfe = (size_t)h.nmf * h.nz;
         off[c] = o;
-        o += 4 * al256(nlin * sizeof(cplx));                       // lin[2], F1, F2
-        o += 3 * al256(nmfe * sizeof(cplx));                       // mf, Fmf1, Fmf2
-        o += 3 * al256(h.nxy * sizeof(double));                    // kx0, ky, kx_init
-        o += 2 * al256(h.nxy * sizeof(int));                       // kxi, kyi
-        o += al256(h.NZ * sizeof(cplx));                           // twiddles
-        o += al256((size_t)(h.p.ny / 2) * h.nz * sizeof(double));  // 1/lap2
-        o += al256((size_t)h.max_cta * h.PL * sizeof(double));     // partials
-        o += al256((size_t)((h.max_cta + RED_GROUP - 1) / RED_GROUP) * h.PL * sizeof(double));
-        o += al256(sizeof(DevClock));
-        o += al256((size_t)8 * h.NZ * sizeof(double));  // mean-field profile cache
-        o += al256((size_t)6 * h.nz * sizeof(double));  // integrating-factor tables
+        o += 4 * gslot(nlin * sizeof(cplx));                       // lin[2], F1, F2
+        o += 3 * gslot(nmfe * sizeof(cplx));                       // mf, Fmf1, Fmf2
+        o += 3 * gslot(h.nxy * sizeof(double));                    // kx0, ky, kx_init
+        o += 2 * gslot(h.nxy * sizeof(int));                       // kxi, kyi
+        o += gslot(h.NZ * sizeof(cplx));                           // twiddles
+        o += gslot((size_t)(h.p.ny / 2) * h.nz * sizeof(double));  // 1/lap2
+        o += gslot((size_t)h.max_cta * h.PL * sizeof(double));     // partials
+        o += gslot((size_t)((h.max_cta + RED_GROUP - 1) / RED_GROUP) * h.PL * sizeof(double));
+        o += gslot(sizeof(DevClock));
+        o += gslot((size_t)8 * h.NZ * sizeof(double));  // mean-field profile cache
+        o += gslot((size_t)6 * h.nz * sizeof(double));  // integrating-factor tables
     }
     b->arena_bytes = o;
     if (cudaMalloc(&b->arena, o) != cudaSuccess) {
@@ -770,7 +806,8 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
         const size_t nlin = (size_t)h.nxy * 4 * h.nz, nmfe = (size_t)h.nmf * h.nz;
         auto take = [&](size_t bytes) {
             unsigned char* r = p;
-            p += al256(bytes);
+            p += gslot(bytes);
+            guard_add(b->guards, r, bytes);
             return r;
         };
         h.lin[0] = reinterpret_cast<cplx*>(take(nlin * sizeof(cplx)));
@@ -815,11 +852,12 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
             return bail(QLGPU_ERR_CUDA);
         }
     }
-#define QB_ALLOC(ptr, bytes)                          \
-    if (cudaMalloc(&(ptr), (bytes)) != cudaSuccess) { \
-        b->err = "cudaMalloc failed for " #ptr;       \
-        return bail(QLGPU_ERR_CUDA);                  \
-    }                                                 \
+#define QB_ALLOC(ptr, bytes)                                              \
+    if (cudaMalloc(&(ptr), (bytes) + QLGPU_GUARD_BYTES) != cudaSuccess) { \
+        b->err = "cudaMalloc failed for " #ptr;                           \
+        return bail(QLGPU_ERR_CUDA);                                      \
+    }                                                                     \
+    guard_add(b->guards, (ptr), (bytes));                                 \
     cudaMemsetAsync((ptr), 0, (bytes), b->stream);
     QB_ALLOC(b->d_cases, sizeof(BatchCase) * ncases);
     QB_ALLOC(b->d_ctas, sizeof(BatchCta) * (size_t)max_grid);
@@ -831,8 +869,13 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
     QB_ALLOC(b->d_ec, sizeof(ens::EnsCase) * ncases);
     QB_ALLOC(b->d_flags, sizeof(int) * ncases);
     QB_ALLOC(b->d_tvec, sizeof(double) * ncases);
+    QB_ALLOC(b->d_noise, sizeof(NoiseSpec) * ncases);
     QB_ALLOC(b->d_tw8, sizeof(cplx) * 240);
 #undef QB_ALLOC
+    if (guard_arm(b->guards, b->stream) != cudaSuccess) {
+        b->err = "guard zones";
+        return bail(QLGPU_ERR_CUDA);
+    }
     {
         // 8-point twiddles of the queue engine, tw[q T + t] = exp(2 pi i q t / NZ), T = NZ / 8
         std::vector<double> tw8(480, 0.0);
@@ -1048,7 +1091,7 @@ int qlgpu_batch_step(qlgpu_batch_t* b, int nsteps, int diag_every, double* diag_
                       col[2 * bad]);
         return bfail(b, QLGPU_ERR_STATUS, buf);
     }
-    return QLGPU_OK;
+    return debug_verify(b);
 }
 
 int qlgpu_batch_step_timed(qlgpu_batch_t* b, int nsteps, float* ms) {
@@ -1497,3 +1540,35 @@ int qlgpu_batch_set_record(qlgpu_batch_t* b, int c, cplx* rec_lin, cplx* rec_mf,
 }
 
 cudaStream_t qlgpu_batch_cuda_stream(qlgpu_batch_t* b) { return b ? b->stream : nullptr; }
+
+int qlgpu_batch_debug_guard_poke(qlgpu_batch_t* b, int zone) {
+    if (!b) return QLGPU_ERR_ARG;
+    if (!QLGPU_DEBUG_BUILD) return bfail(b, QLGPU_ERR_UNSUPPORTED, "guard zones exist in the debug build only");
+    if (zone < 0 || zone >= (int)b->guards.zones.size()) return bfail(b, QLGPU_ERR_ARG, "no such guard zone");
+    QB_CK(cudaSetDevice(b->device));
+    QB_CK(guard_poke(b->guards, zone, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_set_noise(qlgpu_batch_t* b, int c, double f_noise, double k_low, double k_high,
+                          unsigned long long seed, int drive_only_velocity, int drive_only_magnetic) {
+    if (!b) return QLGPU_ERR_ARG;
+    if (c < 0 || c >= b->ncases) return bfail(b, QLGPU_ERR_ARG, "case index out of range");
+    if (!std::isfinite(f_noise) || !(k_low >= 0) || !(k_high >= k_low))
+        return bfail(b, QLGPU_ERR_ARG, "noise: finite f_noise, 0 <= k_low <= k_high");
+    CaseHost& h = b->cs[c];
+    if ((drive_only_velocity || drive_only_magnetic) && h.p.model != QLGPU_MODEL_MHD_FULLQLIN)
+        return bfail(b, QLGPU_ERR_UNSUPPORTED, "drive_only_velocity / drive_only_magnetic are MHD_FullQlin inputs");
+    QB_CK(cudaSetDevice(b->device));
+    const NoiseSpec ns = noise_spec(h.p, h.NZ, h.p.dt, f_noise, k_low, k_high, seed, drive_only_velocity != 0,
+                                    drive_only_magnetic != 0);
+    QB_CK(cudaMemcpyAsync(b->d_noise + c, &ns, sizeof(ns), cudaMemcpyHostToDevice, b->stream));
+    QB_CK(cudaStreamSynchronize(b->stream));
+    const bool on = f_noise != 0.0;
+    if (on != h.noise_on) {
+        h.noise_on = on;
+        b->descr_dirty = true;
+    }
+    return QLGPU_OK;
+}

@@ -15,6 +15,7 @@
 #include "../../include/qlgpu.h"
 #include "../../include/qlgpu_dns.h"
 #include "qlgpu_dns.cuh"
+#include "qlgpu_guard.h"
 #include "qlgpu_host.h"
 
 using namespace qlgpu;
@@ -81,6 +82,7 @@ struct qlgpu_dns {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     std::vector<double> kx_tab;
     std::string err;
+    qlgpu::GuardList guards;  // debug build: canary zones after the device buffers
 };
 
 static int fail(qlgpu_dns* h, int code, const std::string& msg) {
@@ -110,6 +112,7 @@ static void release(qlgpu_dns* h) {
         if (b) cudaFree(b);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
+    guard_release(h->guards);
     if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -228,10 +231,11 @@ int qlgpu_dns_create(const qlgpu_dns_params* p, int device, qlgpu_dns_t** out) {
     const size_t plane = (size_t)h->Kyn * p->Mx * p->NZ;
     auto alloc = [&](void** ptr, size_t bytes) { return cudaMalloc(ptr, bytes); };
     int rc = QLGPU_OK;
-#define DNS_AL(ptr, bytes)                                                   \
-    if (rc == QLGPU_OK) {                                                    \
-        cudaError_t e2 = alloc((void**)&(ptr), (bytes));                     \
-        if (e2 != cudaSuccess) rc = cuda_fail(h, e2, "cudaMalloc " #ptr);    \
+#define DNS_AL(ptr, bytes)                                                         \
+    if (rc == QLGPU_OK) {                                                          \
+        cudaError_t e2 = alloc((void**)&(ptr), (bytes) + QLGPU_GUARD_BYTES);       \
+        if (e2 != cudaSuccess) rc = cuda_fail(h, e2, "cudaMalloc " #ptr);          \
+        else guard_add(h->guards, (ptr), (bytes));                                 \
     }
     DNS_AL(a.lin, ns * sizeof(cplx));
     DNS_AL(a.F[0], ns * sizeof(cplx));
@@ -272,6 +276,7 @@ int qlgpu_dns_create(const qlgpu_dns_params* p, int device, qlgpu_dns_t** out) {
         if (e3 == cudaSuccess) e3 = ensure_smem_attr((const void*)h->k_phys, h->s_phys);
         if (e3 == cudaSuccess) e3 = cudaEventCreate(&h->ev[0]);
         if (e3 == cudaSuccess) e3 = cudaEventCreate(&h->ev[1]);
+        if (e3 == cudaSuccess) e3 = guard_arm(h->guards, h->stream);
         if (e3 != cudaSuccess) rc = cuda_fail(h, e3, "dns setup");
     }
     if (rc != QLGPU_OK) {
@@ -372,10 +377,18 @@ static int launch_steps(qlgpu_dns* h, int nsteps) {
     return QLGPU_OK;
 }
 
+// The status word after a call's launches (bit 1: non-finite state); in the debug build also
+// the index checks' bit and the guard zones after every buffer.
 static int check_status(qlgpu_dns* h) {
-    int st = 0;
+    int st = 0, g = 0;
     DNS_CK(h, cudaMemcpyAsync(&st, h->a.status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     DNS_CK(h, cudaStreamSynchronize(h->stream));
+    DNS_CK(h, guard_check(h->guards, h->stream, &g));
+    st |= g;
+    if (st & (QLGPU_STATUS_BOUNDS | QLGPU_STATUS_CANARY))
+        return fail(h, QLGPU_ERR_STATUS,
+                    (st & QLGPU_STATUS_BOUNDS) ? "debug build: an index check failed"
+                                               : "debug build: a guard zone was overwritten");
     if (st) return fail(h, QLGPU_ERR_STATUS, "non-finite DNS state");
     return QLGPU_OK;
 }
@@ -442,7 +455,7 @@ int qlgpu_dns_rhs(qlgpu_dns_t* h, double t, double* F) {
     const size_t ns = (size_t)h->nxy * 6 * h->nz;
     DNS_CK(h, cudaMemcpyAsync(F, h->a.F[0], ns * sizeof(cplx), cudaMemcpyDeviceToHost, h->stream));
     DNS_CK(h, cudaStreamSynchronize(h->stream));
-    return QLGPU_OK;
+    return QLGPU_DEBUG_BUILD ? check_status(h) : QLGPU_OK;
 }
 
 int qlgpu_dns_status(qlgpu_dns_t* h, int* status) {

@@ -21,6 +21,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "qlgpu_debug.cuh"
 #include "qlgpu_fft.cuh"
 
 namespace qlgpu {
@@ -99,7 +100,7 @@ __global__ void __launch_bounds__(BLOCK, 2) dns_inv_zx(DnsArgs a) {
     const int ky = blockIdx.x, f = blockIdx.y, tid = threadIdx.x;
     for (int b = tid; b < MX; b += BLOCK) bin2col[b] = -1;
     __syncthreads();
-    for (int c = tid; c < a.ncol; c += BLOCK) bin2col[xbin(a.kx0[ky + a.Kyn * c], a.dkx, MX)] = c;
+    for (int c = tid; c < a.ncol; c += BLOCK) bin2col[QLGPU_CHECK_INDEX(xbin(a.kx0[QLGPU_CHECK_INDEX(ky + a.Kyn * c, a.nxy, a.status)], a.dkx, MX), MX, a.status)] = c;
     __syncthreads();
     {  // z inverse of every column of the plane
         constexpr int T = GZ::T, NG = BLOCK / T;
@@ -107,11 +108,11 @@ __global__ void __launch_bounds__(BLOCK, 2) dns_inv_zx(DnsArgs a) {
         const unsigned gm = group_mask(T);
         cplx* xg = xch + g * GZ::XSIZE;
         for (int c = g; c < a.ncol; c += NG) {
-            const cplx* src = a.lin + ((size_t)(ky + a.Kyn * c) * 6 + f) * a.nz;
+            const cplx* src = a.lin + ((size_t)QLGPU_CHECK_INDEX(ky + a.Kyn * c, a.nxy, a.status) * 6 + f) * a.nz;
             cplx x[GZ::P];
 #pragma unroll
             for (int k2 = 0; k2 < GZ::P; ++k2) {
-                const int s = stored_index<GZ>(t + T * k2);
+                const int s = QLGPU_CHECK_STORED(stored_index<GZ>(t + T * k2), a.nz, a.status);
                 x[k2] = s >= 0 ? cscale(src[s], a.scale) : mk(0.0, 0.0);
             }
             inv_fft<GZ>(x, xg, a.twz, t, gm);
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__(BLOCK, 2) dns_fwd_xz(DnsArgs a) {
     for (int b = tid; b < MX; b += BLOCK) bin2col[b] = -1;
     const cplx* src = a.P + ((size_t)p * a.Kyn + ky) * MX * NZ;
     __syncthreads();
-    for (int c = tid; c < a.ncol; c += BLOCK) bin2col[xbin(a.kx0[ky + a.Kyn * c], a.dkx, MX)] = c;
+    for (int c = tid; c < a.ncol; c += BLOCK) bin2col[QLGPU_CHECK_INDEX(xbin(a.kx0[QLGPU_CHECK_INDEX(ky + a.Kyn * c, a.nxy, a.status)], a.dkx, MX), MX, a.status)] = c;
     __syncthreads();
     {  // x forward of every z row (loads: consecutive z per warp, whole sectors), kept at
        // the plane's column bins
@@ -311,10 +312,10 @@ __global__ void __launch_bounds__(BLOCK, 2) dns_fwd_xz(DnsArgs a) {
 #pragma unroll
             for (int j = 0; j < GZ::P; ++j) x[j] = S[c * K::SROW + zpos<GZ>(t, j)];
             fwd_fft<GZ>(x, xg, a.twz, t, gm);
-            cplx* dst = a.T + ((size_t)p * a.nxy + (ky + a.Kyn * c)) * a.nz;
+            cplx* dst = a.T + ((size_t)p * a.nxy + QLGPU_CHECK_INDEX(ky + a.Kyn * c, a.nxy, a.status)) * a.nz;
 #pragma unroll
             for (int k2 = 0; k2 < GZ::P; ++k2) {
-                const int s = stored_index<GZ>(t + T * k2);
+                const int s = QLGPU_CHECK_STORED(stored_index<GZ>(t + T * k2), a.nz, a.status);
                 if (s >= 0) dst[s] = x[k2];
             }
         }

@@ -49,6 +49,7 @@
 #include <type_traits>
 
 #include "qlgpu_batch.cuh"
+#include "qlgpu_debug.cuh"
 
 namespace qlgpu {
 namespace ens {
@@ -161,6 +162,13 @@ __device__ __forceinline__ void xform(cplx (&x)[8], cplx* xg, const cplx* tw, in
     __syncwarp();
 }
 
+// A store of the new state or right-hand side: read again one stage later, after
+// the whole ensemble has streamed through L2, so it is marked evict-first
+// (st.global.cs) and leaves L2 to the prefetched fields of the next modes.
+__device__ __forceinline__ void st_stream(cplx* p, cplx v) {
+    __stcs(reinterpret_cast<double2*>(p), make_double2(v.x, v.y));
+}
+
 // ---------------------------------------------------------------------------
 // Tensor-memory scratchpad of one thread: Ex (16 columns), Ey (16), S (32).
 // ---------------------------------------------------------------------------
@@ -267,6 +275,7 @@ struct ChunkHdr {
     StageArgs A;
     // constants of the chunk's stage from the case's clock (thread 0, after the header)
     double tclock, t_new, qt, ts, Om2, cn_t_old, cn_dtlin_old;
+    unsigned long long nstep;  // the step's noise counter (driven cases)
     int cn_old_init, diag_due, has_prev, pad2;
     int c, r, ok, top;
     unsigned tk;
@@ -302,19 +311,20 @@ __device__ __noinline__ void top_stage(const EnsLaunch& L, ChunkHdr& hd, int c, 
     double* spec = tot + ((E::PL + 1) & ~1);   // [2 NEMF (H+1)]
     cplx* xo = reinterpret_cast<cplx*>(spec + ((2 * NEMF * (G::H + 1) + 1) & ~1));
     double* mfr = reinterpret_cast<double*>(xo + 3 * G::XSIZE);
+    // chunk slots in slot order; 32 loads in flight per thread (this sum is on the case's
+    // critical path: every CTA waits for the stage it releases)
+    constexpr int U = 32;
     for (int idx = tid; idx < E::PL; idx += THREADS) {
         const double* src = hd.A.partials + idx;
         double sum = 0.0;
-        int jj = 0;
-        for (; jj + 4 <= nch; jj += 4) {
-            const double v0 = __ldcg(src + (size_t)(jj + 0) * E::PL), v1 = __ldcg(src + (size_t)(jj + 1) * E::PL);
-            const double v2 = __ldcg(src + (size_t)(jj + 2) * E::PL), v3 = __ldcg(src + (size_t)(jj + 3) * E::PL);
-            sum += v0;
-            sum += v1;
-            sum += v2;
-            sum += v3;
+        for (int jj = 0; jj < nch; jj += U) {
+            double v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) v[u] = jj + u < nch ? __ldcg(src + (size_t)(jj + u) * E::PL) : 0.0;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (jj + u < nch) sum += v[u];
         }
-        for (; jj < nch; ++jj) sum += __ldcg(src + (size_t)jj * E::PL);
         tot[idx] = sum;
     }
     __syncthreads();
@@ -361,7 +371,7 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
     cplx* stg = Kw + E::K_CPLX + (size_t)pi * 4 * E::nz;           // this pair's staged fields
     cplx* xg = Kw + E::K_CPLX + E::STG_CPLX;                        // this warp's exchange buffers
     uint64_t* bar = bars + warp * MAX_PAIRS_PER_WARP + pi;
-    const int c = it.c, j = it.j;
+    const int c = it.c, j = QLGPU_CHECK_INDEX(it.j, L.ec[it.c].nch, &L.ctl->status);
     const BatchCase* cs = L.cases + c;
     const EnsCase ec = L.ec[c];
     const int s = r % 3, n = r / 3;
@@ -429,6 +439,7 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         hd.ts = __dadd_rn(tc, S.t_off);
         hd.Om2 = __dmul_rn(2.0, P.Omega);
         hd.has_prev = (S.has_prev && A.Fprev) ? 1 : 0;
+        hd.nstep = A.noise ? __ldcg(&A.clk->nstep) : 0ull;
     }
     // ---- tables of the case and stage
     if (fresh) {
@@ -486,7 +497,7 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
     for (int wb = first; wb < mend; wb += MPP) {  // warp-uniform
         const int mraw = wb + pi;
         const bool valid = mraw < mend;
-        m = valid ? mraw : mend - 1;
+        m = QLGPU_CHECK_INDEX(valid ? mraw : mend - 1, P.nxy, &L.ctl->status);
         // L2 prefetch of the pair's next mode (fields and previous right-hand side)
         if (leader && mraw + MPP < mend) {
             l2_prefetch(lin_in + (size_t)(mraw + MPP) * 4 * nzd, fbytes);
@@ -508,11 +519,8 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         const double mult = valid ? ((ky == 0.0) ? 1.0 : 2.0) : 0.0;
         const double kxe = __dadd_rn(a, __dmul_rn(__dmul_rn(P.q, S.dt_lin), ky));
         const double hxy = __dsub_rn(-__dmul_rn(kxe, kxe), __dmul_rn(ky, ky));
-        double em_u = 1.0, em_b = 1.0, kxo = 0.0;
-        if (INTEG == INTEG_EXP) {
-            em_u = exp(S.linC * P.nu * hxy);
-            em_b = exp(S.linC * P.cb * hxy);
-        } else {
+        double kxo = 0.0;  // CN: kx at the old operator's time
+        if (INTEG == INTEG_CN) {
             if (hd.cn_old_init) kxo = kx_at(kx0, P.q, tclock, ky);
             else kxo = __dadd_rn(kx_at(kx0, P.q, hd.cn_t_old, ky), __dmul_rn(__dmul_rn(P.q, hd.cn_dtlin_old), ky));
         }
@@ -549,9 +557,18 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
             }
         };
         // RK update of one field from F in registers (F_out / lin_out stores)
-        auto update = [&](int f, const cplx (&F)[8], int rr, int sx, double em, const double* ekzt) {
+        // the previous right-hand side of field f at this lane's 8 entries, loaded together before an
+        // update loop (one L2 round trip instead of one per entry: the loop's stores would order them)
+        auto load_fp = [&](int f, cplx (&fpv)[8]) {
+#pragma unroll
+            for (int rr = 0; rr < 8; ++rr) {
+                const int sx = sidx<E>(t, rr);
+                fpv[rr] = (fpm && !rdead<E>(rr) && sx >= 0) ? ldc(fpm + f * nzd + sx) : mk(0.0, 0.0);
+            }
+        };
+        auto update = [&](int f, const cplx (&F)[8], int rr, int sx, double em, const double* ekzt, cplx fp) {
+            sx = QLGPU_CHECK_INDEX(sx, nzd, &L.ctl->status);
             const cplx uin = stg[f * nzd + sx];
-            const cplx fp = fpm ? ldc(fpm + f * nzd + sx) : mk(0.0, 0.0);
             cplx nv;
             if (INTEG == INTEG_EXP) {
                 const double e = em * ekzt[sx];
@@ -567,8 +584,8 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
                                                  : lap_end<MODEL_BQLIN>(P, kxo, ky, kz2);
                 nv = rk_update<INTEG_CN>(S, L, linop_f<MODEL_BQLIN>(P, lo, f), F[rr], fp, uin, fpm != nullptr);
             }
-            if (fo) stc(fo + f * nzd + sx, F[rr]);
-            stc(uo + f * nzd + sx, zero ? mk(0.0, 0.0) : nv);
+            if (fo) st_stream(fo + f * nzd + sx, F[rr]);
+            st_stream(uo + f * nzd + sx, zero ? mk(0.0, 0.0) : nv);
         };
 
         // ---- slot 1: z-components R_uz / R_bz -> K: (a c f0 - i b f1) il2 / NZ (MHD_BQlin.cpp:144-146)
@@ -624,16 +641,8 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
             xform<E>(x, xg, tw, g, t);
 #pragma unroll
             for (int rr = 0; rr < 8; ++rr) x[rr] = conjc(x[rr]);
-            tm_st4c(ta + TM_S, x);  // S (B); the U lanes' copy is never read
+            tm_st4c(ta + TM_S, x);  // S (B) / F_b (U), read in slot 7 and the update phase
             tm_st4c(ta + TM_S + 16, x + 4);
-            if (role == 0 && valid) {
-#pragma unroll
-                for (int rr = 0; rr < 8; ++rr) {
-                    if (rdead<E>(rr)) continue;
-                    const int sx = sidx<E>(t, rr);
-                    if (sx >= 0) update(2, x, rr, sx, em_b, ekz_b);
-                }
-            }
         }
         // ---- slot 4: R_zeta / R_eta: acc += i b By R
         {
@@ -701,7 +710,6 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         // ---- slot 6: forward -> F_eta (U) / F_zeta (B)
         {
             xform<E>(x, xg, tw, g, t);
-            const int f = role ? 1 : 3;
             const int fl = role ? 0 : 2;           // linear term field
             const double cl = role ? (P.q - Om2) : -P.q;
             if (valid) {
@@ -715,13 +723,9 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
                     const cplx F = conjc(x[rr]);
                     x[rr] = cadd(F, imul(l0, cl * cc));
                 }
-#pragma unroll
-                for (int rr = 0; rr < 8; ++rr) {
-                    if (rdead<E>(rr)) continue;
-                    const int sx = sidx<E>(t, rr);
-                    if (sx >= 0) update(f, x, rr, sx, role ? em_u : em_b, role ? ekz_u : ekz_b);
-                }
             }
+            tm_st4c(ta + TM_ACC, x);  // F_eta (U) / F_zeta (B) until the update phase; acc is dead here
+            tm_st4c(ta + TM_ACC + 16, x + 4);
         }
         // ---- slot 7: U inverse R_uy (Ey); B forward 2 kx ky dBy KB -> F_u
         {
@@ -781,11 +785,52 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
                         const cplx F = conjc(x[rr]);
                         const cplx lin = cadd(cadd(F, cscale(u0, rl)), imul(z1, Om2 * cc));
                         x[rr] = cadd(sv[i], cscale(lin, ilapF));
-                        update(0, x, rr, sx, em_u, ekz_u);
                     }
                 }
             }
             tm_st8d(ta + TM_EY, ey);
+        }
+        // ---- RK updates of the mode's four fields (RK3CN_Elin.cpp:102-104, RK3CN.cpp:105-107) in one
+        // phase after the transforms: U updates b (F in TM_S) and eta (TM_ACC), B updates u (registers)
+        // and zeta (TM_ACC).  A field's previous right-hand side is loaded as one batch of eight
+        // entries per lane, the second field's after the first is stored (fewer live registers).
+        {
+            const int fs = role ? 0 : 2, fa = role ? 1 : 3;
+            const double* ekzt = role ? ekz_u : ekz_b;
+            cplx fpv[8];
+            if (valid) load_fp(fs, fpv);
+            // the integrating factor of the role's fields, computed while the loads are in flight
+            const double em = (INTEG == INTEG_EXP) ? exp(S.linC * (role ? P.nu : P.cb) * hxy) : 1.0;
+            tm_wait_st();  // F (slot 6) is stored before it is read back
+            {
+                cplx FS[8];
+                tm_ld8c(ta + TM_S, FS);
+                if (role) {
+#pragma unroll
+                    for (int rr = 0; rr < 8; ++rr) FS[rr] = x[rr];
+                }
+                if (valid) {
+#pragma unroll
+                    for (int rr = 0; rr < 8; ++rr) {
+                        if (rdead<E>(rr)) continue;
+                        const int sx = sidx<E>(t, rr);
+                        if (sx >= 0) update(fs, FS, rr, sx, em, ekzt, fpv[rr]);
+                    }
+                }
+            }
+            if (valid) load_fp(fa, fpv);
+            {
+                cplx FA[8];
+                tm_ld8c(ta + TM_ACC, FA);
+                if (valid) {
+#pragma unroll
+                    for (int rr = 0; rr < 8; ++rr) {
+                        if (rdead<E>(rr)) continue;
+                        const int sx = sidx<E>(t, rr);
+                        if (sx >= 0) update(fa, FA, rr, sx, em, ekzt, fpv[rr]);
+                    }
+                }
+            }
         }
         // ---- after the mode: remap bookkeeping, next mode's copy, diagnostics
         if (zero && valid && role == 0 && t == 0) A.kx0[m] = kx0;
@@ -798,6 +843,12 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         {
             const int wn = wb + MPP;
             if (leader && wn < mend) bulk_load(stg, lin_in + (size_t)min(wn + pi, mend - 1) * 4 * nzd, fbytes, bar);
+        }
+        if (A.noise) {
+            // Model::DrivingNoise after the step (main.cpp:111-113), before the diagnostics see it
+            if (valid && !zero)
+                noise_mode(A.noise, hd.nstep, uo, nzd, lp, 2 * T, m, kx0, ky, kxi, kyi, P.q, tclock, P.kzL);
+            __syncwarp();
         }
         if (diag_due && valid && !zero) {
             // Calc_Energy_AM_Diss per mode at t_new (MHD_BQlin.cpp:365-407): U sums the magnetic
@@ -962,7 +1013,8 @@ __global__ void __launch_bounds__(THREADS, 1) ens_kernel(const __grid_constant__
         const unsigned tk = hd.tk;
         if (tk >= total) break;
         const int r = (int)(tk / (unsigned)L.R);
-        const RoundItem it = L.round[tk % (unsigned)L.R];
+        RoundItem it = L.round[tk % (unsigned)L.R];
+        it.c = QLGPU_CHECK_INDEX(it.c, L.ncases, &L.ctl->status);
         const unsigned long long t1 = (L.trace && tid == 0) ? gtimer() : 0ull;
         switch (L.ec[it.c].NZ) {
             case 16: run_chunk<16, INTEG>(L, hd, it, r, tmem, bars, bar_ph); break;

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/qlgpu.h"
+#include "qlgpu_guard.h"
 #include "qlgpu_host.h"
 #include "qlgpu_types.h"
 
@@ -48,6 +49,8 @@ struct qlgpu_handle {
     int grid = 0, warps = 4, block = 128;
     size_t smem = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    qlgpu::GuardList guards;  // debug build: canary zones after the device buffers
+    int* d_dbg = nullptr;     // debug-build index checks of the adjoint kernels (the clock is restored there)
     std::vector<double> kx_tab, ky_tab;
     std::vector<int> kxi_tab, kyi_tab;
     std::vector<double> il2_tab, ekz_tab;
@@ -56,6 +59,7 @@ struct qlgpu_handle {
     // forcing (include/qlgpu.h: qlgpu_set_noise, qlgpu_set_cfl)
     double noise_f = 0.0, noise_klo = 0.0, noise_khi = 0.0;
     unsigned long long noise_seed = 0;
+    int noise_only_vel = 0, noise_only_mag = 0;  // MHD_FullQlin drive_only_* switches
     double cfl = 0.0, dt_max = 0.0;
     double dt_sum = 0.0;                 // Integrator::mean_time_step accumulators
     unsigned long long steps_taken = 0;  // since set_state; the noise counter's step word
@@ -68,3 +72,7 @@ struct qlgpu_handle {
 // One step of the handle's state on its stream (three stage launches); hook,
 // when set, runs on the host before each stage launch with the stage index.
 void qlgpu_enqueue_step(qlgpu_t* h, cudaEvent_t* ev, const std::function<void(int)>& hook);
+
+// Debug build: the index checks' status bits and the guard zones of the handle after a
+// call's launches (QLGPU_ERR_STATUS when one fired).  QLGPU_OK at once in a release build.
+int qlgpu_debug_verify(qlgpu_t* h);

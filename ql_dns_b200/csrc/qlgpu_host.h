@@ -268,6 +268,28 @@ inline std::vector<double> ekz_table(const qlgpu_params& p, const DevParams& d) 
     return e;
 }
 
+// Noise constants of a case stepping with dt (MHD_FullQlin.cpp:45-66,804;
+// MHD_BQlin.cpp:23-36,563): ky = 0 pairs are driven by MHD_FullQlin only.
+inline NoiseSpec noise_spec(const qlgpu_params& p, int NZ, double dt, double f_noise, double k_low, double k_high,
+                            unsigned long long seed, int only_velocity, int only_magnetic) {
+    NoiseSpec n;
+    std::memset(&n, 0, sizeof(n));
+    const int Ny = (p.ny / 2) * 2;
+    const double tot = (double)p.nx * (double)Ny * (double)NZ;
+    const double mult_noise_fac = (1.0 / (16 * 32 * 32)) * (1.0 / (16 * 32 * 32));
+    n.lo2 = k_low * k_low;
+    n.hi2 = k_high * k_high;
+    n.multfac = dt * (tot * tot) * mult_noise_fac;
+    n.sd = f_noise / std::sqrt(2.0);
+    n.seed = seed;
+    n.pair_ky0 = p.model == QLGPU_MODEL_MHD_FULLQLIN;
+    n.drive_u = !only_magnetic;
+    n.drive_b = !only_velocity;
+    n.nxh = p.nx / 2;
+    n.nyh = Ny / 2;
+    return n;
+}
+
 // Stage constants of RK3CN_Elin::Step / RK3CN::Step for stage s of a step
 // (RK3CN_Elin.cpp:89-91,122-125,155-158; RK3CN.cpp:92-94).
 inline StageConst stage_const(const qlgpu_params& p, int s) {

@@ -4,6 +4,8 @@
 #pragma once
 #include <type_traits>
 
+#include "qlgpu_debug.cuh"
+#include "qlgpu_noise.cuh"
 #include "qlgpu_stage.cuh"
 
 namespace qlgpu {
@@ -176,6 +178,7 @@ __device__ __forceinline__ void mean_field_stage(const StageArgs& A, const DevPa
     C->t = t_new;
     C->timevar = __dadd_rn(C->timevar, P.dt);
     C->since += 1;
+    C->nstep += 1;
     if (!diag_due) return;
     // Calc_Energy_AM_Diss (MHD_BQlin.cpp:408-477)
     double eMB = 0, aMB = 0, dMB = 0, eMU = 0, aMU = 0, dMU = 0;
@@ -201,7 +204,7 @@ __device__ __forceinline__ void mean_field_stage(const StageArgs& A, const DevPa
     const double du = ds[4] * P.divfac, db = ds[5] * P.divfac;
     const int r = C->ndiag;
     if (r < A.diag_cap) {
-        double* o = A.diag_ring + (size_t)r * 15;
+        double* o = A.diag_ring + (size_t)QLGPU_CHECK_INDEX(r, A.diag_cap, &C->status) * 15;
         o[0] = t_new;
         o[1] = eMU / 2; o[2] = eMB / 2; o[3] = eu / 2; o[4] = eb / 2;
         o[5] = aMU; o[6] = aMB; o[7] = au; o[8] = abv;
@@ -428,7 +431,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     for (int base = wglobal * PW; base < P.nxy; base += WG * PW) {
         const int mode_raw = base + pi;
         const bool valid = mode_raw < P.nxy;
-        const int mode = valid ? mode_raw : P.nxy - 1;
+        const int mode = QLGPU_CHECK_INDEX(valid ? mode_raw : P.nxy - 1, P.nxy, &A.clk->status);
         if (pf_lane && mode_raw + WG * PW < P.nxy) {
             l2_prefetch(A.lin_in + (size_t)(mode_raw + WG * PW) * 4 * P.nz, pf_bytes);
             if (pf_prev) l2_prefetch(pf_prev + (size_t)(mode_raw + WG * PW) * 4 * P.nz, pf_bytes);
@@ -477,6 +480,12 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
                     }
                     if (t == 0) A.kx0[mode] = kx0;
                 }
+            }
+            if (A.noise && !zeroed) {
+                // Model::DrivingNoise after the step (main.cpp:111-113), before the diagnostics see it
+                noise_mode(A.noise, __ldcg(&A.clk->nstep), A.lin_out + (size_t)mode * 4 * P.nz, P.nz, t, G::T,
+                           mode, kx0, ky, __ldg(A.kxi + mode), __ldg(A.kyi + mode), P.q, tclock, P.kzL);
+                __syncwarp(gmask);
             }
             if (diag_due && !zeroed)
                 mode_diag<G>(P, A.lin_out + (size_t)mode * 4 * P.nz, __ldg(A.kxi + mode), __ldg(A.kyi + mode), kx0,
@@ -547,7 +556,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     __syncthreads();
     if (tr) A.trace[3] = gtimer();
     const int ngroups = (ncta + RED_GROUP - 1) / RED_GROUP;
-    const int grp = cta / RED_GROUP;
+    const int grp = QLGPU_CHECK_INDEX(cta / RED_GROUP, 64, &A.clk->status);  // DevClock::cnt_group
     const int c0 = grp * RED_GROUP;
     const int cn_in = min(RED_GROUP, ncta - c0);
     if (tid == 0) {
@@ -561,12 +570,12 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     for (int idx = tid; idx < PL; idx += blockDim.x) {
         // CTAs in order; four loads in flight at a time
         double s = 0.0;
-        for (int c = 0; c < cn_in; c += 4) {
-            double v[4];
+        for (int c = 0; c < cn_in; c += 8) {
+            double v[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] = c + u < cn_in ? __ldcg(A.partials + (size_t)(c0 + c + u) * PL + idx) : 0.0;
+            for (int u = 0; u < 8; ++u) v[u] = c + u < cn_in ? __ldcg(A.partials + (size_t)(c0 + c + u) * PL + idx) : 0.0;
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < 8; ++u)
                 if (c + u < cn_in) s += v[u];
         }
         gpart[idx] = s;
@@ -583,12 +592,12 @@ __device__ __forceinline__ bool stage_body(const StageArgs& A, const DevParams& 
     __threadfence();
     for (int idx = tid; idx < PL; idx += blockDim.x) {
         double s = 0.0;
-        for (int g = 0; g < ngroups; g += 4) {
-            double v[4];
+        for (int g = 0; g < ngroups; g += 8) {
+            double v[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] = g + u < ngroups ? __ldcg(A.gpartials + (size_t)(g + u) * PL + idx) : 0.0;
+            for (int u = 0; u < 8; ++u) v[u] = g + u < ngroups ? __ldcg(A.gpartials + (size_t)(g + u) * PL + idx) : 0.0;
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < 8; ++u)
                 if (g + u < ngroups) s += v[u];
         }
         tot[idx] = s;

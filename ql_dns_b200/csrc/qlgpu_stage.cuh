@@ -16,6 +16,7 @@
 // that arrives last at the top performs the mean-field stage.  Everything is
 // FP64.
 #pragma once
+#include "qlgpu_debug.cuh"
 #include "qlgpu_fft.cuh"
 #include "qlgpu_priv.cuh"
 #include "qlgpu_types.h"
@@ -276,7 +277,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
 #pragma unroll
             for (int k2 = 0; k2 < Pn; ++k2) {
                 const int k = t + G::T * k2;
-                const int s = stored_index<G>(k);
+                const int s = QLGPU_CHECK_STORED(stored_index<G>(k), P.nz, &A.clk->status);
                 cplx v = mk(0.0, 0.0);
                 if (s >= 0 && kind != 4) {
                     const cplx g0 = ldu<STG>(p0 + s);
@@ -424,7 +425,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
             cplx uin[4], fpv[4], l0[4], l1[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                const int s = stored_index<G>(t + G::T * (4 * c4 + i));
+                const int s = QLGPU_CHECK_STORED(stored_index<G>(t + G::T * (4 * c4 + i)), P.nz, &A.clk->status);
                 const int sl = s < 0 ? 0 : s;
                 uin[i] = ldu<STG>(fin + sl);
                 fpv[i] = fpp ? ldc(fpp + sl) : mk(0.0, 0.0);
@@ -435,7 +436,7 @@ __device__ __forceinline__ void bqlin_pair(const StageArgs& A, const DevParams& 
             for (int i = 0; i < 4; ++i) {
                 const int k2 = 4 * c4 + i;
                 const int k = t + G::T * k2;
-                const int s = stored_index<G>(k);
+                const int s = QLGPU_CHECK_STORED(stored_index<G>(k), P.nz, &A.clk->status);
                 if (s < 0) continue;
                 const double c = kzval(kz_int<G>(k), P.kzL);
                 const double kz2 = kz2val(c);
@@ -588,7 +589,7 @@ __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParam
 #pragma unroll
             for (int k2 = 0; k2 < Pn; ++k2) {
                 const int k = t + G::T * k2;
-                const int s = stored_index<G>(k);
+                const int s = QLGPU_CHECK_STORED(stored_index<G>(k), P.nz, &A.clk->status);
                 cplx v = mk(0.0, 0.0);
                 if (s >= 0) {
                     const cplx g0 = ldu<STG>(p0 + s);
@@ -695,7 +696,7 @@ __device__ __forceinline__ void fullqlin_pair(const StageArgs& A, const DevParam
             for (int i = 0; i < 4; ++i) {
                 const int k2 = 4 * c4 + i;
                 const int k = t + G::T * k2;
-                const int s = stored_index<G>(k);
+                const int s = QLGPU_CHECK_STORED(stored_index<G>(k), P.nz, &A.clk->status);
                 if (s < 0) continue;
                 const double c = kzval(kz_int<G>(k), P.kzL);
                 const double kz2 = kz2val(c);

@@ -46,6 +46,20 @@ struct DevClock {
     unsigned cnt_top;
     int mfr_valid;     // mean-field profiles cache holds the current mean field
     unsigned cnt_group[64];
+    unsigned long long nstep;  // steps since the clock was set: the noise counter of the next step
+};
+
+// Driving noise of one case (Model::DrivingNoise, MHD_BQlin.cpp:558-618 and
+// MHD_FullQlin.cpp:786-1045), added to every mode after its last-stage update.
+struct NoiseSpec {
+    double lo2, hi2;     // noise_range_ bounds squared (MHD_FullQlin.cpp:51-52)
+    double multfac;      // dt (Nx Ny NZ)^2 mult_noise_fac_ (MHD_FullQlin.cpp:63-66,804)
+    double sd;           // f_noise/sqrt(2), the standard deviation of each part (:45)
+    unsigned long long seed;
+    int pair_ky0;        // MHD_FullQlin: ky = 0 modes driven in conjugate pairs (dont_drive_ky0_modes_ = 0)
+    int drive_u, drive_b;  // (u, zeta) / (b, eta) driven: !drive_only_magnetic / !drive_only_velocity (:21-22)
+    int nxh, nyh;        // Nx/2, Ny/2: the Kdata layout that locates a kx > 0 mode's kx < 0 partner
+    int pad;
 };
 
 // The Crank-Nicolson old-operator fields of a DevClock at a stage's start (the
@@ -99,6 +113,7 @@ struct StageArgs {
     double* rec_kx;
     double* rec_t;
     CnRec* rec_cn;          // the CN old-operator fields at the stage start (null: off)
+    const NoiseSpec* noise;  // last stage of a driven batch case: noise after each mode's update (null: off)
     StageConst sc;
 };
 
@@ -157,6 +172,8 @@ struct BatchLaunch {
     int nsteps;
     int parity;                    // 1: the first step starts from lin buffer 1
     long long wait_ns;             // bound on one wait for the other CTAs of a case
+    int ncases;
+    int pad;
 };
 
 // ---------------------------------------------------------------------------
@@ -186,7 +203,7 @@ struct EnsLaunch {
     int R;                   // items per round
     int nrounds;             // 3 K
     int parity;
-    int pad;
+    int ncases;
     long long wait_ns;
     unsigned long long* trace;  // optional [grid][4] %globaltimer sums: stage waits, chunks, mean-field stages, count
 };
@@ -199,3 +216,5 @@ struct EnsLaunch {
 #define QLGPU_STATUS_UNSTABLE 2    // |mean field| > 1e20 (solution.cpp:184)
 #define QLGPU_STATUS_DIAG_FULL 4   // diagnostic ring overflowed (records dropped)
 #define QLGPU_STATUS_TIMEOUT 8     // batch: a CTA gave up waiting for the other CTAs of its case
+#define QLGPU_STATUS_BOUNDS 16     // debug build: a device index check failed (the access was redirected)
+#define QLGPU_STATUS_CANARY 32     // debug build: a guard zone after a device buffer was overwritten

@@ -99,9 +99,13 @@ class QLSolver:
         _capi.check(self.L.qlgpu_step(self.h, int(nsteps), 0, None, 0, None), self.h)
         return np.zeros((0, 15))
 
-    def set_noise(self, f_noise: float, k_low: float, k_high: float, seed: int = 0):
-        """Model::DrivingNoise after every step (MHD_BQlin); f_noise = 0 turns it off."""
+    def set_noise(self, f_noise: float, k_low: float, k_high: float, seed: int = 0,
+                  drive_only_velocity: bool = False, drive_only_magnetic: bool = False):
+        """Model::DrivingNoise after every step; f_noise = 0 turns it off.  MHD_FullQlin also
+        drives ky = 0 modes in conjugate pairs and takes the drive_only_* switches."""
         _capi.check(self.L.qlgpu_set_noise(self.h, float(f_noise), float(k_low), float(k_high), int(seed)), self.h)
+        _capi.check(self.L.qlgpu_set_noise_fields(self.h, int(bool(drive_only_velocity)),
+                                                  int(bool(drive_only_magnetic))), self.h)
 
     def set_cfl(self, cfl: float, dt_max: float = 0.0):
         """Variable dt = cfl / Calculate_CFL capped at dt_max (cfl = 0: fixed dt)."""

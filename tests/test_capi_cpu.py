@@ -73,3 +73,14 @@ def test_invalid_parameters_rejected_before_device():
     for bad, code in ((dict(NZ=48), 2), (dict(nx=7), 1), (dict(dt=-0.1), 2), (dict(nu=0.0), 1)):
         cp = _capi.to_c(mri_16x16_nz32(**bad))
         assert L.qlgpu_create(ctypes.byref(cp), 0, ctypes.byref(h)) == code, bad
+
+
+def test_debug_library_exports_every_declared_symbol():
+    # the QLGPU_DEBUG variant (index checks, guard zones) has the same C ABI
+    lib_path = build(debug=True)
+    dl = ctypes.CDLL(lib_path)
+    for name in declared_functions():
+        assert hasattr(dl, name), name
+    assert dl.qlgpu_debug_build() == 1
+    rl = ctypes.CDLL(_capi.LIB_PATH)
+    assert rl.qlgpu_debug_build() == 0

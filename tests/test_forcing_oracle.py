@@ -93,3 +93,70 @@ def test_cfl_time_step(model):
     assert len(d) == 5 and abs(t - 12 * dtm) < 1e-14 and dtm < cfl / p.q
     kmax = max(2 * math.pi / p.L[0] * p.nx / 2, 2 * math.pi / p.L[1] * p.ny / 2, 2 * math.pi / p.L[2] * p.NZ / 3)
     assert dtm > cfl / (kmax * 0.2 + p.q)
+
+
+def ky0_pairs(p):
+    """(kx > 0, kx < 0) mode indices of the ky = 0 pairs (Kdata.cpp:124-146)."""
+    kt = ktables(p)
+    pos = {int(kt["kx_index"][i]): i for i in range(p.nxy) if kt["ky_index"][i] == 0}
+    return [(pos[a], pos[-a]) for a in range(1, p.nx // 2)]
+
+
+def test_fullqlin_noise_ky0_conjugate_pairs():
+    # MHD_FullQlin::DrivingNoise (MHD_FullQlin.cpp:786-1045): ky != 0 as MHD_BQlin, and
+    # ky = 0 driven so that f(-kx, 0, -kz) = conj f(kx, 0, kz) holds exactly
+    p = QLParams(model=1, nx=16, ny=16, NZ=48, dt=0.01, remap=0, B0z=0.0, omega=1.0)
+    lin, mf, kx0 = initial_state(p, 0, sigma=0.0, B0=0.0)
+    f, klo, khi = 0.3, 0.5, 60.0
+    _, lo, *_ = O.run_forced(p, 0.0, lin, mf, kx0, 1, f_noise=f, k_lo=klo, k_hi=khi, seed=5)
+    kt = ktables(p)
+    ky0 = kt["ky_index"] == 0
+    drive, mu, mz = noise_amplitudes(p, 0.0, p.dt, klo, khi)
+    # ky != 0: exactly MHD_BQlin's entries
+    pb = QLParams(model=0, nx=16, ny=16, NZ=48, dt=0.01, remap=0)
+    lb, mb, kb = initial_state(pb, 0, sigma=0.0, B0=0.0)
+    _, lob, *_ = O.run_forced(pb, 0.0, lb, mb, kb, 1, f_noise=f, k_lo=klo, k_hi=khi, seed=5)
+    assert np.array_equal(lo[~ky0], lob[~ky0])
+    # ky = 0: the (0, 0) mode and kz = 0 stay zero; every pair is conjugate at mirrored kz
+    i00 = [i for i in range(p.nxy) if ky0[i] and kt["kx_index"][i] == 0][0]
+    assert not np.any(lo[i00]) and not np.any(lo[ky0][:, :, 0])
+    nz = p.nz
+    mirror = (nz - np.arange(1, nz)) % nz
+    driven = 0
+    for ip, ineg in ky0_pairs(p):
+        assert np.array_equal(lo[ip][:, 1:], np.conj(lo[ineg][:, mirror]))
+        kx = kt["kx"][ineg]
+        lapF = -kx * kx - kt["kz"][1:] ** 2
+        band = (lapF > -khi * khi) & (lapF < -klo * klo)
+        assert np.all(lo[ineg][:, 1:][:, band] != 0) and not np.any(lo[ineg][:, 1:][:, ~band])
+        driven += band.sum()
+    assert driven > 50
+    # the normalised ky = 0 draws are complex normals of variance f^2 as well
+    tot = float(p.nx * p.ny * p.NZ)
+    m = p.dt * tot * tot * (1.0 / (16 * 32 * 32)) ** 2
+    z = []
+    for ip, ineg in ky0_pairs(p):
+        kz = kt["kz"][1:]
+        lap2 = -kz * kz
+        lapF = -kt["kx"][ineg] ** 2 + lap2
+        band = (lapF > -khi * khi) & (lapF < -klo * klo)
+        amp = [np.sqrt(m * lap2 / lapF), np.sqrt(-m * lap2)]
+        for v in range(4):
+            z.append(lo[ineg][v, 1:][band] / amp[v % 2][band])
+    z = np.concatenate(z)
+    assert abs(np.mean(np.abs(z) ** 2) / f ** 2 - 1) < 5 * math.sqrt(2.0 / z.size)
+
+
+@pytest.mark.parametrize("only", ["velocity", "magnetic"])
+def test_fullqlin_drive_only_switches(only):
+    # drive_only_velocity / drive_only_magnetic (MHD_FullQlin.cpp:21-22): the other pair of
+    # fields stays undriven, the driven pair draws the same numbers as with both on
+    p = QLParams(model=1, nx=8, ny=16, NZ=32, dt=0.01, remap=0, omega=1.0)
+    lin, mf, kx0 = initial_state(p, 0, sigma=0.0, B0=0.0)
+    kw = dict(f_noise=0.2, k_lo=0.5, k_hi=60.0, seed=11)
+    _, both, *_ = O.run_forced(p, 0.0, lin, mf, kx0, 1, **kw)
+    _, one, *_ = O.run_forced(p, 0.0, lin, mf, kx0, 1, drive_only_velocity=only == "velocity",
+                              drive_only_magnetic=only == "magnetic", **kw)
+    on, off = ((0, 1), (2, 3)) if only == "velocity" else ((2, 3), (0, 1))
+    assert np.array_equal(one[:, on], both[:, on]) and np.any(one[:, on])
+    assert not np.any(one[:, off])

@@ -53,10 +53,12 @@ def bq_cases(integ=0):
             for i, (nx, ny, NZ, eta) in enumerate(specs)]
 
 
-def run_batch(cases, sts, n, diag_every=1, mapping=None, tune=0, engine=None, chunks=None):
+def run_batch(cases, sts, n, diag_every=1, mapping=None, tune=0, engine=None, chunks=None, noise=None):
     require_gpu()
     res = []
     with QLBatch(cases) as b:
+        for c, args in (noise or {}).items():
+            b.set_noise(c, *args[:4], **args[4] if len(args) > 4 else {})
         if engine is not None:
             b.set_engine(engine)
             assert b.engine() == engine
@@ -338,3 +340,47 @@ def test_set_states_get_states_match_per_case_calls(engine):
     for p, (lin, mf, kx0), (_, _, k_default), (t, lo, mo, ko) in zip(cases, sts, base, a):
         t2, lo2, mo2, ko2, _ = O.run(p, 0.25, lin, mf, k_default if kx0 is None else kx0, 6)
         assert abs(t - t2) < 1e-15 and rel(lo, lo2) < TOL and np.array_equal(ko, ko2)
+
+
+@pytest.mark.parametrize("engine", ["queue", "items"])
+def test_batch_noise_per_case_matches_oracle(engine):
+    # Model::DrivingNoise inside the batch step (main.cpp:111-113): each case its own
+    # f_noise, band and seed, or none; the counter restarts with the case's state
+    cases = bq_cases()[:6]
+    sts = states(cases, sigma=1e-3)
+    n = 12
+    noise = {0: (0.05, 0.5, 40.0, 11), 2: (0.02, 1.0, 80.0, 12), 4: (0.08, 0.0, 30.0, 13),
+             5: (0.03, 0.5, 50.0, 14)}
+    res, _ = run_batch(cases, sts, n, diag_every=3, engine=engine, noise=noise)
+    for c, (p, (lin, mf, kx0), (t, lo, mo, ko, d)) in enumerate(zip(cases, sts, res)):
+        if c in noise:
+            f, klo, khi, seed = noise[c]
+            t2, lo2, mo2, ko2, d2, _ = O.run_forced(p, 0.0, lin, mf, kx0, n, diag_every=3, f_noise=f, k_lo=klo,
+                                                    k_hi=khi, seed=seed)
+        else:
+            t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, n, diag_every=3)
+        assert t == t2 and np.array_equal(ko, ko2)
+        assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL, (c, rel(lo, lo2), rel(mo, mo2))
+        assert d.shape == d2.shape and series_rel(d, d2) < TOL
+
+
+def test_batch_fullqlin_noise_matches_oracle():
+    # MHD_FullQlin cases (work-item engine) with the ky = 0 conjugate pairs and the
+    # drive_only_* switches (MHD_FullQlin.cpp:21-22,786-1045)
+    cases = [c for c in mixed_cases(model=1) if c.NZ <= 128][:4]
+    sts = states(cases, sigma=1e-3)
+    n = 10
+    noise = {0: (0.05, 0.5, 40.0, 21), 1: (0.04, 0.5, 60.0, 22, {"drive_only_velocity": True}),
+             3: (0.06, 0.0, 50.0, 23, {"drive_only_magnetic": True})}
+    res, _ = run_batch(cases, sts, n, diag_every=5, engine="items", noise=noise)
+    for c, (p, (lin, mf, kx0), (t, lo, mo, ko, d)) in enumerate(zip(cases, sts, res)):
+        if c in noise:
+            a = noise[c]
+            kw = a[4] if len(a) > 4 else {}
+            t2, lo2, mo2, ko2, d2, _ = O.run_forced(p, 0.0, lin, mf, kx0, n, diag_every=5, f_noise=a[0], k_lo=a[1],
+                                                    k_hi=a[2], seed=a[3], **kw)
+        else:
+            t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, n, diag_every=5)
+        assert t == t2 and np.array_equal(ko, ko2)
+        assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL, (c, rel(lo, lo2), rel(mo, mo2))
+        assert d.shape == d2.shape and series_rel(d, d2) < TOL

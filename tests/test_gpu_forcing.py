@@ -94,10 +94,35 @@ def test_noise_and_cfl_together_and_off_again():
     assert t4 == t5 and rel(lo4, lo5) < TOL
 
 
-def test_noise_refused_for_fullqlin():
+@pytest.mark.parametrize("integ", [0, 1])
+@pytest.mark.parametrize("only", [None, "velocity", "magnetic"])
+def test_fullqlin_noise_matches_oracle(integ, only):
+    # MHD_FullQlin::DrivingNoise with its ky = 0 conjugate pairs (MHD_FullQlin.cpp:786-1045)
+    # and the drive_only_* switches (:21-22)
+    p = QLParams(model=1, integrator=integ, nx=16, ny=16, NZ=32, dt=0.02, B0z=0.01, omega=1.0)
+    st = initial_state(p, 8, sigma=1e-3, B0=0.05, mean_u=0.01)
+    n, noise = 30, (0.05, 0.5, 40.0, 4321)
+    kw = dict(drive_only_velocity=only == "velocity", drive_only_magnetic=only == "magnetic")
+    require_gpu()
+    with QLSolver(p) as s:
+        s.set_state(0.0, *st)
+        s.set_noise(*noise, **kw)
+        d = s.step(n, diag_every=5)
+        t, lo, mo, ko = s.get_state()
+    t2, lo2, mo2, ko2, d2, _ = O.run_forced(p, 0.0, *st, n, diag_every=5, f_noise=noise[0], k_lo=noise[1],
+                                            k_hi=noise[2], seed=noise[3], **kw)
+    assert t == t2 and np.array_equal(ko, ko2)
+    assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL, (rel(lo, lo2), rel(mo, mo2))
+    assert series_rel(d, d2[1:]) < TOL
+    t3, lo3, *_ = O.run(p, 0.0, *st, n)
+    assert rel(lo3, lo2) > 1e-2
+
+
+def test_drive_only_switches_refused_for_bqlin():
     from ql_dns_b200._capi import QLGPUError
     require_gpu()
-    with QLSolver(QLParams(model=1, nx=8, ny=8, NZ=32)) as s:
+    with QLSolver(QLParams(model=0, nx=8, ny=8, NZ=32)) as s:
+        s.set_noise(0.1, 1.0, 10.0)
         with pytest.raises(QLGPUError) as ei:
-            s.set_noise(0.1, 1.0, 10.0)
+            s.set_noise(0.1, 1.0, 10.0, drive_only_velocity=True)
         assert ei.value.code == 2
