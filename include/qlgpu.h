@@ -344,11 +344,13 @@ int qlgpu_batch_set_engine(qlgpu_batch_t* b, int engine);
 int qlgpu_batch_engine(const qlgpu_batch_t* b, int* engine);
 
 /* Queue engine: CTA passes per chunk for the NZ classes 16, 32, 64, 128
- * (passes4[i] >= 1; a pass steps 16 warps x 32/(NZ/4) modes).  Selects the
+ * (passes4[i] >= 1; a pass steps 12 warps x 32/(NZ/4) modes).  Selects the
  * queue engine.  qlgpu_batch_tune searches these when the queue engine is
  * active. */
 int qlgpu_batch_set_chunks(qlgpu_batch_t* b, const int* passes4);
-/* The current passes per chunk of the four NZ classes (after qlgpu_batch_tune: the tuned ones). */
+/* The current passes per chunk of the four NZ classes: after qlgpu_batch_tune the
+ * tuned ones; before, 4 per class, or fewer where 4 would leave SMs without a chunk
+ * (a small batch). */
 int qlgpu_batch_chunks(const qlgpu_batch_t* b, int* passes4);
 
 /* Profiling aid of the queue engine (QLGPU_TRACE=1 in the environment at

@@ -460,6 +460,62 @@ int plan_and_apply(qlgpu_batch_t* b, int warps, const int* fixed_k) {
 int ens_class(int NZ) { return NZ == 16 ? 0 : NZ == 32 ? 1 : NZ == 64 ? 2 : 3; }
 size_t tw8_offset(int NZ) { return NZ == 16 ? 0 : NZ == 32 ? 16 : NZ == 64 ? 48 : 112; }  // cplx
 
+// Default CTA passes per chunk of each NZ class, before any tuning.  Four passes
+// keep the fixed cost of a chunk small (about 12 us against about 25 us per pass,
+// the same at every NZ by the choice of modes per pass; measured on B200).  When
+// four passes leave CTAs without a chunk (a small batch), the combination of
+// {1, 2, 3, 4} that minimises whole waves of chunks times the mean chunk time is
+// taken instead.
+void default_passes(qlgpu_batch_t* b) {
+    constexpr double PASS_US = 25.0, CHUNK_US = 12.0;
+    const int grid = b->sms;
+    std::vector<int> need(b->ncases), cls(b->ncases);
+    bool present[4] = {false, false, false, false};
+    for (int c = 0; c < b->ncases; ++c) {
+        const CaseHost& h = b->cs[c];
+        const int mpp = ens::modes_per_pass(h.NZ);
+        need[c] = (h.nxy + mpp - 1) / mpp;
+        cls[c] = ens_class(h.NZ);
+        present[cls[c]] = true;
+    }
+    auto chunks_and_work = [&](const int (&p)[4], double* work) {
+        long C = 0;
+        double W = 0.0;
+        for (int c = 0; c < b->ncases; ++c) {
+            const int pc = p[cls[c]];
+            const long n = (need[c] + pc - 1) / pc;
+            C += n;
+            W += (double)n * (pc * PASS_US + CHUNK_US);
+        }
+        *work = W;
+        return C;
+    };
+    int best[4] = {4, 4, 4, 4};
+    double W4 = 0.0;
+    if (chunks_and_work(best, &W4) >= grid) {
+        std::copy(best, best + 4, b->qpasses);
+        return;
+    }
+    double best_est = 1e300;
+    for (int code = 0; code < 256; ++code) {
+        int p[4];
+        bool skip = false;
+        for (int k = 0; k < 4; ++k) {
+            p[k] = 1 + ((code >> (2 * k)) & 3);
+            if (!present[k] && p[k] != 4) skip = true;
+        }
+        if (skip) continue;
+        double W = 0.0;
+        const long C = chunks_and_work(p, &W);
+        const double est = (double)((C + grid - 1) / grid) * (W / (double)C);
+        if (est < best_est - 1e-9) {
+            best_est = est;
+            std::copy(p, p + 4, best);
+        }
+    }
+    std::copy(best, best + 4, b->qpasses);
+}
+
 bool queue_usable(const qlgpu_batch_t* b) {
     if (!b->queue_ok || b->engine != QLGPU_BATCH_ENGINE_QUEUE) return false;
     for (const CaseHost& h : b->cs)
@@ -515,7 +571,7 @@ int queue_plan(qlgpu_batch_t* b) {
     if (smem > b->smem_optin) return bfail(b, QLGPU_ERR_UNSUPPORTED, "queue engine: shared memory request too large");
     QB_CK(ensure_smem_attr(k, smem));
     int occ = 0;
-    QB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, ens::ENS_THREADS, smem));
+    QB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, ens::threads(), smem));
     if (occ < 1) return bfail(b, QLGPU_ERR_UNSUPPORTED, "queue engine: the CTA does not fit an SM");
     b->qsmem = smem;
     b->qgrid = b->sms;
@@ -892,6 +948,7 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
         b->queue_ok = b->model == MODEL_BQLIN;
         for (int c = 0; c < ncases; ++c)
             if (cases[c].NZ > 128) b->queue_ok = false;
+        if (b->queue_ok) default_passes(b);
         const char* tr = std::getenv("QLGPU_TRACE");
         if (tr && tr[0] == '1' &&
             cudaMalloc(&b->d_qtrace, sizeof(unsigned long long) * 4 * (size_t)b->sms) != cudaSuccess) {
@@ -1351,7 +1408,7 @@ int qlgpu_batch_mapping(const qlgpu_batch_t* b, int* info4, int* ncta) {
             if (rc) return rc;
         }
         if (info4) {
-            info4[0] = ens::ENS_THREADS / 32;
+            info4[0] = ens::threads() / 32;
             info4[1] = b->qgrid;
             info4[2] = 1;
             info4[3] = (int)b->qsmem;

@@ -34,6 +34,7 @@ const void* kernel(int integ) {
 }
 
 size_t smem_bytes(int NZ) { return chunk_smem(NZ); }
+int threads() { return THREADS; }
 int modes_per_pass(int NZ) { return pass_modes(NZ); }
 
 }  // namespace ens

@@ -10,9 +10,8 @@
 namespace qlgpu {
 namespace ens {
 
-constexpr int ENS_THREADS = 512;
-
 cudaError_t launch(int integ, const EnsLaunch& L, int grid, size_t smem, cudaStream_t st);
+int threads();               // threads per CTA of the persistent kernel
 const void* kernel(int integ);
 size_t smem_bytes(int NZ);   // dynamic shared memory of one NZ class (16, 32, 64, 128)
 int modes_per_pass(int NZ);  // modes a CTA steps at once

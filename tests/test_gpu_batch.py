@@ -231,7 +231,7 @@ def test_queue_engine_matches_oracle(integ):
     sts = states(cases)
     n = 30
     res, m = run_batch(cases, sts, n, engine="queue")
-    assert m["warps"] == 16
+    assert m["warps"] == 12
     for p, (lin, mf, kx0), (t, lo, mo, ko, d) in zip(cases, sts, res):
         t2, lo2, mo2, ko2, d2 = O.run(p, 0.0, lin, mf, kx0, n, diag_every=1)
         assert t == t2 and np.array_equal(ko, ko2)
