@@ -730,6 +730,9 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
             tm_st4c(ta + TM_ACC, x);  // F_eta (U) / F_zeta (B) until the update phase; acc is dead here
             tm_st4c(ta + TM_ACC + 16, x + 4);
         }
+        // previous rhs of the first field the update phase writes (U: b, B: u), requested before
+        // slot 7's transform so that the transform covers the L2 round trip
+        cplx fpv0[8];
         // ---- slot 7: U inverse R_uy (Ey); B forward 2 kx ky dBy KB -> F_u
         {
             if (role == 0) {
@@ -755,6 +758,7 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
                     x[rr] = mk(w * kw.x, -w * kw.y);  // conj(2 a b dBy R_bz)
                 }
             }
+            if (valid) load_fp(role ? 0 : 2, fpv0);
             xform<E>(x, xg, tw, g, t);
             tm_wait_st();  // S (slot 3) and Ey (slot 5) are stored before they are read back
             double ey[8];
@@ -795,13 +799,15 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         }
         // ---- RK updates of the mode's four fields (RK3CN_Elin.cpp:102-104, RK3CN.cpp:105-107) in one
         // phase after the transforms: U updates b (F in TM_S) and eta (TM_ACC), B updates u (registers)
-        // and zeta (TM_ACC).  A field's previous right-hand side is loaded as one batch of eight
-        // entries per lane, the second field's after the first is stored (fewer live registers).
+        // and zeta (TM_ACC).  A field's previous right-hand side arrives as one batch of eight entries
+        // per lane: the first field's was requested before slot 7, the second field's is requested
+        // after the first is stored (fewer live registers).
         {
             const int fs = role ? 0 : 2, fa = role ? 1 : 3;
             const double* ekzt = role ? ekz_u : ekz_b;
             cplx fpv[8];
-            if (valid) load_fp(fs, fpv);
+#pragma unroll
+            for (int rr = 0; rr < 8; ++rr) fpv[rr] = fpv0[rr];
             // the integrating factor of the role's fields, computed while the loads are in flight
             const double em = (INTEG == INTEG_EXP) ? exp(S.linC * (role ? P.nu : P.cb) * hxy) : 1.0;
             tm_wait_st();  // F (slot 6) is stored before it is read back
