@@ -120,7 +120,10 @@ int qlgpu_rhs(qlgpu_t* h, double t, double dt_lin, const double* lin_in, const d
  * loads the library until the process exits.  Limits: at most 8192 (kx,ky)
  * modes and ny <= 256 (larger cases return QLGPU_ERR_ARG; use qlgpu_rhs).
  * The first call on each device looks up the scratch address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * (cudaGetSymbolAddress) and the device's SM count and shared-memory limit;
+ * make that first call before any stream capture.  These are kept for the
+ * life of the process: they do not survive cudaDeviceReset (call no
+ * qlgpu_rhs_noalloc after a reset).
  * All calls share the scratch: calls that overlap on the GPU (other streams,
  * other host threads) race and must be serialised by the caller.  Errors are
  * reported through qlgpu_last_error(NULL, ...). */

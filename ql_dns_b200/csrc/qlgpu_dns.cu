@@ -135,25 +135,47 @@ static void make_stages(qlgpu_dns* h) {
     h->st[0] = s0; h->st[1] = s1; h->st[2] = s2;
 }
 
+// One launch of the step with programmatic dependent launch: the kernel may be
+// scheduled while the previous one drains (it waits in pdl_start before it touches
+// global memory), which hides the launch gap between the short kernels of a stage.
+template <typename... Args>
+static cudaError_t launch_pdl(void (*k)(Args...), dim3 grid, int block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // Products of the current state: launches A, B, C.
 static cudaError_t enqueue_products(qlgpu_dns* h) {
     const DnsArgs& a = h->a;
-    h->k_inv<<<dim3(h->Kyn, 6), BLOCK, h->s_inv, h->stream>>>(a);
-    h->k_phys<<<dim3(h->p.Mx, h->p.NZ / h->zc), h->phys_threads, h->s_phys, h->stream>>>(a);
-    h->k_fwd<<<dim3(h->Kyn, NPROD), BLOCK, h->s_fwd, h->stream>>>(a);
-    return cudaGetLastError();
+    cudaError_t e = launch_pdl(h->k_inv, dim3(h->Kyn, 6), BLOCK, h->s_inv, h->stream, a);
+    if (e == cudaSuccess)
+        e = launch_pdl(h->k_phys, dim3(h->p.Mx, h->p.NZ / h->zc), h->phys_threads, h->s_phys, h->stream, a);
+    if (e == cudaSuccess) e = launch_pdl(h->k_fwd, dim3(h->Kyn, NPROD), BLOCK, h->s_fwd, h->stream, a);
+    return e;
 }
 
 static cudaError_t enqueue_step(qlgpu_dns* h) {
     const int n = h->nxy * h->nz;
     for (int s = 0; s < 3; ++s) {
         cudaError_t e = enqueue_products(h);
+        if (e == cudaSuccess)
+            e = launch_pdl(dns_update, dim3((n + BLOCK - 1) / BLOCK), BLOCK, 0, h->stream, h->a, h->st[s]);
         if (e != cudaSuccess) return e;
-        dns_update<<<(n + BLOCK - 1) / BLOCK, BLOCK, 0, h->stream>>>(h->a, h->st[s]);
     }
-    dns_remap_kx<<<(h->nxy + 255) / 256, 256, 0, h->stream>>>(h->a);
-    dns_advance_clock<<<1, 32, 0, h->stream>>>(h->a);
-    return cudaGetLastError();
+    cudaError_t e = launch_pdl(dns_remap_kx, dim3((h->nxy + 255) / 256), 256, 0, h->stream, h->a);
+    if (e == cudaSuccess) e = launch_pdl(dns_advance_clock, dim3(1), 32, 0, h->stream, h->a);
+    return e;
 }
 
 static cudaError_t enqueue_diag(qlgpu_dns* h) {

@@ -57,6 +57,15 @@ struct DnsStage {
     double t_abs;                                 // rhs_only: absolute time
 };
 
+// Programmatic dependent launch (the step's kernels are launched with it): a
+// kernel lets the next one be scheduled as soon as all its CTAs have started, and
+// waits for the previous kernel to complete (and its memory to be visible) before
+// it touches global memory.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_start() {
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+
 __device__ __forceinline__ unsigned group_mask(int T) {
     const int lane = threadIdx.x & 31;
     const unsigned m = (T == 32) ? 0xffffffffu : ((1u << T) - 1u);
@@ -90,6 +99,7 @@ struct InvZX {
 
 template <int NZ, int MX>
 __global__ void __launch_bounds__(BLOCK, 2) dns_inv_zx(DnsArgs a) {
+    pdl_start();
     using K = InvZX<NZ, MX>;
     using GZ = typename K::GZ;
     using GX = typename K::GX;
@@ -180,6 +190,7 @@ __device__ __forceinline__ double product(int p, const double* v) {
 
 template <int MY>
 __global__ void __launch_bounds__(Phys<MY>::THREADS, 2) dns_phys(DnsArgs a) {
+    pdl_start();
     using K = Phys<MY>;
     using GY = typename K::GY;
     constexpr int T = GY::T, NG = K::NG, ZC = K::ZC, PY = K::PY;
@@ -270,6 +281,7 @@ struct FwdXZ {
 
 template <int MX, int NZ>
 __global__ void __launch_bounds__(BLOCK, 2) dns_fwd_xz(DnsArgs a) {
+    pdl_start();
     using K = FwdXZ<MX, NZ>;
     using GZ = typename K::GZ;
     using GX = typename K::GX;
@@ -343,6 +355,7 @@ __device__ __forceinline__ double lap_order(const DnsArgs& a, double kx0, double
 __device__ __forceinline__ cplx cmuli(cplx a) { return mk(-a.y, a.x); }  // i a
 
 __global__ void __launch_bounds__(BLOCK) dns_update(DnsArgs a, DnsStage st) {
+    pdl_start();
     const int idx = blockIdx.x * BLOCK + threadIdx.x;
     if (idx >= a.nxy * a.nz) return;
     const int mode = idx / a.nz, s = idx % a.nz;
@@ -458,6 +471,7 @@ __global__ void __launch_bounds__(BLOCK) dns_update(DnsArgs a, DnsStage st) {
 // After the last stage: shift kx0 of the columns that left the box (their
 // fields were zeroed by dns_update), MHD_FullQlin.cpp:464-481.
 __global__ void dns_remap_kx(DnsArgs a) {
+    pdl_start();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nxy || !a.remap) return;
     const double tn = a.clock[0] + a.dt;
@@ -466,6 +480,7 @@ __global__ void dns_remap_kx(DnsArgs a) {
 }
 
 __global__ void dns_advance_clock(DnsArgs a) {
+    pdl_start();
     if (threadIdx.x == 0 && blockIdx.x == 0) a.clock[0] = a.clock[0] + a.dt;
 }
 
