@@ -568,9 +568,28 @@ def run_gpu(args):
         return ms, recs_all, outs, {"set_states_ms": 1e3 * (h1 - h0), "steps_ms": 1e3 * (h2 - h1),
                                     "get_states_ms": 1e3 * (h3 - h2)}
 
+    def e2e_roundtrip():
+        """Every step a full host round trip: the state of all cases in from pinned memory, one
+        step with its records read back, the state out (a caller that keeps the state on the host)."""
+        torch.cuda.synchronize()
+        barrier(ws)
+        ee0 = torch.cuda.Event(enable_timing=True)
+        ee1 = torch.cuda.Event(enable_timing=True)
+        ee0.record(ext)
+        cur, nxt = pin_in, pin_out  # the last e2e use of pin_in: it is overwritten here
+        for _ in range(args.steps):
+            batch.set_states(0.0, cur)
+            batch.step(1, diag_every=1)
+            batch.get_states(nxt)
+            cur, nxt = nxt, cur
+        ee1.record(ext)
+        ee1.synchronize()
+        return max_over_ranks(ws, ee0.elapsed_time(ee1))
+
     e2e_run(True)  # warm-up of the one-step graph
     e2e_ms, recs_all, outs, phases = e2e_run(True)
     one_ms, _, _, one_phases = e2e_run(False)
+    rt_ms = e2e_roundtrip()
     state_bytes = sum(lin.nbytes + mf.nbytes + kx0.nbytes for lin, mf, kx0 in sts)
     e2e = {"value": job_modes * args.steps / (e2e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": state_bytes / args.steps,
@@ -580,7 +599,12 @@ def run_gpu(args):
            "phases_host_ms": phases,
            "one_call": {"value": job_modes * args.steps / (one_ms / 1e3), "unit": UNIT,
                         "path": "as above with one QLBatch.step(K, diag_every=1): one launch, every step's 48 "
-                                "records read back after it", "phases_host_ms": one_phases}}
+                                "records read back after it", "phases_host_ms": one_phases},
+           "state_roundtrip_every_step": {
+               "value": job_modes * args.steps / (rt_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": NCASES * 15 * 8 + state_bytes,
+               "path": "every step: QLBatch.set_states (pinned) of all cases, QLBatch.step(1, diag_every=1), "
+                       "QLBatch.get_states (pinned); for a caller that keeps the state in host memory"}}
     batch.close()
 
     parity = ensemble_parity(cases, sts, recs_all, outs, timed_out, args) if rank == 0 else None

@@ -457,6 +457,8 @@ int plan_and_apply(qlgpu_batch_t* b, int warps, const int* fixed_k) {
 // ---------------------------------------------------------------------------
 // Chunk-queue engine
 // ---------------------------------------------------------------------------
+constexpr int QTRACE_MAX_CTAS_PER_SM = 4;  // bound of the queue grid: at most this many CTAs per SM
+
 int ens_class(int NZ) { return NZ == 16 ? 0 : NZ == 32 ? 1 : NZ == 64 ? 2 : 3; }
 size_t tw8_offset(int NZ) { return NZ == 16 ? 0 : NZ == 32 ? 16 : NZ == 64 ? 48 : 112; }  // cplx
 
@@ -574,7 +576,8 @@ int queue_plan(qlgpu_batch_t* b) {
     QB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, ens::threads(), smem));
     if (occ < 1) return bfail(b, QLGPU_ERR_UNSUPPORTED, "queue engine: the CTA does not fit an SM");
     b->qsmem = smem;
-    b->qgrid = b->sms;
+    if (occ > QTRACE_MAX_CTAS_PER_SM) occ = QTRACE_MAX_CTAS_PER_SM;
+    b->qgrid = b->sms * occ;  // every resident CTA (a cooperative launch)
     b->qdirty = false;
     drop_graphs(b);
     return QLGPU_OK;
@@ -951,7 +954,8 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
         if (b->queue_ok) default_passes(b);
         const char* tr = std::getenv("QLGPU_TRACE");
         if (tr && tr[0] == '1' &&
-            cudaMalloc(&b->d_qtrace, sizeof(unsigned long long) * 4 * (size_t)b->sms) != cudaSuccess) {
+            cudaMalloc(&b->d_qtrace, sizeof(unsigned long long) * 4 * QTRACE_MAX_CTAS_PER_SM * (size_t)b->sms) !=
+                cudaSuccess) {
             b->err = "trace buffer";
             return bail(QLGPU_ERR_CUDA);
         }

@@ -61,7 +61,11 @@ constexpr int THREADS = 32 * WARPS;
 // TMEM columns of one lane: Ex (8 doubles), Ey (8 doubles), S (8 complex), acc (8 complex)
 constexpr int TM_EX = 0, TM_EY = 16, TM_S = 32, TM_ACC = 64;
 constexpr int COLS_PER_WARP = 96;
-constexpr int TCOLS = 512;  // a power of two >= COLS_PER_WARP * (WARPS / 4): warps w, w+4, ... share lane quarter w%4
+constexpr int CTAS_PER_SM = 1;  // resident CTAs per SM (their TMEM allocations share the SM's 512 columns)
+// TMEM columns per CTA: a power of two >= COLS_PER_WARP * ceil(WARPS / 4) (warps w, w+4, ... share lane
+// quarter w%4), at most 512 / CTAS_PER_SM
+constexpr int TCOLS = COLS_PER_WARP * ((WARPS + 3) / 4) <= 128 ? 128 : COLS_PER_WARP * ((WARPS + 3) / 4) <= 256 ? 256 : 512;
+static_assert(TCOLS * CTAS_PER_SM <= 512, "TMEM columns of the resident CTAs");
 constexpr int NEMF = 2;                                  // stress profiles Ex, Ey
 constexpr int MAX_PAIRS_PER_WARP = 8;                    // NZ = 16
 
@@ -978,7 +982,7 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
 // The persistent kernel: tickets in order, one chunk per ticket.
 // ---------------------------------------------------------------------------
 template <int INTEG>
-__global__ void __launch_bounds__(THREADS, 1) ens_kernel(const __grid_constant__ EnsLaunch L) {
+__global__ void __launch_bounds__(THREADS, CTAS_PER_SM) ens_kernel(const __grid_constant__ EnsLaunch L) {
     __shared__ ChunkHdr hd;
     __shared__ __align__(8) uint64_t bars[WARPS * MAX_PAIRS_PER_WARP];
     __shared__ unsigned char bar_ph[WARPS * MAX_PAIRS_PER_WARP];
