@@ -384,3 +384,19 @@ def test_batch_fullqlin_noise_matches_oracle():
         assert t == t2 and np.array_equal(ko, ko2)
         assert rel(lo, lo2) < TOL and rel(mo, mo2) < TOL, (c, rel(lo, lo2), rel(mo, mo2))
         assert d.shape == d2.shape and series_rel(d, d2) < TOL
+
+
+def test_default_chunk_passes_give_every_sm_a_chunk():
+    # sixteen 32x32-mode NZ=64 cases (the adjoint workload): four CTA passes per chunk would
+    # make 64 chunks for 148 SMs, so the default takes fewer; the 48-case ensemble keeps four
+    require_gpu()
+    small = [QLParams(nx=32, ny=32, NZ=64, dt=0.01) for _ in range(16)]
+    with QLBatch(small) as b:
+        b.set_engine("queue")
+        m = b.mapping()
+        assert m["chunk_passes"][64] < 4
+        assert sum(m["ncta"]) >= 100, m["ncta"]
+    cases, _, _ = mri_ensemble(48)
+    with QLBatch(cases) as b:
+        b.set_engine("queue")
+        assert all(v == 4 for v in b.mapping()["chunk_passes"].values())
