@@ -88,7 +88,10 @@ struct EG {
     static constexpr size_t o_kz = o_prof + 8 * 3 * (size_t)NZ_;            // kz value per spectral slot
     static constexpr size_t o_ekz = o_kz + 8 * (size_t)NZ_;                 // [2][NZE] integrating factors
     static constexpr size_t o_warp = o_ekz + 8 * 2 * (size_t)NZE;
-    static constexpr size_t K_CPLX = (size_t)PPW * 2 * NZ_;                 // per warp: KU, KB of its pairs
+    // per pair KU, then KB shifted by T slots: for T <= 4 the two roles of a pair share a quarter
+    // warp, and without the shift their K accesses fall on the same banks
+    static constexpr int KPAIR = 2 * NZ_ + T;
+    static constexpr size_t K_CPLX = (size_t)PPW * KPAIR;                    // per warp: KU, KB of its pairs
     static constexpr size_t STG_CPLX = (size_t)PPW * 4 * nz;                 // staged mode fields
     static constexpr size_t X_CPLX = (size_t)GPW * 8 * T;                    // exchange buffers
     static constexpr size_t X_OFF = K_CPLX + STG_CPLX;                        // per warp: [K | STG | X]
@@ -542,8 +545,8 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         cplx* __restrict__ uo = lin_out + (size_t)m * 4 * nzd;
         cplx* __restrict__ fo = A.Fout ? A.Fout + (size_t)m * 4 * nzd : nullptr;
         const cplx* __restrict__ fpm = has_prev ? A.Fprev + (size_t)m * 4 * nzd : nullptr;
-        cplx* KU = Kw + (size_t)pi * 2 * NZ;
-        cplx* KB = KU + NZ;
+        cplx* KU = Kw + (size_t)pi * E::KPAIR;
+        cplx* KB = KU + NZ + T;
         cplx* Kown = role ? KB : KU;
         cplx* Koth = role ? KU : KB;
         const int ksw = pi & E::SWZ;
