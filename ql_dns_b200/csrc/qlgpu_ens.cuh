@@ -41,9 +41,10 @@
 //   7 inv R_uy : Ey += Re(KB R_uy*)             fwd 2 kx ky dBy KB -> F_u = S + ilapF(...)
 //
 // Slot 7 is an inverse transform in U and a forward one in B: both run the
-// same routine.  The stress accumulators Ex, Ey and the held spectrum S live
-// in tensor memory (TMEM) as a per-lane scratchpad, so a thread holds only
-// the transform in flight and one accumulator in registers.
+// same routine.  The stress accumulators Ex, Ey, the held spectrum S and the
+// previous right-hand sides live in tensor memory (TMEM) as a per-lane
+// scratchpad, so a thread holds only the transform in flight and one
+// accumulator in registers.
 #pragma once
 #include <cstdint>
 #include <type_traits>
@@ -58,14 +59,16 @@ namespace ens {
 // registers: fewer spills, and the smaller shared-memory footprint leaves more L1
 constexpr int WARPS = 12;
 constexpr int THREADS = 32 * WARPS;
-// TMEM columns of one lane: Ex (8 doubles), Ey (8 doubles), S (8 complex), acc (8 complex)
-constexpr int TM_EX = 0, TM_EY = 16, TM_S = 32, TM_ACC = 64;
-constexpr int COLS_PER_WARP = 96;
+// TMEM columns of one lane: Ex (8 doubles), Ey (8 doubles), S (8 complex), acc (8 complex), the
+// previous right-hand sides of the two fields the lane updates (8 complex each)
+constexpr int TM_EX = 0, TM_EY = 16, TM_S = 32, TM_ACC = 64, TM_FPA = 96, TM_FPB = 128;
+constexpr int COLS_PER_WARP = 160;
 constexpr int CTAS_PER_SM = 1;  // resident CTAs per SM (their TMEM allocations share the SM's 512 columns)
 // TMEM columns per CTA: a power of two >= COLS_PER_WARP * ceil(WARPS / 4) (warps w, w+4, ... share lane
 // quarter w%4), at most 512 / CTAS_PER_SM
 constexpr int TCOLS = COLS_PER_WARP * ((WARPS + 3) / 4) <= 128 ? 128 : COLS_PER_WARP * ((WARPS + 3) / 4) <= 256 ? 256 : 512;
 static_assert(TCOLS * CTAS_PER_SM <= 512, "TMEM columns of the resident CTAs");
+static_assert(COLS_PER_WARP * ((WARPS + 3) / 4) <= TCOLS, "TMEM columns of the warps sharing a lane quarter");
 constexpr int NEMF = 2;                                  // stress profiles Ex, Ey
 constexpr int MAX_PAIRS_PER_WARP = 8;                    // NZ = 16
 
@@ -566,14 +569,14 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
                 x[rr] = (!rdead<E>(rr) && sx >= 0) ? cscale(stg[(f0 + fa) * nzd + sx], fac) : mk(0.0, 0.0);
             }
         };
-        // RK update of one field from F in registers (F_out / lin_out stores)
-        // the previous right-hand side of field f at this lane's 8 entries, loaded together before an
-        // update loop (one L2 round trip instead of one per entry: the loop's stores would order them)
+        // the previous right-hand side of field f at this lane's 8 entries: requested before the
+        // transform of slot 2 (first updated field) or slot 4 (second), parked in TMEM after it, so the
+        // L2 round trip is covered by the transform and the update phase reads TMEM
         auto load_fp = [&](int f, cplx (&fpv)[8]) {
 #pragma unroll
             for (int rr = 0; rr < 8; ++rr) {
                 const int sx = sidx<E>(t, rr);
-                fpv[rr] = (fpm && !rdead<E>(rr) && sx >= 0) ? ldc(fpm + f * nzd + sx) : mk(0.0, 0.0);
+                fpv[rr] = (valid && fpm && !rdead<E>(rr) && sx >= 0) ? ldc(fpm + f * nzd + sx) : mk(0.0, 0.0);
             }
         };
         auto update = [&](int f, const cplx (&F)[8], int rr, int sx, double em, const double* ekzt, cplx fp) {
@@ -620,7 +623,14 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         // ---- slot 2: R_u / R_b
         {
             load_plain(0);
-            xform<E>(x, xg, tw, g, t);
+            if (has_prev) {
+                cplx fpq[8];
+                load_fp(role ? 0 : 2, fpq);  // U: b, B: u
+                xform<E>(x, xg, tw, g, t);
+                tm_st8c(ta + TM_FPA, fpq);
+            } else {
+                xform<E>(x, xg, tw, g, t);
+            }
             double ex[8];
             tm_ld8d(ta + TM_EX, ex);
             const double sg = role ? -mult : mult;
@@ -657,7 +667,14 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         // ---- slot 4: R_zeta / R_eta: acc += i b By R
         {
             load_plain(1);
-            xform<E>(x, xg, tw, g, t);
+            if (has_prev) {
+                cplx fpq[8];
+                load_fp(role ? 1 : 3, fpq);  // U: eta, B: zeta
+                xform<E>(x, xg, tw, g, t);
+                tm_st8c(ta + TM_FPB, fpq);
+            } else {
+                xform<E>(x, xg, tw, g, t);
+            }
             tm_wait_st();
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -737,9 +754,6 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
             tm_st4c(ta + TM_ACC, x);  // F_eta (U) / F_zeta (B) until the update phase; acc is dead here
             tm_st4c(ta + TM_ACC + 16, x + 4);
         }
-        // previous rhs of the first field the update phase writes (U: b, B: u), requested before
-        // slot 7's transform so that the transform covers the L2 round trip
-        cplx fpv0[8];
         // ---- slot 7: U inverse R_uy (Ey); B forward 2 kx ky dBy KB -> F_u
         {
             if (role == 0) {
@@ -765,7 +779,6 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
                     x[rr] = mk(w * kw.x, -w * kw.y);  // conj(2 a b dBy R_bz)
                 }
             }
-            if (valid) load_fp(role ? 0 : 2, fpv0);
             xform<E>(x, xg, tw, g, t);
             tm_wait_st();  // S (slot 3) and Ey (slot 5) are stored before they are read back
             double ey[8];
@@ -806,21 +819,18 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         }
         // ---- RK updates of the mode's four fields (RK3CN_Elin.cpp:102-104, RK3CN.cpp:105-107) in one
         // phase after the transforms: U updates b (F in TM_S) and eta (TM_ACC), B updates u (registers)
-        // and zeta (TM_ACC).  A field's previous right-hand side arrives as one batch of eight entries
-        // per lane: the first field's was requested before slot 7, the second field's is requested
-        // after the first is stored (fewer live registers).
+        // and zeta (TM_ACC).  The previous right-hand sides wait in TM_FPA / TM_FPB (slots 2 and 4).
         {
             const int fs = role ? 0 : 2, fa = role ? 1 : 3;
             const double* ekzt = role ? ekz_u : ekz_b;
-            cplx fpv[8];
-#pragma unroll
-            for (int rr = 0; rr < 8; ++rr) fpv[rr] = fpv0[rr];
-            // the integrating factor of the role's fields, computed while the loads are in flight
+            cplx fpv[8] = {};
+            // the integrating factor of the role's fields, computed while the TMEM loads are in flight
             const double em = (INTEG == INTEG_EXP) ? exp(S.linC * (role ? P.nu : P.cb) * hxy) : 1.0;
             tm_wait_st();  // F (slot 6) is stored before it is read back
             {
                 cplx FS[8];
                 tm_ld8c(ta + TM_S, FS);
+                if (has_prev) tm_ld8c(ta + TM_FPA, fpv);
                 if (role) {
 #pragma unroll
                     for (int rr = 0; rr < 8; ++rr) FS[rr] = x[rr];
@@ -834,7 +844,7 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
                     }
                 }
             }
-            if (valid) load_fp(fa, fpv);
+            if (has_prev) tm_ld8c(ta + TM_FPB, fpv);
             {
                 cplx FA[8];
                 tm_ld8c(ta + TM_ACC, FA);
