@@ -294,8 +294,11 @@ int qlgpu_batch_step_timed(qlgpu_batch_t* b, int nsteps, float* ms);
 
 /* Autotuner: times probe_steps-step launches of candidate mappings (CTA
  * width, CTAs per case, cases per CTA) on a copy of the state, fits the cost
- * model to the per-case times and keeps the fastest mapping.  The state is
- * unchanged.  *best_ms (may be NULL) = time of the kept mapping's probe. */
+ * model to the per-case times and keeps the fastest mapping.  Queue engine: a
+ * coordinate search, two sweeps, over the passes per chunk of each NZ class,
+ * each candidate timed as the best of three launches of max(probe_steps, 6)
+ * steps.  The state is unchanged.  *best_ms (may be NULL) = time of the kept
+ * mapping's probe. */
 int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms);
 
 /* The planner's cost model (after qlgpu_batch_tune: fitted to the measured

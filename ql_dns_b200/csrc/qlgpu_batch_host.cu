@@ -137,9 +137,9 @@ __global__ void batch_collect_kernel(const BatchCase* cases, int ncases, const B
     }
 }
 
-// set_states: case c's clock starts at t (reset_case_clock for every case at once) and,
-// where kx_default[c], its kx0 is the unsheared table.  One block per case.
-__global__ void batch_set_clocks_kernel(const BatchCase* cases, int ncases, double t, const int* kx_default) {
+// set_states: case c's clock starts at t (reset_case_clock for every case at once).  One block
+// per case.
+__global__ void batch_set_clocks_kernel(const BatchCase* cases, int ncases, double t) {
     const int c = blockIdx.x;
     if (c >= ncases) return;
     DevClock* k = cases[c].A[0].clk;
@@ -150,16 +150,33 @@ __global__ void batch_set_clocks_kernel(const BatchCase* cases, int ncases, doub
         k->t = t;
         k->old_init = 1;
     }
-    if (kx_default[c]) {
-        const int nxy = cases[c].P.nxy;
-        for (int i = threadIdx.x; i < nxy; i += blockDim.x) cases[c].A[0].kx0[i] = cases[c].kx_init[i];
-    }
 }
 
-// get_states: every case's clock time into one array.
-__global__ void batch_gather_t_kernel(const BatchCase* cases, int ncases, double* out) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncases; c += gridDim.x * blockDim.x)
-        out[c] = cases[c].A[0].clk->t;
+// The small per-case arrays of set_states / get_states travel as one block (one copy instead of
+// two per case): case c's mean fields [2 nmf nz] and kx0 [nxy] at off[c], then one value per case
+// at off[ncases] (set: 1 where kx0 is given, else the case takes its unsheared table; get: t).
+__global__ void batch_scatter_small_kernel(const BatchCase* cases, int ncases, const double* src,
+                                           const long long* off) {
+    const int c = blockIdx.x;
+    if (c >= ncases) return;
+    const BatchCase& bc = cases[c];
+    const int nmf2 = 2 * bc.P.nmf * bc.P.nz, nxy = bc.P.nxy;
+    const double* sp = src + off[c];
+    double* mf = reinterpret_cast<double*>(bc.A[0].mf);
+    for (int i = threadIdx.x; i < nmf2; i += blockDim.x) mf[i] = sp[i];
+    const double* kx = src[off[ncases] + c] != 0.0 ? sp + nmf2 : bc.kx_init;
+    for (int i = threadIdx.x; i < nxy; i += blockDim.x) bc.A[0].kx0[i] = kx[i];
+}
+__global__ void batch_gather_small_kernel(const BatchCase* cases, int ncases, double* dst, const long long* off) {
+    const int c = blockIdx.x;
+    if (c >= ncases) return;
+    const BatchCase& bc = cases[c];
+    const int nmf2 = 2 * bc.P.nmf * bc.P.nz, nxy = bc.P.nxy;
+    double* dp = dst + off[c];
+    const double* mf = reinterpret_cast<const double*>(bc.A[0].mf);
+    for (int i = threadIdx.x; i < nmf2; i += blockDim.x) dp[i] = mf[i];
+    for (int i = threadIdx.x; i < nxy; i += blockDim.x) dp[nmf2 + i] = bc.A[0].kx0[i];
+    if (threadIdx.x == 0) dst[off[ncases] + c] = bc.A[0].clk->t;
 }
 
 }  // namespace
@@ -211,8 +228,13 @@ struct qlgpu_batch {
     int drop_case = -1;                  // failure-detection aid: a chunk of this case is left out
     bool qdirty = true;
     unsigned long long* d_qtrace = nullptr;  // [grid][4] per-CTA time sums of the last queue launch (QLGPU_TRACE=1)
-    int* d_flags = nullptr;                  // [ncases] per-case flags of set_states
-    double* d_tvec = nullptr;                // [ncases] clock times of get_states
+    // the small arrays of set_states / get_states in one block (batch_scatter_small_kernel)
+    std::vector<long long> soff;             // [ncases + 1] offsets in doubles
+    long long* d_soff = nullptr;
+    double* d_small = nullptr;
+    double* h_small = nullptr;               // pinned
+    int* h_col = nullptr;                    // pinned copy of d_collect
+    double* h_diag = nullptr;                // pinned copy of d_diag
     NoiseSpec* d_noise = nullptr;            // [ncases] driving-noise constants
     GuardList guards;                        // debug build: canary zones after the device buffers
 };
@@ -750,10 +772,13 @@ int qlgpu_batch_destroy(qlgpu_batch_t* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
     void* bufs[] = {b->arena,   b->d_cases, b->d_ctas, b->d_epoch, b->d_ctl, b->d_case_end, b->d_collect,
-                    b->d_out15, b->d_diag,  b->d_ec,   b->d_round, b->d_tw8, b->d_qtrace, b->d_flags, b->d_tvec,
-                    b->d_noise};
+                    b->d_out15, b->d_diag,  b->d_ec,   b->d_round, b->d_tw8, b->d_qtrace, b->d_noise, b->d_soff,
+                    b->d_small};
     for (void* p : bufs)
         if (p) cudaFree(p);
+    if (b->h_small) cudaFreeHost(b->h_small);
+    if (b->h_col) cudaFreeHost(b->h_col);
+    if (b->h_diag) cudaFreeHost(b->h_diag);
     for (cudaEvent_t e : b->ev)
         if (e) cudaEventDestroy(e);
     guard_release(b->guards);
@@ -926,11 +951,23 @@ int qlgpu_batch_create(const qlgpu_params* cases, int ncases, int device, qlgpu_
     QB_ALLOC(b->d_collect, sizeof(int) * (2 * ncases + 2));
     QB_ALLOC(b->d_out15, sizeof(double) * 15);
     QB_ALLOC(b->d_ec, sizeof(ens::EnsCase) * ncases);
-    QB_ALLOC(b->d_flags, sizeof(int) * ncases);
-    QB_ALLOC(b->d_tvec, sizeof(double) * ncases);
     QB_ALLOC(b->d_noise, sizeof(NoiseSpec) * ncases);
     QB_ALLOC(b->d_tw8, sizeof(cplx) * 240);
+    b->soff.assign(ncases + 1, 0);
+    for (int c = 0; c < ncases; ++c)
+        b->soff[c + 1] = b->soff[c] + 2LL * b->cs[c].nmf * b->cs[c].nz + b->cs[c].nxy;
+    const size_t small_bytes = sizeof(double) * ((size_t)b->soff[ncases] + ncases);
+    QB_ALLOC(b->d_soff, sizeof(long long) * (ncases + 1));
+    QB_ALLOC(b->d_small, small_bytes);
 #undef QB_ALLOC
+    if (cudaHostAlloc(&b->h_small, small_bytes, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc(&b->h_col, sizeof(int) * (2 * ncases + 2), cudaHostAllocDefault) != cudaSuccess ||
+        cudaMemcpyAsync(b->d_soff, b->soff.data(), sizeof(long long) * (ncases + 1), cudaMemcpyHostToDevice,
+                        b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess) {
+        b->err = "staging buffers";
+        return bail(QLGPU_ERR_CUDA);
+    }
     if (guard_arm(b->guards, b->stream) != cudaSuccess) {
         b->err = "guard zones";
         return bail(QLGPU_ERR_CUDA);
@@ -1040,20 +1077,24 @@ int qlgpu_batch_set_states(qlgpu_batch_t* b, double t, const double* const* lin,
         int rc = upload_descriptors(b);
         if (rc) return rc;
     }
-    std::vector<int> dflt(b->ncases, 1);
-    for (int c = 0; c < b->ncases; ++c) {
+    const int nc = b->ncases;
+    double* flag = b->h_small + b->soff[nc];
+    for (int c = 0; c < nc; ++c) {
         CaseHost& h = b->cs[c];
         const size_t nlin = (size_t)h.nxy * 4 * h.nz, nmfe = (size_t)h.nmf * h.nz;
         QB_CK(cudaMemcpyAsync(h.lin[b->cur], lin[c], nlin * sizeof(cplx), cudaMemcpyHostToDevice, b->stream));
-        QB_CK(cudaMemcpyAsync(h.mf, mf[c], nmfe * sizeof(cplx), cudaMemcpyHostToDevice, b->stream));
-        if (kx0 && kx0[c]) {
-            dflt[c] = 0;
-            QB_CK(cudaMemcpyAsync(h.kx0, kx0[c], h.nxy * sizeof(double), cudaMemcpyHostToDevice, b->stream));
-        }
+        // the mean fields and kx0 go through the staging block (one copy for every case)
+        double* sp = b->h_small + b->soff[c];
+        std::memcpy(sp, mf[c], nmfe * sizeof(cplx));
+        flag[c] = (kx0 && kx0[c]) ? 1.0 : 0.0;
+        if (kx0 && kx0[c]) std::memcpy(sp + 2 * nmfe, kx0[c], h.nxy * sizeof(double));
     }
-    // the clocks (and the default kx0) of every case in one launch, after the copies above
-    QB_CK(cudaMemcpyAsync(b->d_flags, dflt.data(), sizeof(int) * b->ncases, cudaMemcpyHostToDevice, b->stream));
-    batch_set_clocks_kernel<<<b->ncases, 128, 0, b->stream>>>(b->d_cases, b->ncases, t, b->d_flags);
+    QB_CK(cudaMemcpyAsync(b->d_small, b->h_small, sizeof(double) * ((size_t)b->soff[nc] + nc), cudaMemcpyHostToDevice,
+                          b->stream));
+    batch_scatter_small_kernel<<<nc, 128, 0, b->stream>>>(b->d_cases, nc, b->d_small, b->d_soff);
+    QB_CK(cudaGetLastError());
+    // the clocks of every case in one launch, after the copies above
+    batch_set_clocks_kernel<<<nc, 128, 0, b->stream>>>(b->d_cases, nc, t);
     QB_CK(cudaGetLastError());
     QB_CK(cudaStreamSynchronize(b->stream));
     return QLGPU_OK;
@@ -1066,24 +1107,27 @@ int qlgpu_batch_get_states(qlgpu_batch_t* b, double* t, double* const* lin, doub
         int rc = upload_descriptors(b);
         if (rc) return rc;
     }
-    for (int c = 0; c < b->ncases; ++c) {
+    const int nc = b->ncases;
+    for (int c = 0; c < nc; ++c) {
         CaseHost& h = b->cs[c];
-        const size_t nlin = (size_t)h.nxy * 4 * h.nz, nmfe = (size_t)h.nmf * h.nz;
+        const size_t nlin = (size_t)h.nxy * 4 * h.nz;
         if (lin && lin[c])
             QB_CK(cudaMemcpyAsync(lin[c], h.lin[b->cur], nlin * sizeof(cplx), cudaMemcpyDeviceToHost, b->stream));
-        if (mf && mf[c]) QB_CK(cudaMemcpyAsync(mf[c], h.mf, nmfe * sizeof(cplx), cudaMemcpyDeviceToHost, b->stream));
-        if (kx0 && kx0[c])
-            QB_CK(cudaMemcpyAsync(kx0[c], h.kx0, h.nxy * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
     }
-    std::vector<double> tt(b->ncases, 0.0);
-    if (t) {
-        batch_gather_t_kernel<<<1, 128, 0, b->stream>>>(b->d_cases, b->ncases, b->d_tvec);
-        QB_CK(cudaGetLastError());
-        QB_CK(cudaMemcpyAsync(tt.data(), b->d_tvec, sizeof(double) * b->ncases, cudaMemcpyDeviceToHost, b->stream));
-    }
+    // the mean fields, kx0 and clocks of every case through the staging block: one copy
+    batch_gather_small_kernel<<<nc, 128, 0, b->stream>>>(b->d_cases, nc, b->d_small, b->d_soff);
+    QB_CK(cudaGetLastError());
+    QB_CK(cudaMemcpyAsync(b->h_small, b->d_small, sizeof(double) * ((size_t)b->soff[nc] + nc), cudaMemcpyDeviceToHost,
+                          b->stream));
     QB_CK(cudaStreamSynchronize(b->stream));
-    if (t)
-        for (int c = 0; c < b->ncases; ++c) t[c] = tt[c];
+    for (int c = 0; c < nc; ++c) {
+        const CaseHost& h = b->cs[c];
+        const size_t nmfe = (size_t)h.nmf * h.nz;
+        const double* sp = b->h_small + b->soff[c];
+        if (mf && mf[c]) std::memcpy(mf[c], sp, nmfe * sizeof(cplx));
+        if (kx0 && kx0[c]) std::memcpy(kx0[c], sp + 2 * nmfe, h.nxy * sizeof(double));
+        if (t) t[c] = b->h_small[b->soff[nc] + c];
+    }
     return QLGPU_OK;
 }
 
@@ -1111,9 +1155,12 @@ int qlgpu_batch_step(qlgpu_batch_t* b, int nsteps, int diag_every, double* diag_
     if (diag_every > 0 && b->diag_cap != max_diag) {
         // one block for every case's records, laid out as diag_out: [case][max_diag][15]
         if (b->d_diag) cudaFree(b->d_diag);
+        if (b->h_diag) cudaFreeHost(b->h_diag);
         b->d_diag = nullptr;
+        b->h_diag = nullptr;
         b->diag_cap = 0;
         QB_CK(cudaMalloc(&b->d_diag, sizeof(double) * 15 * (size_t)max_diag * b->ncases));
+        QB_CK(cudaHostAlloc(&b->h_diag, sizeof(double) * 15 * (size_t)max_diag * b->ncases, cudaHostAllocDefault));
         b->diag_cap = max_diag;
         for (int c = 0; c < b->ncases; ++c) {
             b->cs[c].diag = b->d_diag + (size_t)c * max_diag * 15;
@@ -1131,14 +1178,16 @@ int qlgpu_batch_step(qlgpu_batch_t* b, int nsteps, int diag_every, double* diag_
     int rc = run_launch(b, nsteps, diag_every > 0 ? 1 : 0);
     if (rc) return rc;
     const int nc = b->ncases;
-    std::vector<int> col(2 * (size_t)nc + 2);
+    // the statuses and records come back through pinned buffers (asynchronous copies)
     batch_collect_kernel<<<(nc + 127) / 128, 128, 0, b->stream>>>(b->d_cases, nc, b->d_ctl, b->d_collect);
     QB_CK(cudaGetLastError());
-    QB_CK(cudaMemcpyAsync(col.data(), b->d_collect, col.size() * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
-    if (diag_every > 0)
-        QB_CK(cudaMemcpyAsync(diag_out, b->d_diag, sizeof(double) * 15 * (size_t)max_diag * nc,
-                              cudaMemcpyDeviceToHost, b->stream));
+    QB_CK(cudaMemcpyAsync(b->h_col, b->d_collect, sizeof(int) * (2 * (size_t)nc + 2), cudaMemcpyDeviceToHost,
+                          b->stream));
+    const size_t rec_bytes = sizeof(double) * 15 * (size_t)max_diag * nc;
+    if (diag_every > 0) QB_CK(cudaMemcpyAsync(b->h_diag, b->d_diag, rec_bytes, cudaMemcpyDeviceToHost, b->stream));
     QB_CK(cudaStreamSynchronize(b->stream));
+    const int* col = b->h_col;
+    if (diag_every > 0) std::memcpy(diag_out, b->h_diag, rec_bytes);
     if (col[2 * nc] & QLGPU_STATUS_TIMEOUT) return check_launch_status(b);
     int bad = -1;
     for (int c = 0; c < nc; ++c) {
@@ -1208,17 +1257,20 @@ int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms) {
             int rc = queue_plan(b);
             if (rc) return rc;
         }
+        // a probe: the best of three launches of at least 6 steps after a warm-up launch (one
+        // short launch per candidate let launch-to-launch noise pick the passes)
+        const int qsteps = std::max(probe_steps, 6);
         auto qprobe = [&](double* ms) -> int {
             QB_CK(ensure_smem_attr(ens::kernel(b->integ), b->qsmem));
             double best_of = 1e300;
-            for (int rep = 0; rep < 2; ++rep) {  // the first launch of a plan is a warm-up
+            for (int rep = 0; rep < 4; ++rep) {  // the first launch of a plan is a warm-up
                 QB_CK(cudaEventRecord(b->ev[0], b->stream));
-                QB_CK(enqueue_queue(b, probe_steps, 0));
+                QB_CK(enqueue_queue(b, qsteps, 0));
                 QB_CK(cudaEventRecord(b->ev[1], b->stream));
                 QB_CK(cudaEventSynchronize(b->ev[1]));
                 float f = 0;
                 QB_CK(cudaEventElapsedTime(&f, b->ev[0], b->ev[1]));
-                b->cur = (b->cur + probe_steps) & 1;
+                b->cur = (b->cur + qsteps) & 1;
                 int rc = check_launch_status(b);
                 if (rc) return rc;
                 if (rep > 0) best_of = std::min(best_of, (double)f);
@@ -1231,25 +1283,27 @@ int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms) {
         double best = 0;
         int rc = qprobe(&best);
         if (rc) return rc;
-        for (int cls = 3; cls >= 0; --cls) {
-            if (!present[cls]) continue;
-            const int keep = b->qpasses[cls];
-            int bestp = keep;
-            for (int pp : {1, 2, 3, 4, 6, 8}) {
-                if (pp == keep) continue;
-                b->qpasses[cls] = pp;
-                rc = queue_plan(b);
-                if (rc) return rc;
-                double ms = 0;
-                rc = qprobe(&ms);
-                if (rc) return rc;
-                if (ms < best) {
-                    best = ms;
-                    bestp = pp;
+        // two sweeps: the best passes of a class depend on the other classes' chunks
+        for (int sweep = 0; sweep < 2; ++sweep)
+            for (int cls = 3; cls >= 0; --cls) {
+                if (!present[cls]) continue;
+                const int keep = b->qpasses[cls];
+                int bestp = keep;
+                for (int pp : {1, 2, 3, 4, 6, 8}) {
+                    if (pp == keep) continue;
+                    b->qpasses[cls] = pp;
+                    rc = queue_plan(b);
+                    if (rc) return rc;
+                    double ms = 0;
+                    rc = qprobe(&ms);
+                    if (rc) return rc;
+                    if (ms < best) {
+                        best = ms;
+                        bestp = pp;
+                    }
                 }
+                b->qpasses[cls] = bestp;
             }
-            b->qpasses[cls] = bestp;
-        }
         rc = queue_plan(b);
         if (rc) return rc;
         if (best_ms) *best_ms = best;
