@@ -554,9 +554,11 @@ def run_gpu(args):
         pin_out.append((pinned_like(lin), pinned_like(mf), pinned_like(kx0)))
     ext = torch.cuda.ExternalStream(batch.stream())
 
-    def e2e_run(per_step: bool):
+    def e2e_run(per_step):
         """State of all cases in from pinned host memory, K steps with the energy / stress /
-        dissipation record of every step read back, state of all cases out."""
+        dissipation record of every step read back, state of all cases out.  per_step: "async"
+        (one call per step, each step's records collected while the next step runs), "sync"
+        (one call per step that returns its records) or False (one call for the K steps)."""
         torch.cuda.synchronize()
         barrier(ws)
         ee0 = torch.cuda.Event(enable_timing=True)
@@ -566,7 +568,14 @@ def run_gpu(args):
         batch.set_states(0.0, pin_in)
         h1 = time.perf_counter()
         recs_all = [[] for _ in range(NCASES)]
-        if per_step:
+        if per_step == "async":
+            batch.step_async(1, diag_every=1)
+            for s in range(args.steps):
+                if s + 1 < args.steps:
+                    batch.step_async(1, diag_every=1)
+                for c, r in enumerate(batch.step_collect()):
+                    recs_all[c].append(r)
+        elif per_step == "sync":
             for _ in range(args.steps):
                 for c, r in enumerate(batch.step(1, diag_every=1)):
                     recs_all[c].append(r)
@@ -603,17 +612,22 @@ def run_gpu(args):
         ee1.synchronize()
         return max_over_ranks(ws, ee0.elapsed_time(ee1))
 
-    e2e_run(True)  # warm-up of the one-step graph
-    e2e_ms, recs_all, outs, phases = e2e_run(True)
+    e2e_run("async")  # warm-up of the one-step graph
+    e2e_ms, recs_all, outs, phases = e2e_run("async")
+    sync_ms, _, _, sync_phases = e2e_run("sync")
     one_ms, _, _, one_phases = e2e_run(False)
     rt_ms = e2e_roundtrip()
     state_bytes = sum(lin.nbytes + mf.nbytes + kx0.nbytes for lin, mf, kx0 in sts)
     e2e = {"value": job_modes * args.steps / (e2e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": state_bytes / args.steps,
            "d2h_bytes_per_step": NCASES * 15 * 8 + state_bytes / args.steps,
-           "path": "QLBatch.set_states (pinned, all 48 cases), K x QLBatch.step(1, diag_every=1) (one launch and "
-                   "the 48 records read back per step), QLBatch.get_states (pinned)",
+           "path": "QLBatch.set_states (pinned, all 48 cases), K x QLBatch.step_async(1, diag_every=1) (one "
+                   "launch per step; the 48 records of each step read back by QLBatch.step_collect while the "
+                   "next step runs), QLBatch.get_states (pinned)",
            "phases_host_ms": phases,
+           "per_step_sync": {"value": job_modes * args.steps / (sync_ms / 1e3), "unit": UNIT,
+                             "path": "as above with K x QLBatch.step(1, diag_every=1), each call waiting for its "
+                                     "step and records", "phases_host_ms": sync_phases},
            "one_call": {"value": job_modes * args.steps / (one_ms / 1e3), "unit": UNIT,
                         "path": "as above with one QLBatch.step(K, diag_every=1): one launch, every step's 48 "
                                 "records read back after it", "phases_host_ms": one_phases},

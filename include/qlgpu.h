@@ -288,6 +288,17 @@ int qlgpu_batch_diagnostics(qlgpu_batch_t* b, int c, double* out15);
  * diag_out + c*max_diag*15 and its count to ndiag[c]. */
 int qlgpu_batch_step(qlgpu_batch_t* b, int nsteps, int diag_every, double* diag_out, int max_diag, int* ndiag);
 
+/* Asynchronous stepping, for a caller that reads every step's records while the
+ * next steps run: qlgpu_batch_step_async queues nsteps steps of every case (one
+ * launch) and the copy of their records and statuses into pinned memory, and
+ * returns without waiting.  At most two calls are outstanding.
+ * qlgpu_batch_step_collect waits for the oldest and returns its records and
+ * status as qlgpu_batch_step does (max_diag as given to its step_async).  The
+ * other batch calls that step, tune or move state refuse while a step is
+ * outstanding (QLGPU_ERR_ARG). */
+int qlgpu_batch_step_async(qlgpu_batch_t* b, int nsteps, int diag_every, int max_diag);
+int qlgpu_batch_step_collect(qlgpu_batch_t* b, double* diag_out, int max_diag, int* ndiag);
+
 /* As qlgpu_batch_step without diagnostics; *ms = device time of the launch
  * (CUDA events on the batch stream). */
 int qlgpu_batch_step_timed(qlgpu_batch_t* b, int nsteps, float* ms);

@@ -29,6 +29,7 @@ EXPORTS = ["qlgpu_create", "qlgpu_destroy", "qlgpu_dims", "qlgpu_set_state", "ql
            "qlgpu_adjoint_maxwell",
            "qlgpu_batch_create", "qlgpu_batch_destroy", "qlgpu_batch_dims", "qlgpu_batch_set_state",
            "qlgpu_batch_get_state", "qlgpu_batch_diagnostics", "qlgpu_batch_step", "qlgpu_batch_step_timed",
+           "qlgpu_batch_step_async", "qlgpu_batch_step_collect",
            "qlgpu_batch_tune", "qlgpu_batch_mapping", "qlgpu_batch_set_mapping", "qlgpu_batch_status",
            "qlgpu_batch_set_wait", "qlgpu_batch_debug_drop_item", "qlgpu_batch_stream",
            "qlgpu_batch_last_error", "qlgpu_batch_set_engine", "qlgpu_batch_engine", "qlgpu_batch_set_chunks",
@@ -123,6 +124,8 @@ def load(path: str | None = None):
     L.qlgpu_batch_diagnostics.argtypes = [vp, ctypes.c_int, dp]
     L.qlgpu_batch_step.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ip]
     L.qlgpu_batch_step_timed.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.qlgpu_batch_step_async.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.qlgpu_batch_step_collect.argtypes = [vp, dp, ctypes.c_int, ip]
     L.qlgpu_batch_tune.argtypes = [vp, ctypes.c_int, dp]
     L.qlgpu_batch_mapping.argtypes = [vp, ip, ip]
     L.qlgpu_batch_set_mapping.argtypes = [vp, ctypes.c_int, ip]

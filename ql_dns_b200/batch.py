@@ -21,6 +21,7 @@ class QLBatch:
 
     def __init__(self, cases: list[QLParams], device: int = -1):
         self.cases = list(cases)
+        self._pending = []  # max_diag of each outstanding step_async call
         self.L = _capi.load()
         arr = (_capi.qlgpu_params * len(cases))(*[_capi.to_c(p) for p in cases])
         b = ctypes.c_void_p()
@@ -127,6 +128,25 @@ class QLBatch:
                               self.b)
             return [out[c, : nd[c]] for c in range(nc)]
         _capi.check_batch(self.L.qlgpu_batch_step(self.b, int(nsteps), 0, None, 0, None), self.b)
+        return [np.zeros((0, 15)) for _ in range(nc)]
+
+    def step_async(self, nsteps: int, diag_every: int = 0) -> None:
+        """Queues nsteps steps of every case and returns at once (at most two outstanding);
+        step_collect() returns the oldest call's records."""
+        cap = nsteps // diag_every + 2 if diag_every > 0 else 0
+        _capi.check_batch(self.L.qlgpu_batch_step_async(self.b, int(nsteps), int(diag_every), cap), self.b)
+        self._pending.append(cap)
+
+    def step_collect(self) -> list[np.ndarray]:
+        """Waits for the oldest step_async call; per case its diagnostic records [n, 15]."""
+        nc = len(self.cases)
+        cap = self._pending.pop(0)
+        if cap > 0:
+            out = np.zeros((nc, cap, 15))
+            nd = (ctypes.c_int * nc)()
+            _capi.check_batch(self.L.qlgpu_batch_step_collect(self.b, _capi.dptr(out), cap, nd), self.b)
+            return [out[c, : nd[c]] for c in range(nc)]
+        _capi.check_batch(self.L.qlgpu_batch_step_collect(self.b, None, 0, None), self.b)
         return [np.zeros((0, 15)) for _ in range(nc)]
 
     def step_timed(self, nsteps: int) -> float:

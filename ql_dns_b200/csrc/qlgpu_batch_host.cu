@@ -235,6 +235,16 @@ struct qlgpu_batch {
     double* h_small = nullptr;               // pinned
     int* h_col = nullptr;                    // pinned copy of d_collect
     double* h_diag = nullptr;                // pinned copy of d_diag
+    // asynchronous steps (qlgpu_batch_step_async): a ring of two slots, each with pinned copies of
+    // the launch's statuses, control block and records, and an event after those copies
+    struct AsyncSlot {
+        int* col = nullptr;
+        BatchCtl* ctl = nullptr;
+        double* diag = nullptr;
+        cudaEvent_t done = nullptr;
+        int diag_every = 0, max_diag = 0;
+    } aslot[2];
+    int a_head = 0, a_count = 0;
     NoiseSpec* d_noise = nullptr;            // [ncases] driving-noise constants
     GuardList guards;                        // debug build: canary zones after the device buffers
 };
@@ -731,20 +741,58 @@ int debug_verify(qlgpu_batch_t* b) {
     return QLGPU_OK;
 }
 
+int launch_timeout(qlgpu_batch_t* b, const BatchCtl& ctl) {
+    char buf[200];
+    std::snprintf(buf, sizeof(buf),
+                  "batch: a CTA gave up waiting %s case %d at stage %d (wait bound %.3g s); the state of the "
+                  "batch is undefined",
+                  ctl.fail_where == 1 ? "for a staged copy of" : "for", ctl.fail_case, ctl.fail_stage,
+                  b->wait_ns * 1e-9);
+    return bfail(b, QLGPU_ERR_STATUS, buf);
+}
+
 int check_launch_status(qlgpu_batch_t* b) {
     BatchCtl ctl;
     QB_CK(cudaMemcpyAsync(&ctl, b->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, b->stream));
     QB_CK(cudaStreamSynchronize(b->stream));
-    if (ctl.status & QLGPU_STATUS_TIMEOUT) {
-        char buf[200];
-        std::snprintf(buf, sizeof(buf),
-                      "batch: a CTA gave up waiting %s case %d at stage %d (wait bound %.3g s); the state of the "
-                      "batch is undefined",
-                      ctl.fail_where == 1 ? "for a staged copy of" : "for", ctl.fail_case, ctl.fail_stage,
-                      b->wait_ns * 1e-9);
+    if (ctl.status & QLGPU_STATUS_TIMEOUT) return launch_timeout(b, ctl);
+    return debug_verify(b);
+}
+
+// One block for every case's records, laid out as the callers' diag_out: [case][max_diag][15].
+int alloc_records(qlgpu_batch_t* b, int max_diag) {
+    if (b->d_diag) cudaFree(b->d_diag);
+    if (b->h_diag) cudaFreeHost(b->h_diag);
+    b->d_diag = nullptr;
+    b->h_diag = nullptr;
+    b->diag_cap = 0;
+    QB_CK(cudaMalloc(&b->d_diag, sizeof(double) * 15 * (size_t)max_diag * b->ncases));
+    QB_CK(cudaHostAlloc(&b->h_diag, sizeof(double) * 15 * (size_t)max_diag * b->ncases, cudaHostAllocDefault));
+    b->diag_cap = max_diag;
+    for (int c = 0; c < b->ncases; ++c) {
+        b->cs[c].diag = b->d_diag + (size_t)c * max_diag * 15;
+        b->cs[c].diag_cap = max_diag;
+    }
+    b->descr_dirty = true;
+    return QLGPU_OK;
+}
+
+// Record counts and case statuses of a finished step launch (col = batch_collect_kernel's output).
+int step_records(qlgpu_batch_t* b, const int* col, int diag_every, int max_diag, int* ndiag) {
+    const int nc = b->ncases;
+    int bad = -1;
+    for (int c = 0; c < nc; ++c) {
+        if (diag_every > 0) ndiag[c] = std::min(col[2 * c + 1], max_diag);
+        if (bad < 0 && (col[2 * c] & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE | QLGPU_STATUS_DIAG_FULL)))
+            bad = c;
+    }
+    if (bad >= 0) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "case %d: device status 0x%x (non-finite, unstable or records dropped)", bad,
+                      col[2 * bad]);
         return bfail(b, QLGPU_ERR_STATUS, buf);
     }
-    return debug_verify(b);
+    return QLGPU_OK;
 }
 
 int reset_case_clock(qlgpu_batch_t* b, int c, double t) {
@@ -779,6 +827,12 @@ int qlgpu_batch_destroy(qlgpu_batch_t* b) {
     if (b->h_small) cudaFreeHost(b->h_small);
     if (b->h_col) cudaFreeHost(b->h_col);
     if (b->h_diag) cudaFreeHost(b->h_diag);
+    for (auto& a : b->aslot) {
+        if (a.col) cudaFreeHost(a.col);
+        if (a.ctl) cudaFreeHost(a.ctl);
+        if (a.diag) cudaFreeHost(a.diag);
+        if (a.done) cudaEventDestroy(a.done);
+    }
     for (cudaEvent_t e : b->ev)
         if (e) cudaEventDestroy(e);
     guard_release(b->guards);
@@ -1037,6 +1091,7 @@ int qlgpu_batch_dims(const qlgpu_batch_t* b, int c, int* nxy, int* nz, int* nmf)
 
 int qlgpu_batch_set_state(qlgpu_batch_t* b, int c, double t, const double* lin, const double* mf, const double* kx0) {
     if (!b) return QLGPU_ERR_ARG;
+    if (b->a_count) return bfail(b, QLGPU_ERR_ARG, "asynchronous steps outstanding: collect them first");
     if (c < 0 || c >= b->ncases || !lin || !mf) return bfail(b, QLGPU_ERR_ARG, "bad case index or null state");
     QB_CK(cudaSetDevice(b->device));
     CaseHost& h = b->cs[c];
@@ -1053,6 +1108,7 @@ int qlgpu_batch_set_state(qlgpu_batch_t* b, int c, double t, const double* lin, 
 
 int qlgpu_batch_get_state(qlgpu_batch_t* b, int c, double* t, double* lin, double* mf, double* kx0) {
     if (!b) return QLGPU_ERR_ARG;
+    if (b->a_count) return bfail(b, QLGPU_ERR_ARG, "asynchronous steps outstanding: collect them first");
     if (c < 0 || c >= b->ncases) return bfail(b, QLGPU_ERR_ARG, "bad case index");
     QB_CK(cudaSetDevice(b->device));
     CaseHost& h = b->cs[c];
@@ -1072,6 +1128,7 @@ int qlgpu_batch_set_states(qlgpu_batch_t* b, double t, const double* const* lin,
     if (!b || !lin || !mf) return QLGPU_ERR_ARG;
     for (int c = 0; c < b->ncases; ++c)
         if (!lin[c] || !mf[c]) return bfail(b, QLGPU_ERR_ARG, "null state of case " + std::to_string(c));
+    if (b->a_count) return bfail(b, QLGPU_ERR_ARG, "asynchronous steps outstanding: collect them first");
     QB_CK(cudaSetDevice(b->device));
     if (b->descr_dirty) {
         int rc = upload_descriptors(b);
@@ -1102,6 +1159,7 @@ int qlgpu_batch_set_states(qlgpu_batch_t* b, double t, const double* const* lin,
 
 int qlgpu_batch_get_states(qlgpu_batch_t* b, double* t, double* const* lin, double* const* mf, double* const* kx0) {
     if (!b) return QLGPU_ERR_ARG;
+    if (b->a_count) return bfail(b, QLGPU_ERR_ARG, "asynchronous steps outstanding: collect them first");
     QB_CK(cudaSetDevice(b->device));
     if (b->descr_dirty) {
         int rc = upload_descriptors(b);
@@ -1148,25 +1206,14 @@ int qlgpu_batch_diagnostics(qlgpu_batch_t* b, int c, double* out15) {
 
 int qlgpu_batch_step(qlgpu_batch_t* b, int nsteps, int diag_every, double* diag_out, int max_diag, int* ndiag) {
     if (!b) return QLGPU_ERR_ARG;
+    if (b->a_count) return bfail(b, QLGPU_ERR_ARG, "asynchronous steps outstanding: collect them first");
     if (nsteps < 0) return bfail(b, QLGPU_ERR_ARG, "nsteps < 0");
     if (diag_every > 0 && (!diag_out || !ndiag || max_diag < 1))
         return bfail(b, QLGPU_ERR_ARG, "diag_out, ndiag and max_diag >= 1 required");
     QB_CK(cudaSetDevice(b->device));
     if (diag_every > 0 && b->diag_cap != max_diag) {
-        // one block for every case's records, laid out as diag_out: [case][max_diag][15]
-        if (b->d_diag) cudaFree(b->d_diag);
-        if (b->h_diag) cudaFreeHost(b->h_diag);
-        b->d_diag = nullptr;
-        b->h_diag = nullptr;
-        b->diag_cap = 0;
-        QB_CK(cudaMalloc(&b->d_diag, sizeof(double) * 15 * (size_t)max_diag * b->ncases));
-        QB_CK(cudaHostAlloc(&b->h_diag, sizeof(double) * 15 * (size_t)max_diag * b->ncases, cudaHostAllocDefault));
-        b->diag_cap = max_diag;
-        for (int c = 0; c < b->ncases; ++c) {
-            b->cs[c].diag = b->d_diag + (size_t)c * max_diag * 15;
-            b->cs[c].diag_cap = max_diag;
-        }
-        b->descr_dirty = true;
+        int rc = alloc_records(b, max_diag);
+        if (rc) return rc;
     }
     for (int c = 0; c < b->ncases; ++c) {
         const double tv = diag_every > 0 ? diag_every * b->cs[c].p.dt : 0.0;
@@ -1186,26 +1233,82 @@ int qlgpu_batch_step(qlgpu_batch_t* b, int nsteps, int diag_every, double* diag_
     const size_t rec_bytes = sizeof(double) * 15 * (size_t)max_diag * nc;
     if (diag_every > 0) QB_CK(cudaMemcpyAsync(b->h_diag, b->d_diag, rec_bytes, cudaMemcpyDeviceToHost, b->stream));
     QB_CK(cudaStreamSynchronize(b->stream));
-    const int* col = b->h_col;
     if (diag_every > 0) std::memcpy(diag_out, b->h_diag, rec_bytes);
-    if (col[2 * nc] & QLGPU_STATUS_TIMEOUT) return check_launch_status(b);
-    int bad = -1;
-    for (int c = 0; c < nc; ++c) {
-        if (diag_every > 0) ndiag[c] = std::min(col[2 * c + 1], max_diag);
-        if (bad < 0 && (col[2 * c] & (QLGPU_STATUS_NONFINITE | QLGPU_STATUS_UNSTABLE | QLGPU_STATUS_DIAG_FULL)))
-            bad = c;
-    }
-    if (bad >= 0) {
-        char buf[160];
-        std::snprintf(buf, sizeof(buf), "case %d: device status 0x%x (non-finite, unstable or records dropped)", bad,
-                      col[2 * bad]);
-        return bfail(b, QLGPU_ERR_STATUS, buf);
-    }
+    if (b->h_col[2 * nc] & QLGPU_STATUS_TIMEOUT) return check_launch_status(b);
+    int rc2 = step_records(b, b->h_col, diag_every, max_diag, ndiag);
+    if (rc2) return rc2;
     return debug_verify(b);
+}
+
+int qlgpu_batch_step_async(qlgpu_batch_t* b, int nsteps, int diag_every, int max_diag) {
+    if (!b) return QLGPU_ERR_ARG;
+    if (nsteps < 1) return bfail(b, QLGPU_ERR_ARG, "nsteps < 1");
+    if (diag_every > 0 && max_diag < 1) return bfail(b, QLGPU_ERR_ARG, "max_diag >= 1 required");
+    if (b->a_count == 2) return bfail(b, QLGPU_ERR_ARG, "two asynchronous steps outstanding: collect one first");
+    QB_CK(cudaSetDevice(b->device));
+    const int nc = b->ncases;
+    if (diag_every > 0 && b->diag_cap != max_diag) {
+        if (b->a_count) return bfail(b, QLGPU_ERR_ARG, "max_diag differs from the outstanding step's");
+        int rc = alloc_records(b, max_diag);
+        if (rc) return rc;
+    }
+    for (int c = 0; c < nc; ++c) {
+        const double tv = diag_every > 0 ? diag_every * b->cs[c].p.dt : 0.0;
+        if (tv != b->tv_set[c]) {
+            b->tv_set[c] = tv;
+            b->descr_dirty = true;
+        }
+    }
+    // new descriptors must not be written under a running launch
+    if (b->descr_dirty && b->a_count) QB_CK(cudaStreamSynchronize(b->stream));
+    const int slot = (b->a_head + b->a_count) & 1;
+    qlgpu_batch::AsyncSlot& a = b->aslot[slot];
+    if (!a.col) {
+        QB_CK(cudaHostAlloc(&a.col, sizeof(int) * (2 * (size_t)nc + 2), cudaHostAllocDefault));
+        QB_CK(cudaHostAlloc(&a.ctl, sizeof(BatchCtl), cudaHostAllocDefault));
+        QB_CK(cudaEventCreateWithFlags(&a.done, cudaEventDisableTiming));
+    }
+    const size_t rec_bytes = sizeof(double) * 15 * (size_t)std::max(max_diag, 1) * nc;
+    if (diag_every > 0 && a.max_diag != max_diag) {
+        if (a.diag) cudaFreeHost(a.diag);
+        a.diag = nullptr;
+        a.max_diag = 0;
+        QB_CK(cudaHostAlloc(&a.diag, rec_bytes, cudaHostAllocDefault));
+        a.max_diag = max_diag;
+    }
+    int rc = run_launch(b, nsteps, diag_every > 0 ? 1 : 0);
+    if (rc) return rc;
+    // the copies are queued behind the launch and ahead of the next one, which reuses the buffers
+    batch_collect_kernel<<<(nc + 127) / 128, 128, 0, b->stream>>>(b->d_cases, nc, b->d_ctl, b->d_collect);
+    QB_CK(cudaGetLastError());
+    QB_CK(cudaMemcpyAsync(a.col, b->d_collect, sizeof(int) * (2 * (size_t)nc + 2), cudaMemcpyDeviceToHost, b->stream));
+    QB_CK(cudaMemcpyAsync(a.ctl, b->d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, b->stream));
+    if (diag_every > 0) QB_CK(cudaMemcpyAsync(a.diag, b->d_diag, rec_bytes, cudaMemcpyDeviceToHost, b->stream));
+    QB_CK(cudaEventRecord(a.done, b->stream));
+    a.diag_every = diag_every;
+    b->a_count += 1;
+    return QLGPU_OK;
+}
+
+int qlgpu_batch_step_collect(qlgpu_batch_t* b, double* diag_out, int max_diag, int* ndiag) {
+    if (!b) return QLGPU_ERR_ARG;
+    if (b->a_count == 0) return bfail(b, QLGPU_ERR_ARG, "no asynchronous step outstanding");
+    qlgpu_batch::AsyncSlot& a = b->aslot[b->a_head];
+    if (a.diag_every > 0 && (!diag_out || !ndiag || max_diag != a.max_diag))
+        return bfail(b, QLGPU_ERR_ARG, "diag_out, ndiag and the step's max_diag required");
+    QB_CK(cudaSetDevice(b->device));
+    QB_CK(cudaEventSynchronize(a.done));
+    b->a_head ^= 1;
+    b->a_count -= 1;
+    const int nc = b->ncases;
+    if (a.diag_every > 0) std::memcpy(diag_out, a.diag, sizeof(double) * 15 * (size_t)max_diag * nc);
+    if (a.col[2 * nc] & QLGPU_STATUS_TIMEOUT) return launch_timeout(b, *a.ctl);
+    return step_records(b, a.col, a.diag_every, max_diag, ndiag);
 }
 
 int qlgpu_batch_step_timed(qlgpu_batch_t* b, int nsteps, float* ms) {
     if (!b || !ms || nsteps < 1) return QLGPU_ERR_ARG;
+    if (b->a_count) return bfail(b, QLGPU_ERR_ARG, "asynchronous steps outstanding: collect them first");
     QB_CK(cudaSetDevice(b->device));
     for (int c = 0; c < b->ncases; ++c)
         if (b->tv_set[c] != 0.0) {
@@ -1226,6 +1329,7 @@ int qlgpu_batch_step_timed(qlgpu_batch_t* b, int nsteps, float* ms) {
 
 int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms) {
     if (!b || probe_steps < 1) return QLGPU_ERR_ARG;
+    if (b->a_count) return bfail(b, QLGPU_ERR_ARG, "asynchronous steps outstanding: collect them first");
     QB_CK(cudaSetDevice(b->device));
     // probes run on the batch's own buffers; a copy of the whole arena is restored afterwards
     unsigned char* backup = nullptr;

@@ -343,6 +343,40 @@ def test_set_states_get_states_match_per_case_calls(engine):
 
 
 @pytest.mark.parametrize("engine", ["queue", "items"])
+def test_step_async_matches_step(engine):
+    # two outstanding one-step calls at a time, every step's records collected while the next
+    # step runs: the same records and state as one synchronous call per step
+    from ql_dns_b200._capi import QLGPUError
+    cases = bq_cases()[:5]
+    sts = states(cases)
+    require_gpu()
+    with QLBatch(cases) as b:
+        b.set_engine(engine)
+        b.set_states(0.0, sts)
+        sync = [b.step(1, diag_every=1) for _ in range(5)]
+        a = b.get_states()
+        b.set_states(0.0, sts)
+        got = []
+        b.step_async(1, diag_every=1)
+        for _ in range(4):
+            b.step_async(1, diag_every=1)
+            with pytest.raises(QLGPUError):
+                b.step_async(1, diag_every=1)  # a third outstanding call
+            with pytest.raises(QLGPUError):
+                b.get_states()  # state moves wait for the outstanding steps
+            got.append(b.step_collect())
+        got.append(b.step_collect())
+        with pytest.raises(QLGPUError):
+            b.step_collect()  # nothing outstanding
+        g = b.get_states()
+    for rs, rg in zip(sync, got):
+        for x, y in zip(rs, rg):
+            assert x.shape == (1, 15) and np.array_equal(x, y)
+    for x, y in zip(a, g):
+        assert x[0] == y[0] and np.array_equal(x[1], y[1]) and np.array_equal(x[2], y[2])
+
+
+@pytest.mark.parametrize("engine", ["queue", "items"])
 def test_batch_noise_per_case_matches_oracle(engine):
     # Model::DrivingNoise inside the batch step (main.cpp:111-113): each case its own
     # f_noise, band and seed, or none; the counter restarts with the case's state
