@@ -140,7 +140,7 @@ class QLBatch:
     def step_collect(self) -> list[np.ndarray]:
         """Waits for the oldest step_async call; per case its diagnostic records [n, 15]."""
         nc = len(self.cases)
-        cap = self._pending.pop(0)
+        cap = self._pending.pop(0) if self._pending else 0  # none outstanding: the C call refuses
         if cap > 0:
             out = np.zeros((nc, cap, 15))
             nd = (ctypes.c_int * nc)()
