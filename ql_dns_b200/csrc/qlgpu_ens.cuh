@@ -258,10 +258,15 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(a) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+// proxy_fence: the destination may hold generic-proxy stores (the previous chunk's sums and
+// mean-field scratch reuse the staging buffers), which must be ordered before the async-proxy
+// write.  Within a chunk the buffer is only read by generic loads, which have returned before
+// the warp barrier that precedes the next copy, so no fence is needed there.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar,
+                                          bool proxy_fence) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    if (proxy_fence) asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(bytes) : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(d),
                  "l"(src), "r"(bytes), "r"(b)
@@ -418,7 +423,8 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
     // a pair past the chunk's end stages the chunk's last mode (finite values; its stores and sums
     // are switched off)
     const bool leader = (role == 0 && t == 0);
-    if (leader && first < mend) bulk_load(stg, lin_in + (size_t)min(first + pi, mend - 1) * 4 * nzd, fbytes, bar);
+    if (leader && first < mend)
+        bulk_load(stg, lin_in + (size_t)min(first + pi, mend - 1) * 4 * nzd, fbytes, bar, true);
     // the mode's wavenumbers are loaded one mode ahead (their latency overlaps the previous mode)
     double nky = 0.0, nkx0 = 0.0;
     int nkyi = 0, nkxi = 0;
@@ -868,7 +874,8 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         __syncwarp();  // every lane is done with the staging buffer and K
         {
             const int wn = wb + MPP;
-            if (leader && wn < mend) bulk_load(stg, lin_in + (size_t)min(wn + pi, mend - 1) * 4 * nzd, fbytes, bar);
+            if (leader && wn < mend)
+                bulk_load(stg, lin_in + (size_t)min(wn + pi, mend - 1) * 4 * nzd, fbytes, bar, false);
         }
         if (A.noise) {
             // Model::DrivingNoise after the step (main.cpp:111-113), before the diagnostics see it
