@@ -550,11 +550,13 @@ void default_passes(qlgpu_batch_t* b) {
     std::copy(best, best + 4, b->qpasses);
 }
 
-bool queue_usable(const qlgpu_batch_t* b) {
-    if (!b->queue_ok || b->engine != QLGPU_BATCH_ENGINE_QUEUE) return false;
+bool queue_usable(const qlgpu_batch_t* b) { return b->queue_ok && b->engine == QLGPU_BATCH_ENGINE_QUEUE; }
+
+// Some case records its stage inputs: the queue engine's recording build runs.
+bool queue_rec(const qlgpu_batch_t* b) {
     for (const CaseHost& h : b->cs)
-        if (h.rec_lin) return false;  // the stage-input record is a work-item engine feature
-    return true;
+        if (h.rec_lin) return true;
+    return false;
 }
 
 // Chunks per stage of every case (passes per chunk of its NZ class, raised until
@@ -601,7 +603,7 @@ int queue_plan(qlgpu_batch_t* b) {
                           cudaMemcpyHostToDevice, b->stream));
     QB_CK(cudaMemcpyAsync(b->d_ec, b->ec.data(), sizeof(ens::EnsCase) * nc, cudaMemcpyHostToDevice, b->stream));
     QB_CK(cudaStreamSynchronize(b->stream));
-    const void* k = ens::kernel(b->integ);
+    const void* k = ens::kernel(b->integ, queue_rec(b));
     if (smem > b->smem_optin) return bfail(b, QLGPU_ERR_UNSUPPORTED, "queue engine: shared memory request too large");
     QB_CK(ensure_smem_attr(k, smem));
     int occ = 0;
@@ -638,7 +640,7 @@ cudaError_t enqueue_queue(qlgpu_batch_t* b, int nsteps, int reset_ndiag) {
         e = cudaMemsetAsync(b->d_qtrace, 0, sizeof(unsigned long long) * 4 * b->qgrid, b->stream);
         if (e != cudaSuccess) return e;
     }
-    return ens::launch(b->integ, L, b->qgrid, b->qsmem, b->stream);
+    return ens::launch(b->integ, queue_rec(b), L, b->qgrid, b->qsmem, b->stream);
 }
 
 BatchLaunch launch_args(qlgpu_batch_t* b, int nsteps) {
@@ -679,11 +681,11 @@ int run_launch(qlgpu_batch_t* b, int nsteps, int reset_ndiag, cudaEvent_t ev_bef
         if (rc) return rc;
     }
     // the dynamic shared memory attribute belongs to the kernel, not to this batch
-    if (q) QB_CK(ensure_smem_attr(ens::kernel(b->integ), b->qsmem));
+    if (q) QB_CK(ensure_smem_attr(ens::kernel(b->integ, queue_rec(b)), b->qsmem));
     else QB_CK(ensure_smem_attr(b->bk.kernel(), b->smem));
     auto enqueue = [&]() { return q ? enqueue_queue(b, nsteps, reset_ndiag) : enqueue_launch(b, nsteps, reset_ndiag); };
     if (b->use_graph) {
-        const auto key = std::make_tuple(nsteps, b->cur + (q ? 2 : 0), reset_ndiag);
+        const auto key = std::make_tuple(nsteps, b->cur + (q ? 2 : 0) + (q && queue_rec(b) ? 4 : 0), reset_ndiag);
         auto itg = b->graphs.find(key);
         if (itg == b->graphs.end()) {
             if (b->graphs.size() >= 8) drop_graphs(b);
@@ -1365,7 +1367,7 @@ int qlgpu_batch_tune(qlgpu_batch_t* b, int probe_steps, double* best_ms) {
         // short launch per candidate let launch-to-launch noise pick the passes)
         const int qsteps = std::max(probe_steps, 6);
         auto qprobe = [&](double* ms) -> int {
-            QB_CK(ensure_smem_attr(ens::kernel(b->integ), b->qsmem));
+            QB_CK(ensure_smem_attr(ens::kernel(b->integ, queue_rec(b)), b->qsmem));
             double best_of = 1e300;
             for (int rep = 0; rep < 4; ++rep) {  // the first launch of a plan is a warm-up
                 QB_CK(cudaEventRecord(b->ev[0], b->stream));

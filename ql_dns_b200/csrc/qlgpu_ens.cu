@@ -8,7 +8,7 @@
 namespace qlgpu {
 namespace ens {
 
-template <int INTEG>
+template <int INTEG, bool REC>
 static cudaError_t launch_t(const EnsLaunch& L, int grid, size_t smem, cudaStream_t st) {
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
@@ -21,16 +21,23 @@ static cudaError_t launch_t(const EnsLaunch& L, int grid, size_t smem, cudaStrea
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, ens_kernel<INTEG>, L);
+    return cudaLaunchKernelEx(&cfg, ens_kernel<INTEG, REC>, L);
 }
 
-cudaError_t launch(int integ, const EnsLaunch& L, int grid, size_t smem, cudaStream_t st) {
-    return integ == INTEG_EXP ? launch_t<INTEG_EXP>(L, grid, smem, st) : launch_t<INTEG_CN>(L, grid, smem, st);
+cudaError_t launch(int integ, bool rec, const EnsLaunch& L, int grid, size_t smem, cudaStream_t st) {
+    if (rec)
+        return integ == INTEG_EXP ? launch_t<INTEG_EXP, true>(L, grid, smem, st)
+                                  : launch_t<INTEG_CN, true>(L, grid, smem, st);
+    return integ == INTEG_EXP ? launch_t<INTEG_EXP, false>(L, grid, smem, st)
+                              : launch_t<INTEG_CN, false>(L, grid, smem, st);
 }
 
-const void* kernel(int integ) {
-    return integ == INTEG_EXP ? reinterpret_cast<const void*>(&ens_kernel<INTEG_EXP>)
-                              : reinterpret_cast<const void*>(&ens_kernel<INTEG_CN>);
+const void* kernel(int integ, bool rec) {
+    if (rec)
+        return integ == INTEG_EXP ? reinterpret_cast<const void*>(&ens_kernel<INTEG_EXP, true>)
+                                  : reinterpret_cast<const void*>(&ens_kernel<INTEG_CN, true>);
+    return integ == INTEG_EXP ? reinterpret_cast<const void*>(&ens_kernel<INTEG_EXP, false>)
+                              : reinterpret_cast<const void*>(&ens_kernel<INTEG_CN, false>);
 }
 
 size_t smem_bytes(int NZ) { return chunk_smem(NZ); }

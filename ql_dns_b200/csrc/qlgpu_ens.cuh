@@ -372,7 +372,7 @@ __device__ __noinline__ void top_stage(const EnsLaunch& L, ChunkHdr& hd, int c, 
 // Returns in every thread; the CTA that completed the case's stage ran the
 // mean-field stage and released the case.
 // ---------------------------------------------------------------------------
-template <int NZ, int INTEG>
+template <int NZ, int INTEG, bool REC>
 __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const RoundItem it, const int r,
                                        uint32_t tmem, uint64_t* bars, unsigned char* bar_ph) {
     using E = EG<NZ>;
@@ -459,6 +459,21 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         hd.Om2 = __dmul_rn(2.0, P.Omega);
         hd.has_prev = (S.has_prev && A.Fprev) ? 1 : 0;
         hd.nstep = A.noise ? __ldcg(&A.clk->nstep) : 0ull;
+        // optional record of the stage inputs (the adjoint's window recompute): step n = r / 3
+        // of the launch, stage s, at the layout of the work-item engine's record
+        cplx* rl = cs->rec_lin;
+        StageArgs& W = hd.A;
+        if (rl) {
+            const size_t nlin = (size_t)P.nxy * 4 * nzd, nmfe = (size_t)P.nmf * nzd;
+            W.rec_lin = rl + ((size_t)n * 3 + s) * nlin;
+            W.rec_mf = cs->rec_mf + ((size_t)n * 3 + s) * nmfe;
+            W.rec_kx = s == 0 ? cs->rec_kx + (size_t)n * P.nxy : nullptr;
+            W.rec_t = s == 0 ? cs->rec_t + n : nullptr;
+            W.rec_cn = cs->rec_cn ? cs->rec_cn + (size_t)n * 3 + s : nullptr;
+        } else {
+            W.rec_lin = nullptr;
+            W.rec_mf = nullptr;
+        }
     }
     // ---- tables of the case and stage
     if (fresh) {
@@ -499,6 +514,21 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
     const double* ddBy = prof + 2 * NZ;
     const double* ekz_u = ekz;
     const double* ekz_b = ekz + E::NZE;
+    // the stage's mean fields and, in a step's first stage, kx0 and the clock into the record
+    // (chunk 0 of the case); stable here because the previous stage, its remap and its mean-field
+    // update completed before the stage was released
+    if (REC && A.rec_mf && j == 0) {
+        const int nmfe = P.nmf * nzd;
+        for (int i = tid; i < nmfe; i += THREADS) A.rec_mf[i] = ldc(A.mf + i);
+        if (A.rec_kx)
+            for (int i = tid; i < P.nxy; i += THREADS) A.rec_kx[i] = __ldcg(A.kx0 + i);
+        if (A.rec_t && tid == 0) A.rec_t[0] = __ldcg(&A.clk->t);
+        if (A.rec_cn && tid == 0) {
+            A.rec_cn->t_old = __ldcg(&A.clk->t_old);
+            A.rec_cn->dtlin_old = __ldcg(&A.clk->dtlin_old);
+            A.rec_cn->old_init = __ldcg(&A.clk->old_init);
+        }
+    }
 
     // TMEM scratchpad of this lane (TM_* column offsets)
     const uint32_t ta = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * COLS_PER_WARP);
@@ -565,6 +595,10 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         if (!mbar_wait(bar, phase)) ok = false;
         phase ^= 1u;
         __syncwarp();
+        if (REC && A.rec_lin && valid) {  // record the mode's input fields
+            cplx* dst = A.rec_lin + (size_t)m * 4 * nzd;
+            for (int i = lp; i < 4 * nzd; i += 2 * T) dst[i] = stg[i];
+        }
 
         cplx x[8];
         // spectral input of a plain inverse transform: field f0 + fa over NZ
@@ -1001,7 +1035,7 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
 // ---------------------------------------------------------------------------
 // The persistent kernel: tickets in order, one chunk per ticket.
 // ---------------------------------------------------------------------------
-template <int INTEG>
+template <int INTEG, bool REC>
 __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) ens_kernel(const __grid_constant__ EnsLaunch L) {
     __shared__ ChunkHdr hd;
     __shared__ __align__(8) uint64_t bars[WARPS * MAX_PAIRS_PER_WARP];
@@ -1050,10 +1084,10 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) ens_kernel(const __grid_
         it.c = QLGPU_CHECK_INDEX(it.c, L.ncases, &L.ctl->status);
         const unsigned long long t1 = (L.trace && tid == 0) ? gtimer() : 0ull;
         switch (L.ec[it.c].NZ) {
-            case 16: run_chunk<16, INTEG>(L, hd, it, r, tmem, bars, bar_ph); break;
-            case 32: run_chunk<32, INTEG>(L, hd, it, r, tmem, bars, bar_ph); break;
-            case 64: run_chunk<64, INTEG>(L, hd, it, r, tmem, bars, bar_ph); break;
-            default: run_chunk<128, INTEG>(L, hd, it, r, tmem, bars, bar_ph); break;
+            case 16: run_chunk<16, INTEG, REC>(L, hd, it, r, tmem, bars, bar_ph); break;
+            case 32: run_chunk<32, INTEG, REC>(L, hd, it, r, tmem, bars, bar_ph); break;
+            case 64: run_chunk<64, INTEG, REC>(L, hd, it, r, tmem, bars, bar_ph); break;
+            default: run_chunk<128, INTEG, REC>(L, hd, it, r, tmem, bars, bar_ph); break;
         }
         if (L.trace && tid == 0) {
             tc_sum += gtimer() - t1;
