@@ -297,7 +297,8 @@ struct ChunkHdr {
     int cn_old_init, diag_due, has_prev, pad2;
     int c, r, ok, top;
     unsigned tk;
-    int pad[3];
+    unsigned pre_tk;  // the next ticket, taken after the mode loop
+    int pre_ok, pad1;
 };
 
 // ---------------------------------------------------------------------------
@@ -947,6 +948,11 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
         }
     }
     if (leader) bar_ph[warp * MAX_PAIRS_PER_WARP + pi] = (unsigned char)phase;
+    // the CTA's next ticket, taken now so that the atomic's latency overlaps the sums below.
+    // Holding it cannot deadlock: what is left of this chunk (sums, count, mean-field stage)
+    // never waits, so the smallest unfinished ticket is always running or about to run.
+    unsigned nxt = 0;
+    if (tid == 0) nxt = atomicAdd(L.next, 1u);
     if (!ok && (lane & (2 * T - 1)) == 0) {
         if (atomicOr(&L.ctl->status, QLGPU_STATUS_TIMEOUT) == 0) {
             L.ctl->fail_case = c;
@@ -1016,6 +1022,10 @@ __device__ __noinline__ void run_chunk(const EnsLaunch& L, ChunkHdr& hd, const R
     (void)bc;
 
     // ---- count the chunk; the CTA that completes the case's stage runs the mean-field stage
+    if (tid == 0) {
+        hd.pre_tk = nxt;
+        hd.pre_ok = 1;
+    }
     __threadfence();
     __syncthreads();
     unsigned* ep = L.epoch + (size_t)c * BATCH_EPOCH_STRIDE;
@@ -1044,6 +1054,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) ens_kernel(const __grid_
     const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) {
         hd.ok = 0;
+        hd.pre_ok = 0;
         if (blockIdx.x == 0) L.ctl->t_start = gtimer();
     }
     // the staging barriers are initialised once per launch (a live barrier is never re-initialised);
@@ -1064,7 +1075,8 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) ens_kernel(const __grid_
         if (tid == 0) {
             unsigned tk = total;
             const unsigned long long t0 = L.trace ? gtimer() : 0ull;
-            if (!ld_volatile_i32(&L.ctl->abort)) tk = atomicAdd(L.next, 1u);
+            if (!ld_volatile_i32(&L.ctl->abort)) tk = hd.pre_ok ? hd.pre_tk : atomicAdd(L.next, 1u);
+            hd.pre_ok = 0;
             if (tk < total) {
                 // the case's previous stage must be complete (bounded wait)
                 const int r = (int)(tk / (unsigned)L.R);
